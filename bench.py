@@ -1,0 +1,398 @@
+#!/usr/bin/env python3
+"""Throughput of the pyro_cmc Monte Carlo hot path on B200, in spin-updates/s.
+
+Workload (the one line of output): the L=64 field-cool anneal
+(4,194,304 spins, J1=1, J2=0.1, J3=0.05, B=(0,0,0.5), FP32 spins, FP64
+accumulators). One step = one sampling temperature step of that anneal at
+T=0.5: 32 Metropolis+overrelaxation sweeps, an S(q) sample of all nine
+correlators after every 16 sweeps, one energy sample. A spin-update is one
+Metropolis proposal at one site (each sweep also overrelaxes every site), so a
+step is 32 * N spin-updates. Inputs are synthetic (uniform on S^2, device
+Philox). The lattice (67 MB) is smaller than L2, so the timed loop streams it
+from L2 as production runs do; between timed steps nothing is flushed.
+
+  value   device-timed steps, spins resident in HBM (CUDA events on the
+          system's stream, max over ranks)
+  e2e     the same steps through the host-buffer C-ABI call pc_step_host:
+          pinned-host spins in, spins and energy out, copies inside the timing
+  roofline  the Metropolis colour-pass kernel: 32 B (float4 read + write) per
+          updated site against the measured HBM copy bandwidth
+  cpu_baseline  the oracle (FP64 restatement of the reference sweep) on one
+          host core, on a bounded sample of the same lattice
+Also reported: the batched parallel-tempering form (128 replicas, L in
+{8,12,16,24} x 32 T) and the gradient form (256 x L=8 energy + S(q)
+forward/backward).
+
+--gpus N runs N independent replicas of the workload, one per GPU (the path
+has no exchange across GPUs): scaling "weak", value = all ranks' updates / the
+slowest rank's time. --impl reference runs the CPU reference arm (the oracle
+on all host cores) on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+METRIC = "spin-updates/s on 1 B200 (plain/batched/grad) at matched ⟨E⟩,C_v,S(q) vs CPU"
+UNIT = "spin-updates/s"
+WL = dict(L=64, J1=1.0, J2=0.1, J3=0.05, B=(0.0, 0.0, 0.5), T=0.5, n_sweep=32, ssf_every=16,
+          corr=["xx", "yy", "zz", "xy", "xz", "yz", "yx", "zx", "zy"])
+CONFIG = {"workload": "fieldcool L=64 sampling step (32 sweeps + 2 S(q) samples x 9 correlators + energy)",
+          "L": 64, "n_spins": 16 * 64 ** 3, "J": [1.0, 0.1, 0.05], "B": [0.0, 0.0, 0.5], "T": 0.5,
+          "n_sweep": 32, "ssf_every": 16, "n_corr": 9, "spins": "fp32", "accumulators": "fp64",
+          "l2": "lattice (67 MB) fits in L2; no flush between steps", "parallelism": "replicas"}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the Metropolis colour pass from the committed
+    ncu summary (profiles/colour_pass_L64.md, line 'traffic_bytes_per_launch:')."""
+    p = os.path.join(REPO, "profiles", "colour_pass_L64.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"pyro_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+def run_reference(args, rank):
+    """CPU reference arm: the oracle (the reference's algorithm, FP64,
+    sequential sweep) on all host cores, one independent L=64 lattice per
+    thread; each step is one sweep of every lattice."""
+    if rank != 0:
+        return
+    import oracle
+    ncores = os.cpu_count() or 1
+    mem_gb = 0.0
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                mem_gb = float(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    threads = max(1, min(ncores, int(mem_gb // 3) if mem_gb else ncores, 64))
+    b = oracle.Bench(WL["L"], WL["J1"], WL["J2"], WL["J3"], WL["B"], threads, seed=1)
+    for _ in range(args.warmup):
+        b.run(WL["T"], 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        b.run(WL["T"], 1)
+    dt = time.perf_counter() - t0
+    b.close()
+    rate = threads * b.N * args.steps / dt
+    sample = (f"{args.steps} timed sweeps (after {args.warmup} warm-up) of {threads} independent L=64 lattices "
+              f"(one per thread); Metropolis + overrelaxation, no S(q)")
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": CONFIG,
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_one_core():
+    import oracle
+    b = oracle.Bench(WL["L"], WL["J1"], WL["J2"], WL["J3"], WL["B"], 1, seed=3)
+    b.run(WL["T"], 1)
+    n = 4
+    rate = b.run(WL["T"], n)
+    b.close()
+    return {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} sweeps of one L=64 lattice (4,194,304 spins) after one warm-up sweep, single thread, "
+                      "Metropolis + overrelaxation (no S(q))"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and gradient forms")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    import pyro_cmc_b200 as pc
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    s = pc.pyrochlore_system(WL["L"], J1=WL["J1"], J2=WL["J2"], J3=WL["J3"], B=WL["B"], seed=1000 + rank)
+    s.set_stream(stream.cuda_stream)
+    s.random_spins(17 + rank)
+    s.ssf_configure(WL["corr"], 1)
+    N = s.N()
+    T = WL["T"]
+
+    def device_step():
+        for _ in range(WL["n_sweep"] // WL["ssf_every"]):
+            s.sweep(T, WL["ssf_every"], 1, count=False)
+            s.ssf_sample([0])
+        s.energy()
+
+    for _ in range(args.warmup):
+        device_step()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = s.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        device_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = s.launch_count() - l0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+    value = world * N * WL["n_sweep"] / (ms_max * 1e-3)
+
+    # kernel durations of the colour passes (events around every launch)
+    s.set_kernel_timing(True)
+    device_step()
+    t_met, t_or = s.kernel_times()
+    s.set_kernel_timing(False)
+
+    # end to end through host buffers
+    S4_in = torch.empty((N, 4), dtype=torch.float32, pin_memory=True).numpy()
+    S4_out = torch.empty((N, 4), dtype=torch.float32, pin_memory=True).numpy()
+    S4_in[:] = s.spins_f4()
+    for _ in range(args.warmup):
+        s.step_host(S4_in, S4_out, T, WL["n_sweep"], WL["ssf_every"], 0)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.step_host(S4_in, S4_out, T, WL["n_sweep"], WL["ssf_every"], 0)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = max_over_ranks(e2e_s)
+    e2e = {"value": world * N * WL["n_sweep"] / e2e_s, "unit": UNIT, "h2d_bytes_per_step": N * 16,
+           "d2h_bytes_per_step": N * 16 + 8, "ms_per_step": e2e_s * 1e3,
+           "call": "pc_step_host (pinned host spins in/out)"}
+
+    peak, peak_kind = measured_peaks()
+    alg_bytes = 32.0 * s.Nc()  # one colour pass: one sublattice, float4 read + write per site
+    achieved = alg_bytes / (t_met * 1e-3) / 1e9 if t_met > 0 else None
+    traffic = profile_traffic()
+    roofline = {"bound": "hbm", "kernel": "colour_pass_kernel<Metropolis>", "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "launch_ms": t_met,
+                "overrelax_launch_ms": t_or,
+                "note": "achieved = 32 B x Nc sites per launch / mean CUDA-event launch duration; the neighbour "
+                        "reads (30 float4 per site) are L2 traffic and not counted"}
+
+    extras = {}
+    if not args.no_extras and rank == 0:
+        extras = run_extras(pc, torch, np)
+
+    if rank == 0:
+        cpu = None if (args.no_cpu or world > 1) else cpu_baseline_one_core()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
+                "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
+                "clocks": clk}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    del s
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_extras(pc, torch, np):
+    out = {}
+    stream = torch.cuda.current_stream()  # the non-default stream main() set
+    # batched parallel tempering: 128 replicas, L in {8,12,16,24} x 32 T in [0.02, 2]
+    Ls = [8] * 32 + [12] * 32 + [16] * 32 + [24] * 32
+    Tl = np.geomspace(2.0, 0.02, 32)
+    T = np.concatenate([Tl] * 4)
+    b = pc.pyrochlore_system(Ls, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=7)
+    b.set_stream(stream.cuda_stream)
+    b.random_spins(5)
+    b.pt_configure(T)
+    b.ssf_configure(["xx", "yy", "zz"], len(Ls), sorted(Ls))
+    b.pt_run(8, 10, 16)  # warm-up and graph capture (80 sweeps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rounds = 40
+    e0.record(stream)
+    b.pt_run(rounds, 10, 16)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    n_tot = sum(16 * L ** 3 for L in Ls)
+    batched = n_tot * rounds * 10 / (ms * 1e-3)
+    att, acc = b.pt_exchange_stats()
+    del b
+    # plain single small replica (L=8), the comparison point for batching
+    p1 = pc.pyrochlore_system(8, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=9)
+    p1.set_stream(stream.cuda_stream)
+    p1.random_spins(1)
+    p1.sweep(0.5, 20, 1, count=False)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    p1.sweep(0.5, 200, 1, count=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_small = p1.N() * 200 / (e0.elapsed_time(e1) * 1e-3)
+    del p1
+    out["batched"] = {"value": batched, "unit": UNIT,
+                      "config": "parallel tempering, 128 replicas (L 8/12/16/24 x 32 T geometric in [0.02, 2]), "
+                                "J=(1,0,0.02), B=(0,0,0.1), exchange every 10 sweeps, S(q) xx/yy/zz every 16 sweeps",
+                      "ms_per_10_sweeps": ms / rounds, "exchange_accept": float(acc.sum()) / max(1.0, float(att.sum())),
+                      "plain_single_L8": plain_small, "batched_over_plain_L8": batched / plain_small}
+    # gradient form: 256 x L=8 energy + S^zz(q) forward/backward
+    from pyro_cmc_b200 import autograd as ag
+    B = 256
+    g = pc.pyrochlore_system(8, n_replicas=B, J1=1.0, J2=0.1, J3=-0.05, B=(0.2, 0, 0), seed=3)
+    g.set_stream(stream.cuda_stream)
+    g.ssf_configure(["zz"], 0, [])
+    g.random_spins(11)
+    spins = ag.spins_tensor(g).clone().requires_grad_(True)
+    w = torch.rand((B, 1, 512), device="cuda", dtype=torch.float64)
+    target = torch.zeros((B, 1, 512), device="cuda", dtype=torch.float64)
+
+    def fwd_bwd():
+        e = ag.energy(g, spins)
+        S = ag.ssf(g, spins)
+        loss = (w * (S[..., 0] - target) ** 2).sum() * 1e-8 + e.sum()
+        loss.backward()
+        return loss
+
+    for _ in range(3):
+        fwd_bwd()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(5):
+        with torch.no_grad():
+            ag.energy(g, spins)
+            ag.ssf(g, spins)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / 5
+    e0.record(stream)
+    for _ in range(5):
+        fwd_bwd()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fb_ms = e0.elapsed_time(e1) / 5
+    out["grad"] = {"value": B * g.N() / (fb_ms * 1e-3), "unit": "spins/s (energy + S^zz(q) forward and backward)",
+                   "config": "256 x L=8 (2,097,152 spins), J=(1,0.1,-0.05), B=(0.2,0,0)",
+                   "forward_ms": fwd_ms, "forward_backward_ms": fb_ms,
+                   "backward_over_forward": (fb_ms - fwd_ms) / fwd_ms}
+    del g
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,251 @@
+/*
+ * pyrocmc.h -- C ABI of the B200 (sm_100a) Monte Carlo engine for classical
+ * Heisenberg spins on the pyrochlore lattice (libpyrocmc.so).
+ *
+ * This is the boundary the reference's C++ interfaces sit on: the C++ shims in
+ * pyro_cmc_b200/host/ (CMC::MC_runner, ssf_manager, energy_manager) and the
+ * Python bindings (pyro_cmc_b200/_lib.py) call only these functions. Every
+ * function returns 0 (PC_OK) on success or a PC_ERR_* code; the message of the
+ * last failure on the calling thread is returned by pc_last_error().
+ *
+ * Plain pointers and sizes only. "host" arrays are ordinary CPU memory;
+ * "device" pointers are CUDA global memory on the system's device.
+ *
+ * Conventions (fixed by this library; the reference leaves them to lattice_lib):
+ *   site index   i = sl * Nc + cell, sl = 4*f + p (16 sublattices, pyro_sl = p),
+ *                cell = cx + L*(cy + L*cz), Nc = L^3, N = 16*Nc
+ *                (sublattice-major like src/MC.cpp:32);
+ *   position     x_i = 8*(cx,cy,cz) + R_fcc[f] + link[p]
+ *                (include/pyrochlore_geometry.hpp:12-32);
+ *   k points     K in [0,L)^3, q = 2*pi*K/(8L), flat k = (K0*L + K1)*L + K2;
+ *   SSF          S^{ab}(q) = conj(B^a(q)) B^b(q), B^a(q) = sum_i exp(-i q.x_i) S^a_i
+ *                (equal to ssf_manager's phase-contracted sum,
+ *                include/ssf_manager.hpp:260-293, with a forward-signed,
+ *                unnormalised DFT).
+ *   RNG          Philox4x32-10, key = seed, counter = (site, sweep lo32,
+ *                draw | sweep hi32 << 8, replica); draw 0 = Metropolis,
+ *                2+k = overrelaxation pass k, 250 = random initial state,
+ *                251 = replica exchange.
+ */
+#ifndef PYROCMC_H
+#define PYROCMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PC_OK 0
+#define PC_ERR_INVALID 1     /* bad argument (reference: std::invalid_argument / logic_error) */
+#define PC_ERR_CUDA 2        /* CUDA runtime failure */
+#define PC_ERR_STATE 3       /* call out of order (e.g. sweep before setup_lattice) */
+#define PC_ERR_UNSUPPORTED 4 /* configuration this build does not handle */
+#define PC_ERR_TIMEOUT 5     /* a bounded device-side wait gave up */
+
+typedef struct pc_system pc_system;
+
+/* Message of the last failure on this thread ("" if none). */
+const char* pc_last_error(void);
+/* Library ABI version (major*100 + minor). */
+int pc_version(void);
+
+/* ---------------------------------------------------------------- lifetime */
+
+/* Creates n_replicas independent lattices of L[r]^3 cubic cells each (uneven L
+ * allowed) on the current CUDA device. One replica is the reference's single
+ * Lattice; several are the batched replicas that replace temper's MPI ranks.
+ * Replaces MC_runner(Lattice&, size_t seed) (include/MC.hpp:107-112); the seed
+ * is the Philox key, used as given (no seed-table lookup). */
+int pc_create(int n_replicas, const int32_t* L, uint64_t seed, pc_system** out);
+int pc_destroy(pc_system* sys);
+/* Makes the system launch on an existing CUDA stream (cudaStream_t) instead of
+ * its own, e.g. the caller's framework stream; the caller keeps ownership. */
+int pc_set_stream(pc_system* sys, void* stream);
+
+/* MC_runner::define_coupling (include/MC.hpp:121-124, src/MC.cpp:56-66).
+ * rel_vecs: displacement vectors for pyro_sl 0..3 concatenated, n_rel[p] of
+ * them for sublattice p, 3 int64 each. J: 3x3 row-major, applied by the source
+ * (lower pyro_sl) endpoint; the target endpoint applies J^T.
+ * Duplicate names fail with PC_ERR_INVALID ("Coupling names must be unique"). */
+int pc_define_coupling(pc_system* sys, const char* name, const int64_t* rel_vecs, const int32_t* n_rel,
+                       const double* J);
+/* Replaces the matrix of coupling `spec` (definition order) after setup,
+ * rebuilding the bond tables (and colour classes, which follow the nonzero
+ * bonds). Used by the differentiable path to move J. */
+int pc_set_coupling_matrix(pc_system* sys, int spec, const double* J);
+/* MC_runner::set_global_field / get_global_field (include/MC.hpp:126-127). */
+int pc_set_global_field(pc_system* sys, const double* B3);
+int pc_get_global_field(pc_system* sys, double* B3);
+/* MC_parameters::T_ref (include/MC.hpp:79-82): proposal width sqrt(T/T_ref). */
+int pc_set_T_ref(pc_system* sys, double T_ref);
+/* Overrelaxation form: 0 = random-angle rotation about the local field
+ * (overrelax_all, src/MC.cpp:145-153; default), 1 = reflection
+ * (mirror_about_vector, src/MC.cpp:98-100). */
+int pc_set_overrelax_mode(pc_system* sys, int mode);
+/* Colour classes of the sweep. 0 (default): one class per sublattice, in
+ * sublattice order -- the sweep then visits sites in exactly the reference's
+ * sequential storage order (spins[sl*Nc + cell], src/MC.cpp:157), so the Markov
+ * chain is the reference's. 1: fewest classes (sublattices joined by no
+ * nonzero bond share a class: 4 pyro_sl classes when J3 = 0); a different,
+ * equally valid visiting order with fewer launches. Call before setup. */
+int pc_set_colouring(pc_system* sys, int mode);
+/* MC_runner::setup_lattice (src/MC.cpp:15-52): builds the per-sublattice bond
+ * shells, the colour classes and uploads them. Must follow all couplings. */
+int pc_setup_lattice(pc_system* sys);
+
+/* Pyrochlore displacement tables, derived from the geometry (the vectors d
+ * with |d|^2 = 8, 24, 32 from a site of pyro_sl p to another site):
+ * kind 1 = J1 (nn1_dist, include/pyrochlore_geometry.hpp:110-115),
+ * 2 = J2 (nn2_dist, :117-134), 3 = J3a (nn3a_dist, :137-142; the midpoint is a
+ * site), 4 = J3b (nn3b_dist, :144-149), 10 + nu = the J1 vectors from p that
+ * land on pyro_sl nu (nn1_pair_MN, :151-190). Writes *n vectors (3 int64 each)
+ * into out (room for max_n). */
+int pc_pyrochlore_displacements(int kind, int pyro_sl, int64_t* out, int max_n, int* n);
+
+/* ------------------------------------------------------------ inspection */
+
+int pc_num_replicas(pc_system* sys, int* n);
+int pc_num_spins(pc_system* sys, int replica, int64_t* n);
+/* Colour classes used by the sweep: colour_of_sl[16]. */
+int pc_colours(pc_system* sys, int* n_colours, int32_t* colour_of_sl);
+/* Neighbour site indices of every site of a replica for coupling `spec`
+ * (definition order), in that spec's displacement order: out[N][max_nb], -1
+ * padded. The bit-exact geometry check against the reference tables. */
+int pc_neighbour_table(pc_system* sys, int replica, int spec, int max_nb, int32_t* out);
+/* ipos of each site (wrapped into [0, 8L)) and its sublattice. */
+int pc_site_positions(pc_system* sys, int replica, int64_t* pos, int32_t* sl);
+/* Number of kernels this system has launched so far (graph replays count
+ * their kernel nodes). */
+int pc_launch_count(pc_system* sys, uint64_t* n);
+
+/* ----------------------------------------------------------------- spins */
+
+/* Host <-> device spin state, N x 3 doubles (the Lattice mirror sync). */
+int pc_set_spins(pc_system* sys, int replica, const double* S);
+int pc_get_spins(pc_system* sys, int replica, double* S);
+/* Same, in the device layout: N x 4 floats (x, y, z, unused). */
+int pc_set_spins_f4(pc_system* sys, int replica, const float* S4);
+int pc_get_spins_f4(pc_system* sys, int replica, float* S4);
+/* Uniform on S^2 for every replica, drawn on the device (Philox draw 250). */
+int pc_random_spins(pc_system* sys, uint64_t seed);
+/* Device address of a replica's spin array (float4[N]); valid until destroy. */
+int pc_spins_device(pc_system* sys, int replica, void** dev_ptr);
+/* The per-replica sweep counter (Philox counter); settable for exact resume. */
+int pc_get_sweep_counter(pc_system* sys, int replica, uint64_t* sweep);
+int pc_set_sweep_counter(pc_system* sys, int replica, uint64_t sweep);
+
+/* -------------------------------------------------------------------- MC */
+
+/* MC_runner::sweep_local_Metropolis(T, n_overrelax) (src/MC.cpp:155-163) for
+ * every replica at once, n_sweeps times: one Metropolis pass (Gaussian kick
+ * of width sqrt(T/T_ref), renormalised, src/MC.cpp:111-130) then n_overrelax
+ * overrelaxation passes, each over the colour classes in order.
+ * T[r] per replica (host array). accepted[r] (host, may be NULL) receives the
+ * accepted Metropolis moves summed over the n_sweeps sweeps. */
+int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uint64_t* accepted);
+/* overrelax_all (src/MC.cpp:145-153) alone, with deterministic angles:
+ * theta (host, N doubles for `replica`) or NULL for reflection. For parity
+ * tests of one overrelaxation pass. */
+int pc_overrelax_theta(pc_system* sys, int replica, const double* theta);
+/* total_energy_per_unit_cell (src/MC.cpp:305-312) of every replica (host
+ * e_per_cell[R]) and the magnetisation sum_i S_i (host mag[R][3], may be NULL).
+ * FP64 accumulation. */
+int pc_energy(pc_system* sys, double* e_per_cell, double* mag);
+/* MC_runner::local_field (src/MC.cpp:87-96) of every site of a replica,
+ * without the global field: host h[N][3]. */
+int pc_local_field(pc_system* sys, int replica, double* h);
+
+/* ------------------------------------------------------------------- SSF */
+
+/* ssf_manager constructor (include/ssf_manager.hpp:161-201): the correlator
+ * labels ("xx", "xy", ...; two of x/y/z each) and n_slots accumulator slots
+ * (temperatures), each for replicas of size L_of_slot[slot]. Bad labels fail
+ * with PC_ERR_INVALID and the reference's message. Clears all slots. */
+int pc_ssf_configure(pc_system* sys, const char* const* names, int n_corr, int n_slots, const int32_t* L_of_slot);
+/* ssf_manager::sample (include/ssf_manager.hpp:260-293) for every replica r
+ * with slot_of_replica[r] >= 0 (host array): accumulates S(q) and
+ * (Re S)^2, (Im S)^2 into that slot in FP64 and counts the sample. */
+int pc_ssf_sample(pc_system* sys, const int32_t* slot_of_replica);
+/* Copies a slot out: sum and sq as [n_corr][n_k][2] doubles, n_samples. */
+int pc_ssf_read(pc_system* sys, int slot, double* sum, double* sq, uint64_t* n_samples);
+int pc_ssf_clear(pc_system* sys, int slot);
+/* S(q) of the current configuration of one replica, no accumulation:
+ * out[n_corr][n_k][2] (host). */
+int pc_ssf_current(pc_system* sys, int replica, double* out);
+
+/* -------------------------------------------------------- tempering / energy */
+
+/* Sets up batched parallel tempering over all replicas (replaces the MPI
+ * ranks of src/temper.cpp). Replicas with equal L form a ladder; T[r] is the
+ * initial temperature of replica r, and the ladder's slots are its
+ * temperatures sorted descending (slot order = temper's rank order). Energy
+ * accumulators (energy_manager, include/energy_manager.hpp:19-48) are kept per
+ * slot. Exchange attempts are decided on the device. */
+int pc_pt_configure(pc_system* sys, const double* T);
+/* n_rounds rounds of: n_sweep sweeps at each replica's current temperature;
+ * an SSF sample into the replica's slot whenever the sweep count reaches a
+ * multiple of ssf_every (0 = never; needs pc_ssf_configure with one slot per
+ * replica); one energy sample per slot; a checkerboard exchange attempt
+ * between adjacent temperatures of every ladder (pairs (0,1),(2,3).. on even
+ * rounds, (1,2),.. on odd, src/temper.cpp:437-473). The schedule is captured
+ * as a CUDA graph and replayed. */
+int pc_pt_run(pc_system* sys, int n_rounds, int n_sweep, int ssf_every);
+/* Zeroes the energy accumulators and exchange statistics (after burn-in);
+ * the replica-to-slot assignment and the spins are kept. */
+int pc_pt_reset_stats(pc_system* sys);
+/* Per-slot energy accumulators (sum e, sum e^2, count) and temperatures. */
+int pc_pt_read_energy(pc_system* sys, double* T, double* E, double* E2, uint64_t* n);
+/* Per-slot exchange statistics: attempts/accepts of the pair (slot, slot+1). */
+int pc_pt_read_exchange(pc_system* sys, uint64_t* attempts, uint64_t* accepts);
+/* Current slot of every replica. */
+int pc_pt_slots(pc_system* sys, int32_t* slot_of_replica);
+
+/* ------------------------------------------------------- differentiation */
+
+/* Energy and its gradient for every replica (the autograd path). With upstream
+ * scalar g[r] for e_per_cell[r]:
+ *   grad_S[r][i] = g[r]/Nc * (h_i - B)            (device, float4[N_total], may be NULL)
+ *   grad_J[r][spec][9] = g[r]/Nc * dE/dJ_spec      (host, may be NULL)
+ *   grad_B[r][3] = -g[r]/Nc * sum_i S_i            (host, may be NULL)
+ * and e_per_cell[r] (host). dE/dJ_spec[a][b] = sum over the spec's bonds of
+ * S_src[a] S_tgt[b]. */
+int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* grad_S_dev, double* grad_J,
+                   double* grad_B);
+/* S(q) for every replica into a device buffer out_dev[R][n_corr][n_k][2]
+ * (float64), no accumulation. Uses the correlators of pc_ssf_configure. */
+int pc_ssf_forward(pc_system* sys, void* out_dev);
+/* Backward of pc_ssf_forward: given dLoss/dS (device, same layout as
+ * out_dev: d/dRe, d/dIm), writes dLoss/dS_i into grad_S_dev (float4[N_total],
+ * device). Recomputes the forward transform instead of storing it. */
+int pc_ssf_backward(pc_system* sys, const void* grad_out_dev, void* grad_S_dev);
+
+/* ------------------------------------------------------------------ tuning */
+
+/* Times the sweep kernel over the candidate tile shapes on this system and
+ * keeps the fastest (spin state is saved and restored). */
+int pc_autotune(pc_system* sys);
+/* Current tile shape (threads per CTA, CTAs per SM). */
+int pc_get_tile(pc_system* sys, int* threads, int* ctas_per_sm);
+int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm);
+
+/* --------------------------------------------------------------- bench API */
+
+/* One end-to-end step through host buffers: copies S4_in (host, N x 4 floats,
+ * pinned for full speed) to replica 0, runs n_sweep sweeps at temperature T
+ * with an SSF sample into ssf_slot after every ssf_every sweeps (ssf_slot < 0
+ * or ssf_every = 0: none), takes one energy sample, and copies the spins back
+ * to S4_out and the energy per cell to *e_out. */
+int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, int n_sweep, int ssf_every,
+                 int ssf_slot, double* e_out, uint64_t* accepted);
+/* CUDA events around the last pc_sweep call's kernels: average duration in
+ * milliseconds of the Metropolis and overrelaxation colour-pass kernels. */
+int pc_last_kernel_times(pc_system* sys, double* metropolis_ms, double* overrelax_ms);
+/* Enables per-kernel CUDA-event timing (off by default). */
+int pc_set_kernel_timing(pc_system* sys, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYROCMC_H */

@@ -1,0 +1,182 @@
+"""Differentiable energy and S(q) as torch.autograd.Functions over the C ABI.
+
+Spins are a float32 CUDA tensor [N_total, 4] (x, y, z, unused) in the
+engine's layout: replicas back to back, each sublattice-major
+(site = sl*Nc + cell). Energies are per cubic cell, float64 [R]. S(q) is
+float64 [R, n_corr, n_k, 2] (Re, Im) for the correlators configured with
+System.ssf_configure.
+
+  energy(system, spins, params=None) -> e[R]
+      d/dspins: g/Nc * (h_i - B) (the reference's local field minus the
+      global field, src/MC.cpp:113); d/dparams for params = [J1, J2, J3, Bx,
+      By, Bz] of a pyrochlore system (define_pyrochlore): dE/dJ1 sums the six
+      pair specs through J1[I + (Delta-1) z_mu z_nu], dE/dJ3 the J3a and J3b
+      specs. Hand-written kernel (pc_energy_grad).
+  ssf(system, spins) -> S
+      backward recomputes the forward transform and applies its adjoint
+      (pc_ssf_backward); no transform is stored.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .engine import PAIRS, System, local_axis
+
+
+class _DeviceArray:
+    """Exposes a raw device pointer to torch through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"data": (ptr, False), "shape": tuple(shape), "typestr": typestr,
+                                         "version": 3, "strides": None}
+
+
+def spins_tensor(system: System) -> torch.Tensor:
+    """The system's own device spin buffer as a [N_total, 4] float32 tensor
+    (a view, no copy)."""
+    ptr = system.spins_device_ptr(0)
+    return torch.as_tensor(_DeviceArray(ptr, (system.N_total, 4), "<f4"), device="cuda")
+
+
+def _load(system: System, spins: torch.Tensor):
+    if spins.shape != (system.N_total, 4) or spins.dtype != torch.float32 or not spins.is_cuda:
+        raise ValueError("spins must be a float32 CUDA tensor of shape [N_total, 4]")
+    dst = spins_tensor(system)
+    if spins.data_ptr() != dst.data_ptr():
+        dst.copy_(spins.detach())
+        torch.cuda.current_stream().synchronize()
+
+
+def _apply_params(system: System, params: torch.Tensor):
+    """Sets J1, J2, J3 and B of a pyrochlore system from params[6]."""
+    pp = getattr(system, "pyro_params", None)
+    if pp is None:
+        raise ValueError("params need a system built with define_pyrochlore")
+    J1, J2, J3, bx, by, bz = [float(x) for x in params.detach().cpu().tolist()]
+    if (J1, J2, J3) != (pp["J1"], pp["J2"], pp["J3"]):
+        I3 = np.eye(3)
+        k = 0
+        if pp["split_J1"]:
+            for mu, nu in PAIRS:
+                system.set_coupling_matrix(k, J1 * (I3 + (pp["Delta"] - 1.0) * np.outer(local_axis(mu), local_axis(nu))))
+                k += 1
+        else:
+            system.set_coupling_matrix(k, J1 * I3)
+            k += 1
+        for j in (J2, J3, J3):
+            system.set_coupling_matrix(k, j * I3)
+            k += 1
+        pp.update(J1=J1, J2=J2, J3=J3)
+    system.set_global_field([bx, by, bz])
+
+
+def _param_grads(system: System, gJ: np.ndarray, gB: np.ndarray) -> np.ndarray:
+    """dE/d[J1, J2, J3, Bx, By, Bz] per replica from the per-spec matrix grads."""
+    pp = system.pyro_params
+    R = gJ.shape[0]
+    out = np.zeros((R, 6))
+    k = 0
+    I3 = np.eye(3)
+    if pp["split_J1"]:
+        for mu, nu in PAIRS:
+            dM = I3 + (pp["Delta"] - 1.0) * np.outer(local_axis(mu), local_axis(nu))
+            out[:, 0] += np.einsum("rab,ab->r", gJ[:, k], dM)
+            k += 1
+    else:
+        out[:, 0] += np.einsum("raa->r", gJ[:, k])
+        k += 1
+    out[:, 1] = np.einsum("raa->r", gJ[:, k])
+    out[:, 2] = np.einsum("raa->r", gJ[:, k + 1]) + np.einsum("raa->r", gJ[:, k + 2])
+    out[:, 3:] = gB
+    return out
+
+
+class EnergyFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, spins, params, system):
+        if params is not None:
+            _apply_params(system, params)
+        _load(system, spins)
+        e, _ = system.energy()
+        ctx.system = system
+        ctx.has_params = params is not None
+        ctx.save_for_backward(spins)
+        return torch.as_tensor(e, dtype=torch.float64, device=spins.device)
+
+    @staticmethod
+    def backward(ctx, grad_e):
+        system = ctx.system
+        (spins,) = ctx.saved_tensors
+        _load(system, spins)
+        g = grad_e.detach().to("cpu", torch.float64).numpy()
+        grad_spins = torch.zeros_like(spins)
+        _, gJ, gB = system.energy_grad(g, grad_spins.data_ptr())
+        gp = None
+        if ctx.has_params:
+            gp = torch.as_tensor(_param_grads(system, gJ.reshape(system.R, -1, 3, 3), gB).sum(axis=0),
+                                 dtype=torch.float64, device=spins.device)
+        return grad_spins, gp, None
+
+
+class SSFFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, spins, system):
+        _load(system, spins)
+        nk = system.Nc(0)
+        out = torch.empty((system.R, system.n_corr, nk, 2), dtype=torch.float64, device=spins.device)
+        torch.cuda.current_stream().synchronize()
+        system.ssf_forward_device(out.data_ptr())
+        ctx.system = system
+        ctx.save_for_backward(spins)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        system = ctx.system
+        (spins,) = ctx.saved_tensors
+        _load(system, spins)
+        go = grad_out.detach().to(torch.float64).contiguous()
+        grad_spins = torch.empty_like(spins)
+        torch.cuda.current_stream().synchronize()
+        system.ssf_backward_device(go.data_ptr(), grad_spins.data_ptr())
+        return grad_spins, None
+
+
+def energy(system: System, spins: torch.Tensor, params: torch.Tensor | None = None) -> torch.Tensor:
+    return EnergyFunction.apply(spins, params, system)
+
+
+def ssf(system: System, spins: torch.Tensor) -> torch.Tensor:
+    if len(set(system.L)) != 1:
+        raise ValueError("the differentiable S(q) needs replicas of one size")
+    return SSFFunction.apply(spins, system)
+
+
+def project_tangent(grad: torch.Tensor, spins: torch.Tensor) -> torch.Tensor:
+    """Removes the radial part of a spin gradient: g - (g.S) S (spins stay on S^2)."""
+    S = spins[:, :3]
+    g = grad[:, :3]
+    out = torch.zeros_like(grad)
+    out[:, :3] = g - (g * S).sum(dim=1, keepdim=True) * S
+    return out
+
+
+def gradient_quench(system: System, steps: int = 500, lr: float = 0.05) -> np.ndarray:
+    """Projected gradient descent of the energy on S^2 for every replica
+    (S <- normalise(S - lr * tangent grad)), from the system's current spins.
+    Returns the energy per cubic cell of each replica after every step."""
+    spins = spins_tensor(system)
+    hist = []
+    for _ in range(steps):
+        g = torch.zeros_like(spins)
+        e, _, _ = system.energy_grad(None, g.data_ptr())
+        hist.append(e)
+        t = project_tangent(g, spins)
+        new = spins[:, :3] - lr * t[:, :3]
+        new = new / new.norm(dim=1, keepdim=True)
+        spins[:, :3] = new
+        torch.cuda.current_stream().synchronize()
+    e, _ = system.energy()
+    hist.append(e)
+    return np.array(hist)

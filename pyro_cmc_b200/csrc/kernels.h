@@ -1,0 +1,134 @@
+// kernels.h -- launch interface between the host system (system.cu) and the
+// kernels (sweep.cu, ssf.cu, pt.cu). Plain structs, no torch types.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace pc {
+
+enum PassMode { kMetropolis = 0, kOverrelaxRotate = 1, kOverrelaxReflect = 2, kOverrelaxTheta = 3 };
+
+struct PassArgs {
+    float4* spins;
+    const ReplicaDev* reps;
+    const double* T_rep;         // per-replica temperature (device)
+    const uint64_t* sweep_base;  // device sweep counter
+    uint64_t sweep_offset;       // added to *sweep_base
+    uint64_t seed;
+    float inv_T_ref;
+    float B[3];
+    const SlTable* tables;  // 16 sublattice tables (device)
+    int n_tab;              // sublattices of this colour
+    int tab_sl[4];
+    const Tile* tiles;
+    int n_tiles;
+    unsigned long long* acc;  // per-replica accepted Metropolis moves (device)
+    int or_pass;              // overrelaxation pass index (draw 2 + or_pass)
+    const double* theta;      // kOverrelaxTheta: per-site angle of replica theta_replica (device)
+    int theta_replica;
+};
+
+void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st);
+
+struct EnergyArgs {
+    const float4* spins;
+    const ReplicaDev* reps;
+    const SlTable* tables;  // 16 tables
+    const Tile* tiles;      // all sublattices of all replicas, replica-contiguous
+    int n_tiles;
+    float B[3];
+    double* partial;  // [n_tiles][4]: sum (0.5 S.h - S.B), sum S
+};
+void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st);
+// Sums the tile partials of each replica in tile order: e[r] = sum/Nc, mag[r][3].
+void launch_energy_finalize(const double* partial, const int32_t* tile_begin, const int32_t* tile_end,
+                            const ReplicaDev* reps, int R, double* e, double* mag, cudaStream_t st);
+
+struct FieldArgs {
+    const float4* spins;
+    const ReplicaDev* reps;
+    const SlTable* tables;
+    const Tile* tiles;
+    int n_tiles;
+    float4* h_out;  // local field per site (global float4 layout), no global field
+};
+void launch_local_field(const FieldArgs& a, int threads, cudaStream_t st);
+
+struct GradArgs {
+    const float4* spins;
+    const ReplicaDev* reps;
+    const SlTable* tables;  // full tables (zero shells kept)
+    const Tile* tiles;
+    int n_tiles;
+    int n_spec;
+    float B[3];
+    const double* g;   // per-replica upstream scalar (device)
+    float4* grad_S;    // may be null
+    double* partial;   // [n_tiles][4 + 9*n_spec]
+};
+void launch_energy_grad_partials(const GradArgs& a, int threads, cudaStream_t st);
+void launch_grad_finalize(const double* partial, int width, const int32_t* tile_begin, const int32_t* tile_end,
+                          int R, double* out /*[R][width]*/, cudaStream_t st);
+
+void launch_random_spins(float4* spins, const ReplicaDev* reps, const Tile* tiles, int n_tiles, uint64_t seed,
+                         int threads, cudaStream_t st);
+void launch_advance_counter(uint64_t* counter, uint64_t n, cudaStream_t st);
+
+// ------------------------------------------------------------------ SSF
+struct SsfGeom {
+    int L;
+    int P, Q;  // L = P*Q, two-level Cooley-Tukey split
+    int n_rep;
+    const int32_t* rep_index;  // replicas of this size (device)
+};
+
+// Raises the dynamic shared-memory limits of the SSF kernels (once, host side).
+void ssf_prepare();
+// Stage 1: per (replica, z-plane, z-group): xy DFT of the 4 sublattices of the
+// group, times their xy sublattice phases, summed. G[rep][3][4][L][L][L] float2.
+void launch_ssf_xy(const SsfGeom& g, const float4* spins, const ReplicaDev* reps, float2* G, cudaStream_t st);
+// Stage 2 outputs.
+struct SsfOut {
+    int n_corr;
+    int corr_a[9], corr_b[9];
+    // accumulate mode: sum/sq [slot][n_corr][n_k][2] doubles, slot per replica
+    double* acc_sum;
+    double* acc_sq;
+    const int32_t* slot_of_rep;  // indexed by replica index
+    int64_t slot_stride;         // doubles per slot (n_corr*n_k*2)
+    // value mode: S(q) per replica into val[rep_pos][n_corr][n_k][2]
+    double* val;
+    // amplitude mode: B^a(K) per replica into amp[rep_pos][3][n_k] float2
+    float2* amp;
+};
+void launch_ssf_z(const SsfGeom& g, const float2* G, const SsfOut& o, cudaStream_t st);
+// Backward: Y^c(K) from upstream dS (val layout) and amplitudes; then adjoint
+// transform into grad_S (float4 per site, xyz components written).
+void launch_ssf_adjoint(const SsfGeom& g, const SsfOut& o, const double* dval, const float2* amp, float2* H,
+                        float4* grad_S, const ReplicaDev* reps, cudaStream_t st);
+
+// ------------------------------------------------------------- tempering
+struct PtArgs {
+    int n_ladders;
+    const int32_t* ladder_begin;  // slots of ladder l: [ladder_begin[l], ladder_begin[l+1])
+    const double* T_slot;         // temperature of each slot
+    int32_t* rep_of_slot;
+    int32_t* slot_of_rep;
+    double* T_rep;           // updated: T_rep[r] = T_slot[slot_of_rep[r]]
+    const double* e_rep;     // energy per cell of each replica
+    const ReplicaDev* reps;  // for Nc
+    double* E_sum;           // per slot
+    double* E2_sum;
+    unsigned long long* n_e;
+    unsigned long long* attempts;  // per lower slot
+    unsigned long long* accepts;
+    uint64_t* round;  // device round counter (parity + Philox counter)
+    uint64_t seed;
+    int n_slots;
+};
+void launch_pt_exchange(const PtArgs& a, cudaStream_t st);
+
+}  // namespace pc

@@ -1,0 +1,409 @@
+// sweep.cu -- colour-sliced Metropolis / overrelaxation passes, energy and
+// local-field reductions, energy gradient (sm_100a).
+//
+// One launch updates one colour class: sublattices that share no bond, so all
+// their sites are updated in parallel with the result of a sequential pass in
+// storage order (src/MC.cpp:155-163 visits spins[sl*Nc + cell] in order; inside
+// one sublattice the order is immaterial because no two of its sites are
+// bonded). Spins are float4 (x, y, z, unused) in sublattice-major SoA order,
+// so a warp reads 32 consecutive cells of one sublattice: its own spins and
+// each neighbour slot are coalesced 512-byte loads. The colour's bond tables
+// are staged once per CTA in shared memory; CTAs loop over tiles.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pc {
+
+__device__ __forceinline__ void stage_tables(SlTable* dst, const SlTable* src, int n_tab, const int* sls) {
+    const int words = int(sizeof(SlTable) / 4);
+    for (int t = 0; t < n_tab; ++t) {
+        const int* s = reinterpret_cast<const int*>(src + sls[t]);
+        int* d = reinterpret_cast<int*>(dst + t);
+        for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = s[i];
+    }
+}
+
+// h = sum over shells J_k * sum of neighbour spins (MC_runner::local_field,
+// src/MC.cpp:87-96).
+__device__ __forceinline__ float3 local_field(const float4* __restrict__ S, const SlTable& tb, int cx, int cy, int cz,
+                                              int L, int Nc) {
+    float hx = 0.f, hy = 0.f, hz = 0.f;
+    int e = 0;
+    const int ns = tb.n_shell;
+    for (int k = 0; k < ns; ++k) {
+        float tx = 0.f, ty = 0.f, tz = 0.f;
+        const int end = tb.shell_end[k];
+        for (; e < end; ++e) {
+            const NbEntry nb = tb.nb[e];
+            const int x = wrap1(cx + nb.dx, L), y = wrap1(cy + nb.dy, L), z = wrap1(cz + nb.dz, L);
+            const float4 o = __ldg(&S[size_t(nb.sl) * Nc + x + L * (y + L * z)]);
+            tx += o.x;
+            ty += o.y;
+            tz += o.z;
+        }
+        const float* J = tb.J[k];
+        hx += J[0] * tx + J[1] * ty + J[2] * tz;
+        hy += J[3] * tx + J[4] * ty + J[5] * tz;
+        hz += J[6] * tx + J[7] * ty + J[8] * tz;
+    }
+    return make_float3(hx, hy, hz);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(512) colour_pass_kernel(const PassArgs a) {
+    __shared__ SlTable tab[4];
+    __shared__ unsigned int warp_acc[16];
+    stage_tables(tab, a.tables, a.n_tab, a.tab_sl);
+    __syncthreads();
+    const uint64_t sweep = *a.sweep_base + a.sweep_offset;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const Tile tile = a.tiles[t];
+        const int r = tile.x;
+        const int k = tile.y >> 8, sl = tile.y & 0xff;
+        const ReplicaDev rep = a.reps[r];
+        const int L = rep.L, Nc = rep.Nc;
+        float4* S = a.spins + rep.off;
+        const int cell = tile.z + int(threadIdx.x);
+        bool accepted = false;
+        if (int(threadIdx.x) < tile.w) {
+            const int cx = cell % L, cy = (cell / L) % L, cz = cell / (L * L);
+            const size_t i = size_t(sl) * Nc + cell;
+            const float4 s0 = S[i];
+            float3 h = local_field(S, tab[k], cx, cy, cz, L, Nc);
+            h.x -= a.B[0];
+            h.y -= a.B[1];
+            h.z -= a.B[2];
+            if (MODE == kMetropolis) {
+                const double T = a.T_rep[r];
+                const float sigma = sqrtf(float(T) * a.inv_T_ref);
+                const float invT = float(1.0 / T);
+                const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
+                // Box-Muller on the top 24 bits of words (0,1) and (2,3)
+                const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
+                const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
+                float s_a, c_a, s_b, c_b;
+                sincospif(2.f * u24(w.y), &s_a, &c_a);
+                sincospif(2.f * u24(w.w), &s_b, &c_b);
+                float nx = s0.x + sigma * (r0 * c_a);
+                float ny = s0.y + sigma * (r0 * s_a);
+                float nz = s0.z + sigma * (r1 * c_b);
+                const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+                nx *= inv;
+                ny *= inv;
+                nz *= inv;
+                const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
+                if (dE < 0.f || u24_lowbytes(w) < __expf(-dE * invT)) {
+                    S[i] = make_float4(nx, ny, nz, 0.f);
+                    accepted = true;
+                }
+            } else {
+                const float n2 = h.x * h.x + h.y * h.y + h.z * h.z;
+                if (n2 > 1e-30f) {
+                    float nx, ny, nz;
+                    const float av = h.x * s0.x + h.y * s0.y + h.z * s0.z;
+                    if (MODE == kOverrelaxReflect) {
+                        // mirror_about_vector (src/MC.cpp:98-100)
+                        const float f = 2.f * av / (n2 + 1e-10f);
+                        nx = -s0.x + f * h.x;
+                        ny = -s0.y + f * h.y;
+                        nz = -s0.z + f * h.z;
+                    } else {
+                        // rotate_about_vector (src/MC.cpp:102-109), theta = 2*pi*U
+                        float sn, cs;
+                        if (MODE == kOverrelaxTheta) {
+                            sincosf(float(a.theta[i]), &sn, &cs);
+                        } else {
+                            const uint4 w =
+                                site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
+                            sincospif(2.f * u24(w.x), &sn, &cs);
+                        }
+                        const float f = (1.f - cs) * av / n2;
+                        const float g = sn * rsqrtf(n2);
+                        const float cx_ = h.y * s0.z - h.z * s0.y;
+                        const float cy_ = h.z * s0.x - h.x * s0.z;
+                        const float cz_ = h.x * s0.y - h.y * s0.x;
+                        nx = cs * s0.x + f * h.x + g * cx_;
+                        ny = cs * s0.y + f * h.y + g * cy_;
+                        nz = cs * s0.z + f * h.z + g * cz_;
+                    }
+                    // renormalise: keeps FP32 rounding from drifting |S| away from 1
+                    const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+                    S[i] = make_float4(nx * inv, ny * inv, nz * inv, 0.f);
+                }
+            }
+        }
+        if (MODE == kMetropolis) {
+            const unsigned int c = __popc(__ballot_sync(0xffffffffu, accepted));
+            if (lane == 0) warp_acc[warp] = c;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned int tot = 0;
+                for (int wi = 0; wi < int(blockDim.x >> 5); ++wi) tot += warp_acc[wi];
+                if (tot) atomicAdd(a.acc + r, (unsigned long long)tot);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st) {
+    switch (mode) {
+        case kMetropolis: colour_pass_kernel<kMetropolis><<<grid, threads, 0, st>>>(a); break;
+        case kOverrelaxRotate: colour_pass_kernel<kOverrelaxRotate><<<grid, threads, 0, st>>>(a); break;
+        case kOverrelaxReflect: colour_pass_kernel<kOverrelaxReflect><<<grid, threads, 0, st>>>(a); break;
+        case kOverrelaxTheta: colour_pass_kernel<kOverrelaxTheta><<<grid, threads, 0, st>>>(a); break;
+    }
+}
+
+// ------------------------------------------------------------- reductions
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of NV doubles; result valid in thread 0. `red` holds
+// NV * 32 doubles.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < NV; ++j) red[j * 32 + warp] = v[j];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double x = lane < nw ? red[j * 32 + lane] : 0.0;
+            v[j] = warp_sum(x);
+        }
+    }
+    __syncthreads();
+}
+
+// Energy terms per tile (total_energy_per_unit_cell, src/MC.cpp:305-312):
+// sum_i 0.5 S_i.h_i - S_i.B, plus sum_i S_i. Every sublattice of every
+// replica; tables staged per tile (one sublattice per tile).
+__global__ void __launch_bounds__(512) energy_partials_kernel(const EnergyArgs a) {
+    __shared__ SlTable tab;
+    __shared__ double red[4 * 32];
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const Tile tile = a.tiles[t];
+        const int r = tile.x, sl = tile.y & 0xff;
+        __syncthreads();
+        stage_tables(&tab, a.tables, 1, &sl);
+        __syncthreads();
+        const ReplicaDev rep = a.reps[r];
+        const int L = rep.L, Nc = rep.Nc;
+        const float4* S = a.spins + rep.off;
+        double v[4] = {0, 0, 0, 0};
+        if (int(threadIdx.x) < tile.w) {
+            const int cell = tile.z + int(threadIdx.x);
+            const int cx = cell % L, cy = (cell / L) % L, cz = cell / (L * L);
+            const float4 s0 = S[size_t(sl) * Nc + cell];
+            const float3 h = local_field(S, tab, cx, cy, cz, L, Nc);
+            v[0] = 0.5 * double(s0.x * h.x + s0.y * h.y + s0.z * h.z) -
+                   double(s0.x * a.B[0] + s0.y * a.B[1] + s0.z * a.B[2]);
+            v[1] = s0.x;
+            v[2] = s0.y;
+            v[3] = s0.z;
+        }
+        block_sum<4>(v, red);
+        if (threadIdx.x == 0)
+            for (int j = 0; j < 4; ++j) a.partial[size_t(t) * 4 + j] = v[j];
+    }
+}
+
+void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = a.n_tiles < sms * 4 ? a.n_tiles : sms * 4;
+    energy_partials_kernel<<<grid, threads, 0, st>>>(a);
+}
+
+// One warp per replica: fixed-order sum of its tile partials (deterministic).
+__global__ void energy_finalize_kernel(const double* partial, const int32_t* tb, const int32_t* te,
+                                       const ReplicaDev* reps, int R, double* e, double* mag) {
+    const int r = blockIdx.x;
+    if (r >= R) return;
+    const int lane = threadIdx.x;
+    double v[4] = {0, 0, 0, 0};
+    for (int t = tb[r] + lane; t < te[r]; t += 32)
+        for (int j = 0; j < 4; ++j) v[j] += partial[size_t(t) * 4 + j];
+    for (int j = 0; j < 4; ++j) v[j] = warp_sum(v[j]);
+    if (lane == 0) {
+        e[r] = v[0] / double(reps[r].Nc);
+        if (mag)
+            for (int j = 0; j < 3; ++j) mag[3 * r + j] = v[1 + j];
+    }
+}
+
+void launch_energy_finalize(const double* partial, const int32_t* tile_begin, const int32_t* tile_end,
+                            const ReplicaDev* reps, int R, double* e, double* mag, cudaStream_t st) {
+    energy_finalize_kernel<<<R, 32, 0, st>>>(partial, tile_begin, tile_end, reps, R, e, mag);
+}
+
+__global__ void __launch_bounds__(512) local_field_kernel(const FieldArgs a) {
+    __shared__ SlTable tab;
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const Tile tile = a.tiles[t];
+        const int r = tile.x, sl = tile.y & 0xff;
+        __syncthreads();
+        stage_tables(&tab, a.tables, 1, &sl);
+        __syncthreads();
+        const ReplicaDev rep = a.reps[r];
+        if (int(threadIdx.x) < tile.w) {
+            const int L = rep.L, Nc = rep.Nc;
+            const int cell = tile.z + int(threadIdx.x);
+            const int cx = cell % L, cy = (cell / L) % L, cz = cell / (L * L);
+            const float3 h = local_field(a.spins + rep.off, tab, cx, cy, cz, L, Nc);
+            a.h_out[rep.off + size_t(sl) * Nc + cell] = make_float4(h.x, h.y, h.z, 0.f);
+        }
+    }
+}
+
+void launch_local_field(const FieldArgs& a, int threads, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = a.n_tiles < sms * 4 ? a.n_tiles : sms * 4;
+    local_field_kernel<<<grid, threads, 0, st>>>(a);
+}
+
+// Energy gradient. Per site: grad_S = g/Nc (h - B). Per shell (spec c, J or
+// J^T side): 0.5 S_i (x) t (source side) or 0.5 t (x) S_i (target side), with
+// t the shell's neighbour sum; over all sites this is sum over the spec's bonds
+// of S_src (x) S_tgt = dE/dJ_spec. Partial layout per tile:
+// [0] energy sum, [1..3] sum S, [4 + 9c + 3a + b] dE/dJ_c[a][b].
+__global__ void __launch_bounds__(256) energy_grad_kernel(const GradArgs a) {
+    __shared__ SlTable tab;
+    extern __shared__ double acc[];  // [4 + 9*n_spec]
+    const int width = 4 + 9 * a.n_spec;
+    const int lane = threadIdx.x & 31;
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const Tile tile = a.tiles[t];
+        const int r = tile.x, sl = tile.y & 0xff;
+        __syncthreads();
+        stage_tables(&tab, a.tables, 1, &sl);
+        for (int j = threadIdx.x; j < width; j += blockDim.x) acc[j] = 0.0;
+        __syncthreads();
+        const ReplicaDev rep = a.reps[r];
+        const int L = rep.L, Nc = rep.Nc;
+        const float4* S = a.spins + rep.off;
+        const bool live = int(threadIdx.x) < tile.w;
+        const int cell = tile.z + int(threadIdx.x);
+        const int cx = cell % L, cy = (cell / L) % L, cz = cell / (L * L);
+        float4 s0 = make_float4(0, 0, 0, 0);
+        if (live) s0 = S[size_t(sl) * Nc + cell];
+        float hx = 0.f, hy = 0.f, hz = 0.f;
+        int e = 0;
+        for (int k = 0; k < tab.n_shell; ++k) {
+            float tx = 0.f, ty = 0.f, tz = 0.f;
+            const int end = tab.shell_end[k];
+            for (; e < end; ++e) {
+                if (!live) continue;
+                const NbEntry nb = tab.nb[e];
+                const int x = wrap1(cx + nb.dx, L), y = wrap1(cy + nb.dy, L), z = wrap1(cz + nb.dz, L);
+                const float4 o = __ldg(&S[size_t(nb.sl) * Nc + x + L * (y + L * z)]);
+                tx += o.x;
+                ty += o.y;
+                tz += o.z;
+            }
+            const float* J = tab.J[k];
+            hx += J[0] * tx + J[1] * ty + J[2] * tz;
+            hy += J[3] * tx + J[4] * ty + J[5] * tz;
+            hz += J[6] * tx + J[7] * ty + J[8] * tz;
+            const int spec = tab.shell_spec[k] % 1000;
+            const bool tr = tab.shell_spec[k] >= 1000;
+            const float sv[3] = {s0.x, s0.y, s0.z};
+            const float tv[3] = {tx, ty, tz};
+#pragma unroll
+            for (int p = 0; p < 3; ++p)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    double v = 0.5 * double(tr ? tv[p] * sv[q] : sv[p] * tv[q]);
+                    v = warp_sum(v);
+                    if (lane == 0) atomicAdd(&acc[4 + 9 * spec + 3 * p + q], v);
+                }
+        }
+        double ev = 0.0;
+        if (live) {
+            ev = 0.5 * double(s0.x * hx + s0.y * hy + s0.z * hz) -
+                 double(s0.x * a.B[0] + s0.y * a.B[1] + s0.z * a.B[2]);
+            if (a.grad_S) {
+                const float gs = float(a.g[r] / double(Nc));
+                a.grad_S[rep.off + size_t(sl) * Nc + cell] =
+                    make_float4(gs * (hx - a.B[0]), gs * (hy - a.B[1]), gs * (hz - a.B[2]), 0.f);
+            }
+        }
+        const double v4[4] = {ev, s0.x, s0.y, s0.z};
+        for (int j = 0; j < 4; ++j) {
+            const double v = warp_sum(v4[j]);
+            if (lane == 0) atomicAdd(&acc[j], v);
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < width; j += blockDim.x) a.partial[size_t(t) * width + j] = acc[j];
+    }
+}
+
+void launch_energy_grad_partials(const GradArgs& a, int threads, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = a.n_tiles < sms * 4 ? a.n_tiles : sms * 4;
+    const size_t smem = sizeof(double) * size_t(4 + 9 * a.n_spec);
+    energy_grad_kernel<<<grid, threads, smem, st>>>(a);
+}
+
+__global__ void grad_finalize_kernel(const double* partial, int width, const int32_t* tb, const int32_t* te, int R,
+                                     double* out) {
+    const int r = blockIdx.x;
+    for (int j = threadIdx.x; j < width; j += blockDim.x) {
+        double v = 0.0;
+        for (int t = tb[r]; t < te[r]; ++t) v += partial[size_t(t) * width + j];
+        out[size_t(r) * width + j] = v;
+    }
+}
+
+void launch_grad_finalize(const double* partial, int width, const int32_t* tile_begin, const int32_t* tile_end, int R,
+                          double* out, cudaStream_t st) {
+    grad_finalize_kernel<<<R, 128, 0, st>>>(partial, width, tile_begin, tile_end, R, out);
+}
+
+// Uniform on S^2: z = 1 - 2u, phi = 2 pi u'.
+__global__ void random_spins_kernel(float4* spins, const ReplicaDev* reps, const Tile* tiles, int n_tiles,
+                                    uint64_t seed) {
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const Tile tile = tiles[t];
+        if (int(threadIdx.x) >= tile.w) continue;
+        const int r = tile.x, sl = tile.y & 0xff;
+        const ReplicaDev rep = reps[r];
+        const size_t i = size_t(sl) * rep.Nc + tile.z + threadIdx.x;
+        const uint4 w = site_draw(seed, uint32_t(r), 0, kDrawInit, uint32_t(i));
+        const float z = 1.f - 2.f * u24(w.x);
+        float sn, cs;
+        sincospif(2.f * u24(w.y), &sn, &cs);
+        const float rho = sqrtf(fmaxf(0.f, 1.f - z * z));
+        spins[rep.off + i] = make_float4(rho * cs, rho * sn, z, 0.f);
+    }
+}
+
+void launch_random_spins(float4* spins, const ReplicaDev* reps, const Tile* tiles, int n_tiles, uint64_t seed,
+                         int threads, cudaStream_t st) {
+    const int grid = n_tiles < 4096 ? n_tiles : 4096;
+    random_spins_kernel<<<grid, threads, 0, st>>>(spins, reps, tiles, n_tiles, seed);
+}
+
+__global__ void advance_counter_kernel(uint64_t* c, uint64_t n) { *c += n; }
+void launch_advance_counter(uint64_t* counter, uint64_t n, cudaStream_t st) {
+    advance_counter_kernel<<<1, 1, 0, st>>>(counter, n);
+}
+
+}  // namespace pc

@@ -1,0 +1,1647 @@
+// system.cu -- host side of libpyrocmc.so: the C ABI of include/pyrocmc.h.
+//
+// Owns the device state of a batch of replicas (spins, bond tables, colour
+// tiles, SSF and tempering accumulators), builds the structured bond tables
+// from reference-style coupling specs (MC_runner::setup_lattice,
+// src/MC.cpp:15-52) and launches the kernels of sweep.cu / ssf.cu / pt.cu on
+// the system's stream, replaying captured CUDA graphs for the sweep schedule.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pyrocmc.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using pc::NbEntry;
+using pc::ReplicaDev;
+using pc::SlTable;
+using pc::Tile;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define PC_CK(expr)                                                                                   \
+    do {                                                                                              \
+        cudaError_t e_ = (expr);                                                                      \
+        if (e_ != cudaSuccess) return fail(PC_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define PC_LAUNCH_CK()                                                                                \
+    do {                                                                                              \
+        cudaError_t e_ = cudaGetLastError();                                                          \
+        if (e_ != cudaSuccess) return fail(PC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Geometry of the 16-site cubic cell (include/pyrochlore_geometry.hpp:12-32).
+const int64_t kLink[4][3] = {{1, 1, 1}, {1, -1, -1}, {-1, 1, -1}, {-1, -1, 1}};
+const int64_t kFcc[4][3] = {{0, 0, 0}, {0, 4, 4}, {4, 0, 4}, {4, 4, 0}};
+
+int64_t pmod(int64_t a, int64_t m) {
+    int64_t r = a % m;
+    return r < 0 ? r + m : r;
+}
+std::array<int64_t, 3> r_sl(int sl) {
+    const int f = sl / 4, p = sl % 4;
+    return {kLink[p][0] + kFcc[f][0], kLink[p][1] + kFcc[f][1], kLink[p][2] + kFcc[f][2]};
+}
+// Sublattice of a position (any integer coordinates), -1 if no site.
+int sl_at(const std::array<int64_t, 3>& x) {
+    for (int sl = 0; sl < 16; ++sl) {
+        const auto r = r_sl(sl);
+        if (pmod(x[0] - r[0], 8) == 0 && pmod(x[1] - r[1], 8) == 0 && pmod(x[2] - r[2], 8) == 0) return sl;
+    }
+    return -1;
+}
+
+struct Coupling {
+    std::string name;
+    std::vector<std::array<int64_t, 3>> rel[4];
+    double J[9];
+    double Jt[9];
+};
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(&p, count * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct SsfGroup {
+    int L, P, Q;
+    std::vector<int> reps;
+    DevBuf<int32_t> d_rep_index;  // all replicas of this size
+    DevBuf<int32_t> d_sel_index;  // the replicas selected by the last sample call (capacity reps)
+    int n_sel = 0;
+    DevBuf<float2> d_G;           // stage-1 planes / adjoint scratch
+    DevBuf<float2> d_amp;         // amplitudes B^a(K) for the backward
+};
+
+void split_PQ(int L, int* P, int* Q) {
+    int best = 1;
+    for (int p = 1; p * p <= L; ++p)
+        if (L % p == 0) best = p;
+    *P = best;
+    *Q = L / best;
+}
+
+}  // namespace
+
+struct pc_system {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+
+    int R = 0;
+    std::vector<int> L;
+    std::vector<int64_t> off;
+    int64_t N_tot = 0;
+    uint64_t seed = 0;
+    double T_ref = 1.0;
+    double B[3] = {0, 0, 0};
+    int or_mode = 0;
+    int colouring = 0;
+    std::vector<Coupling> specs;
+    bool ready = false;
+
+    SlTable tab_active[16];
+    SlTable tab_full[16];
+    int n_colours = 0;
+    int colour_of_sl[16];
+    std::vector<std::vector<int>> colour_sls;
+
+    int threads = 256;
+    int ctas_per_sm = 4;
+
+    DevBuf<ReplicaDev> d_reps;
+    DevBuf<float4> d_spins;
+    DevBuf<double> d_T;
+    DevBuf<uint64_t> d_sweep;
+    DevBuf<unsigned long long> d_acc;
+    DevBuf<SlTable> d_tab_active, d_tab_full;
+    std::vector<DevBuf<Tile>> d_colour_tiles;
+    std::vector<int> n_colour_tiles;
+    DevBuf<Tile> d_all_tiles;
+    int n_all_tiles = 0;
+    std::vector<int32_t> tile_begin, tile_end;
+    DevBuf<int32_t> d_tile_begin, d_tile_end;
+    DevBuf<double> d_partial;
+    DevBuf<double> d_e, d_mag;
+    DevBuf<double> d_theta;
+    DevBuf<float4> d_field;
+
+    uint64_t host_sweep = 0;
+    uint64_t launches = 0;
+
+    // sweep graph cache, keyed by n_overrelax
+    std::map<int, std::pair<cudaGraphExec_t, int>> sweep_graphs;
+
+    // kernel timing
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    std::vector<int> ev_kind;  // 0 Metropolis, 1 overrelaxation
+    size_t ev_used = 0;
+
+    // SSF
+    bool ssf_ready = false;
+    int n_corr = 0;
+    int corr_a[9], corr_b[9];
+    int n_slots = 0;
+    std::vector<int> L_of_slot;
+    int64_t slot_stride = 0;
+    DevBuf<double> d_ssf_sum, d_ssf_sq;
+    std::vector<uint64_t> ssf_n;
+    std::vector<SsfGroup> groups;
+    DevBuf<int32_t> d_slot_of_rep;
+
+    // tempering
+    bool pt_ready = false;
+    int n_ladders = 0;
+    std::vector<int32_t> ladder_begin;
+    std::vector<double> T_slot;
+    DevBuf<int32_t> d_ladder_begin, d_rep_of_slot, d_pt_slot_of_rep;
+    DevBuf<double> d_T_slot, d_E_sum, d_E2_sum;
+    DevBuf<unsigned long long> d_n_e, d_att, d_accn;
+    DevBuf<uint64_t> d_round;
+    std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> pt_graphs;  // (n_sweep, phase)
+    uint64_t pt_sweeps_done = 0;
+
+    ~pc_system() {
+        for (auto& g : sweep_graphs) cudaGraphExecDestroy(g.second.first);
+        for (auto& g : pt_graphs) cudaGraphExecDestroy(g.second.first);
+        for (auto& e : ev_pool) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        if (stream && own_stream) cudaStreamDestroy(stream);
+        d_reps.release();
+        d_spins.release();
+        d_T.release();
+        d_sweep.release();
+        d_acc.release();
+        d_tab_active.release();
+        d_tab_full.release();
+        for (auto& t : d_colour_tiles) t.release();
+        d_all_tiles.release();
+        d_tile_begin.release();
+        d_tile_end.release();
+        d_partial.release();
+        d_e.release();
+        d_mag.release();
+        d_theta.release();
+        d_field.release();
+        d_ssf_sum.release();
+        d_ssf_sq.release();
+        for (auto& g : groups) {
+            g.d_rep_index.release();
+            g.d_sel_index.release();
+            g.d_G.release();
+            g.d_amp.release();
+        }
+        d_slot_of_rep.release();
+        d_ladder_begin.release();
+        d_rep_of_slot.release();
+        d_pt_slot_of_rep.release();
+        d_T_slot.release();
+        d_E_sum.release();
+        d_E2_sum.release();
+        d_n_e.release();
+        d_att.release();
+        d_accn.release();
+        d_round.release();
+    }
+
+    int64_t Nc(int r) const { return int64_t(L[size_t(r)]) * L[size_t(r)] * L[size_t(r)]; }
+    int64_t N(int r) const { return 16 * Nc(r); }
+
+    void drop_graphs() {
+        for (auto& g : sweep_graphs) cudaGraphExecDestroy(g.second.first);
+        sweep_graphs.clear();
+        for (auto& g : pt_graphs) cudaGraphExecDestroy(g.second.first);
+        pt_graphs.clear();
+    }
+};
+
+namespace {
+
+int check_sys(pc_system* s, bool need_ready = true) {
+    if (!s) return fail(PC_ERR_INVALID, "null system");
+    if (need_ready && !s->ready) return fail(PC_ERR_STATE, "setup_lattice() has not been called");
+    return PC_OK;
+}
+int check_rep(pc_system* s, int r) {
+    if (r < 0 || r >= s->R) return fail(PC_ERR_INVALID, "replica index out of range");
+    return PC_OK;
+}
+
+// Builds the structured shells of every sublattice for one table kind:
+// identical to setup_lattice's split (src/MC.cpp:28-50): for each spec, the
+// neighbours where this site's pyro_sl <= the other's form a shell applying J,
+// the rest a shell applying J^T. keep_zero=false drops shells whose matrix is
+// all zero (they contribute exactly nothing to the field).
+int build_tables(pc_system* s, bool keep_zero, SlTable* out) {
+    for (int sl = 0; sl < 16; ++sl) {
+        SlTable& t = out[sl];
+        std::memset(&t, 0, sizeof(t));
+        const int p = sl % 4;
+        const auto r = r_sl(sl);
+        for (size_t c = 0; c < s->specs.size(); ++c) {
+            const Coupling& cp = s->specs[c];
+            std::vector<NbEntry> side[2];
+            for (const auto& v : cp.rel[p]) {
+                const std::array<int64_t, 3> x = {r[0] + v[0], r[1] + v[1], r[2] + v[2]};
+                const int sl2 = sl_at(x);
+                if (sl2 < 0) return fail(PC_ERR_INVALID, "coupling " + cp.name + ": displacement does not land on a site");
+                const auto r2 = r_sl(sl2);
+                NbEntry e;
+                int64_t d[3];
+                for (int a = 0; a < 3; ++a) {
+                    d[a] = (x[a] - r2[a]) / 8;
+                    if (d[a] < -1 || d[a] > 1)
+                        return fail(PC_ERR_UNSUPPORTED, "coupling " + cp.name + ": reaches beyond the adjacent cubic cell");
+                }
+                e.dx = int8_t(d[0]);
+                e.dy = int8_t(d[1]);
+                e.dz = int8_t(d[2]);
+                e.sl = uint8_t(sl2);
+                side[(p <= sl2 % 4) ? 0 : 1].push_back(e);
+            }
+            for (int k = 0; k < 2; ++k) {
+                if (side[k].empty()) continue;
+                const double* M = k == 0 ? cp.J : cp.Jt;
+                bool zero = true;
+                for (int i = 0; i < 9; ++i) zero = zero && (M[i] == 0.0);
+                if (zero && !keep_zero) continue;
+                if (t.n_shell >= pc::kMaxShell || t.n_nb + int(side[k].size()) > pc::kMaxNb)
+                    return fail(PC_ERR_UNSUPPORTED, "too many bond shells or neighbours per sublattice");
+                for (const auto& e : side[k]) t.nb[t.n_nb++] = e;
+                t.shell_end[t.n_shell] = t.n_nb;
+                t.shell_spec[t.n_shell] = int(c) + (k == 1 ? 1000 : 0);
+                for (int i = 0; i < 9; ++i) t.J[t.n_shell][i] = float(M[i]);
+                t.n_shell++;
+            }
+        }
+    }
+    return PC_OK;
+}
+
+// Colour classes from the active bonds: sublattices joined by a nonzero bond
+// never share a class. Greedy in sublattice order, at most 4 sublattices per
+// class. With J1/J2 only this yields the 4 pyro_sl classes; J3 (which joins
+// equal pyro_sl) refines them to the 16 conventional sublattices.
+int build_colours(pc_system* s) {
+    bool conflict[16][16] = {};
+    for (int sl = 0; sl < 16; ++sl)
+        for (int e = 0; e < s->tab_active[sl].n_nb; ++e) {
+            const int o = s->tab_active[sl].nb[e].sl;
+            conflict[sl][o] = conflict[o][sl] = true;
+        }
+    for (int sl = 0; sl < 16; ++sl)
+        if (conflict[sl][sl])
+            return fail(PC_ERR_UNSUPPORTED, "a coupling joins a sublattice to itself; sublattice colouring is not valid");
+    s->colour_sls.clear();
+    if (s->colouring == 0) {
+        for (int sl = 0; sl < 16; ++sl) {
+            s->colour_sls.push_back({sl});
+            s->colour_of_sl[sl] = sl;
+        }
+        s->n_colours = 16;
+        return PC_OK;
+    }
+    for (int sl = 0; sl < 16; ++sl) {
+        int c = 0;
+        for (; c < int(s->colour_sls.size()); ++c) {
+            bool ok = s->colour_sls[size_t(c)].size() < 4;
+            for (int o : s->colour_sls[size_t(c)]) ok = ok && !conflict[sl][o];
+            if (ok) break;
+        }
+        if (c == int(s->colour_sls.size())) s->colour_sls.emplace_back();
+        s->colour_sls[size_t(c)].push_back(sl);
+        s->colour_of_sl[sl] = c;
+    }
+    s->n_colours = int(s->colour_sls.size());
+    return PC_OK;
+}
+
+int build_tiles(pc_system* s) {
+    const int T = s->threads;
+    for (auto& t : s->d_colour_tiles) t.release();
+    s->d_colour_tiles.clear();
+    s->n_colour_tiles.clear();
+    s->d_colour_tiles.resize(size_t(s->n_colours));
+    for (int c = 0; c < s->n_colours; ++c) {
+        std::vector<Tile> tiles;
+        const auto& sls = s->colour_sls[size_t(c)];
+        for (int r = 0; r < s->R; ++r)
+            for (size_t k = 0; k < sls.size(); ++k)
+                for (int64_t c0 = 0; c0 < s->Nc(r); c0 += T)
+                    tiles.push_back(make_int4(r, int(k << 8) | sls[k], int(c0), int(std::min<int64_t>(T, s->Nc(r) - c0))));
+        PC_CK(s->d_colour_tiles[size_t(c)].alloc(tiles.size()));
+        PC_CK(cudaMemcpy(s->d_colour_tiles[size_t(c)].p, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+        s->n_colour_tiles.push_back(int(tiles.size()));
+    }
+    std::vector<Tile> all;
+    s->tile_begin.assign(size_t(s->R), 0);
+    s->tile_end.assign(size_t(s->R), 0);
+    for (int r = 0; r < s->R; ++r) {
+        s->tile_begin[size_t(r)] = int(all.size());
+        for (int sl = 0; sl < 16; ++sl)
+            for (int64_t c0 = 0; c0 < s->Nc(r); c0 += T)
+                all.push_back(make_int4(r, sl, int(c0), int(std::min<int64_t>(T, s->Nc(r) - c0))));
+        s->tile_end[size_t(r)] = int(all.size());
+    }
+    s->n_all_tiles = int(all.size());
+    PC_CK(s->d_all_tiles.alloc(all.size()));
+    PC_CK(cudaMemcpy(s->d_all_tiles.p, all.data(), all.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    PC_CK(s->d_tile_begin.alloc(size_t(s->R)));
+    PC_CK(s->d_tile_end.alloc(size_t(s->R)));
+    PC_CK(cudaMemcpy(s->d_tile_begin.p, s->tile_begin.data(), sizeof(int32_t) * size_t(s->R), cudaMemcpyHostToDevice));
+    PC_CK(cudaMemcpy(s->d_tile_end.p, s->tile_end.data(), sizeof(int32_t) * size_t(s->R), cudaMemcpyHostToDevice));
+    // partial sums: energy (4 per tile) and gradient (4 + 9*n_spec per tile)
+    const size_t width = size_t(4 + 9 * std::max<size_t>(1, s->specs.size()));
+    PC_CK(s->d_partial.alloc(size_t(s->n_all_tiles) * width));
+    s->drop_graphs();
+    return PC_OK;
+}
+
+pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_pass) {
+    pc::PassArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.spins = s->d_spins.p;
+    a.reps = s->d_reps.p;
+    a.T_rep = s->d_T.p;
+    a.sweep_base = s->d_sweep.p;
+    a.sweep_offset = sweep_offset;
+    a.seed = s->seed;
+    a.inv_T_ref = float(1.0 / s->T_ref);
+    for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
+    a.tables = s->d_tab_active.p;
+    const auto& sls = s->colour_sls[size_t(colour)];
+    a.n_tab = int(sls.size());
+    for (size_t k = 0; k < sls.size(); ++k) a.tab_sl[k] = sls[k];
+    a.tiles = s->d_colour_tiles[size_t(colour)].p;
+    a.n_tiles = s->n_colour_tiles[size_t(colour)];
+    a.acc = s->d_acc.p;
+    a.or_pass = or_pass;
+    return a;
+}
+
+int grid_for(pc_system* s, int n_tiles) { return std::max(1, std::min(n_tiles, s->sms * s->ctas_per_sm)); }
+
+// Launches one sweep's passes (sweep offset `off` relative to *d_sweep).
+int enqueue_sweep(pc_system* s, uint64_t off, int n_or, bool record_events) {
+    auto record = [&](int kind, bool start) -> int {
+        if (!record_events) return PC_OK;
+        if (start) {
+            if (s->ev_used == s->ev_pool.size()) {
+                cudaEvent_t a, b;
+                PC_CK(cudaEventCreate(&a));
+                PC_CK(cudaEventCreate(&b));
+                s->ev_pool.push_back({a, b});
+                s->ev_kind.push_back(kind);
+            }
+            s->ev_kind[s->ev_used] = kind;
+            PC_CK(cudaEventRecord(s->ev_pool[s->ev_used].first, s->stream));
+        } else {
+            PC_CK(cudaEventRecord(s->ev_pool[s->ev_used].second, s->stream));
+            s->ev_used++;
+        }
+        return PC_OK;
+    };
+    for (int c = 0; c < s->n_colours; ++c) {
+        const pc::PassArgs a = pass_args(s, c, off, 0);
+        int rc = record(0, true);
+        if (rc) return rc;
+        pc::launch_colour_pass(pc::kMetropolis, a, grid_for(s, a.n_tiles), s->threads, s->stream);
+        PC_LAUNCH_CK();
+        rc = record(0, false);
+        if (rc) return rc;
+        s->launches++;
+    }
+    const pc::PassMode om = s->or_mode == 1 ? pc::kOverrelaxReflect : pc::kOverrelaxRotate;
+    for (int k = 0; k < n_or; ++k)
+        for (int c = 0; c < s->n_colours; ++c) {
+            const pc::PassArgs a = pass_args(s, c, off, k);
+            int rc = record(1, true);
+            if (rc) return rc;
+            pc::launch_colour_pass(om, a, grid_for(s, a.n_tiles), s->threads, s->stream);
+            PC_LAUNCH_CK();
+            rc = record(1, false);
+            if (rc) return rc;
+            s->launches++;
+        }
+    return PC_OK;
+}
+
+// A captured graph of one sweep plus the counter advance; nodes = kernels.
+int sweep_graph(pc_system* s, int n_or, cudaGraphExec_t* exec, int* nodes) {
+    auto it = s->sweep_graphs.find(n_or);
+    if (it != s->sweep_graphs.end()) {
+        *exec = it->second.first;
+        *nodes = it->second.second;
+        return PC_OK;
+    }
+    const uint64_t before = s->launches;
+    PC_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_sweep(s, 0, n_or, false);
+    pc::launch_advance_counter(s->d_sweep.p, 1, s->stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(PC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t x = nullptr;
+    PC_CK(cudaGraphInstantiate(&x, g, 0));
+    cudaGraphDestroy(g);
+    const int n = int(s->launches - before) + 1;
+    s->launches = before;  // capture launched nothing
+    s->sweep_graphs[n_or] = {x, n};
+    *exec = x;
+    *nodes = n;
+    return PC_OK;
+}
+
+int run_sweeps(pc_system* s, int n_sweeps, int n_or) {
+    if (s->timing) {
+        for (int i = 0; i < n_sweeps; ++i) {
+            int rc = enqueue_sweep(s, uint64_t(i), n_or, true);
+            if (rc) return rc;
+        }
+        pc::launch_advance_counter(s->d_sweep.p, uint64_t(n_sweeps), s->stream);
+        PC_LAUNCH_CK();
+        s->launches++;
+    } else {
+        cudaGraphExec_t g;
+        int nodes;
+        int rc = sweep_graph(s, n_or, &g, &nodes);
+        if (rc) return rc;
+        for (int i = 0; i < n_sweeps; ++i) {
+            PC_CK(cudaGraphLaunch(g, s->stream));
+            s->launches += uint64_t(nodes);
+        }
+    }
+    s->host_sweep += uint64_t(n_sweeps);
+    return PC_OK;
+}
+
+int enqueue_energy(pc_system* s) {
+    pc::EnergyArgs a;
+    a.spins = s->d_spins.p;
+    a.reps = s->d_reps.p;
+    a.tables = s->d_tab_active.p;
+    a.tiles = s->d_all_tiles.p;
+    a.n_tiles = s->n_all_tiles;
+    for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
+    a.partial = s->d_partial.p;
+    pc::launch_energy_partials(a, s->threads, s->stream);
+    PC_LAUNCH_CK();
+    pc::launch_energy_finalize(s->d_partial.p, s->d_tile_begin.p, s->d_tile_end.p, s->d_reps.p, s->R, s->d_e.p,
+                               s->d_mag.p, s->stream);
+    PC_LAUNCH_CK();
+    s->launches += 2;
+    return PC_OK;
+}
+
+int enqueue_ssf(pc_system* s, const pc::SsfOut& o, bool selected_only) {
+    for (auto& g : s->groups) {
+        pc::SsfGeom geom;
+        geom.L = g.L;
+        geom.P = g.P;
+        geom.Q = g.Q;
+        if (selected_only) {
+            if (g.n_sel == 0) continue;
+            geom.n_rep = g.n_sel;
+            geom.rep_index = g.d_sel_index.p;
+        } else {
+            geom.n_rep = int(g.reps.size());
+            geom.rep_index = g.d_rep_index.p;
+        }
+        pc::launch_ssf_xy(geom, s->d_spins.p, s->d_reps.p, g.d_G.p, s->stream);
+        PC_LAUNCH_CK();
+        pc::launch_ssf_z(geom, g.d_G.p, o, s->stream);
+        PC_LAUNCH_CK();
+        s->launches += 2;
+    }
+    return PC_OK;
+}
+
+pc::SsfOut ssf_out_base(pc_system* s) {
+    pc::SsfOut o;
+    std::memset(&o, 0, sizeof(o));
+    o.n_corr = s->n_corr;
+    for (int c = 0; c < s->n_corr; ++c) {
+        o.corr_a[c] = s->corr_a[c];
+        o.corr_b[c] = s->corr_b[c];
+    }
+    o.slot_stride = s->slot_stride;
+    return o;
+}
+
+int ensure_groups(pc_system* s) {
+    if (!s->groups.empty()) return PC_OK;
+    std::map<int, std::vector<int>> by_L;
+    for (int r = 0; r < s->R; ++r) by_L[s->L[size_t(r)]].push_back(r);
+    for (auto& kv : by_L) {
+        SsfGroup g;
+        g.L = kv.first;
+        split_PQ(g.L, &g.P, &g.Q);
+        if (9 * g.L + 3 * g.L * g.L > 200 * 1024 / 8)
+            return fail(PC_ERR_UNSUPPORTED, "SSF supports L up to 90 (one z plane per CTA in shared memory)");
+        g.reps = kv.second;
+        s->groups.push_back(std::move(g));
+    }
+    pc::ssf_prepare();
+    for (auto& g : s->groups) {
+        PC_CK(g.d_sel_index.alloc(g.reps.size()));
+        PC_CK(g.d_rep_index.alloc(g.reps.size()));
+        PC_CK(cudaMemcpy(g.d_rep_index.p, g.reps.data(), sizeof(int32_t) * g.reps.size(), cudaMemcpyHostToDevice));
+        const size_t L3 = size_t(g.L) * g.L * g.L;
+        PC_CK(g.d_G.alloc(g.reps.size() * 12 * L3));
+    }
+    return PC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pc_last_error(void) { return g_last_error.c_str(); }
+int pc_version(void) { return 100; }
+
+int pc_create(int n_replicas, const int32_t* L, uint64_t seed, pc_system** out) {
+    if (!out) return fail(PC_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    if (n_replicas <= 0 || !L) return fail(PC_ERR_INVALID, "need at least one replica");
+    for (int r = 0; r < n_replicas; ++r)
+        if (L[r] < 1 || L[r] > 1024) return fail(PC_ERR_INVALID, "L must be in [1, 1024]");
+    auto* s = new pc_system();
+    s->R = n_replicas;
+    s->seed = seed;
+    s->L.assign(L, L + n_replicas);
+    s->off.resize(size_t(n_replicas));
+    int64_t o = 0;
+    for (int r = 0; r < n_replicas; ++r) {
+        s->off[size_t(r)] = o;
+        o += s->N(r);
+    }
+    s->N_tot = o;
+    cudaError_t e = cudaGetDevice(&s->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    std::vector<ReplicaDev> reps(static_cast<size_t>(n_replicas));
+    for (int r = 0; r < n_replicas; ++r) reps[size_t(r)] = {L[r], int32_t(s->Nc(r)), s->off[size_t(r)]};
+    if (e == cudaSuccess) e = s->d_reps.alloc(size_t(n_replicas));
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_reps.p, reps.data(), sizeof(ReplicaDev) * reps.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = s->d_spins.alloc(size_t(s->N_tot));
+    if (e == cudaSuccess) e = cudaMemset(s->d_spins.p, 0, sizeof(float4) * size_t(s->N_tot));
+    if (e == cudaSuccess) e = s->d_T.alloc(size_t(n_replicas));
+    if (e == cudaSuccess) e = s->d_sweep.alloc(1);
+    if (e == cudaSuccess) e = cudaMemset(s->d_sweep.p, 0, sizeof(uint64_t));
+    if (e == cudaSuccess) e = s->d_acc.alloc(size_t(n_replicas));
+    if (e == cudaSuccess) e = s->d_e.alloc(size_t(n_replicas));
+    if (e == cudaSuccess) e = s->d_mag.alloc(size_t(3 * n_replicas));
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(PC_ERR_CUDA, std::string("pc_create: ") + cudaGetErrorString(e));
+    }
+    *out = s;
+    return PC_OK;
+}
+
+int pc_destroy(pc_system* sys) {
+    if (!sys) return PC_OK;
+    if (sys->stream) cudaStreamSynchronize(sys->stream);
+    delete sys;
+    return PC_OK;
+}
+
+int pc_set_stream(pc_system* sys, void* stream) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (stream == nullptr || stream == cudaStreamLegacy || stream == cudaStreamPerThread)
+        return fail(PC_ERR_INVALID, "pc_set_stream needs a created stream (the default stream cannot be captured)");
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    if (sys->own_stream) cudaStreamDestroy(sys->stream);
+    sys->stream = static_cast<cudaStream_t>(stream);
+    sys->own_stream = false;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_define_coupling(pc_system* sys, const char* name, const int64_t* rel_vecs, const int32_t* n_rel, const double* J) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (!name || !n_rel || !J) return fail(PC_ERR_INVALID, "null argument");
+    for (const auto& c : sys->specs)
+        if (c.name == name) return fail(PC_ERR_INVALID, "Coupling names must be unique");
+    if (sys->ready) return fail(PC_ERR_STATE, "couplings must be defined before setup_lattice()");
+    Coupling c;
+    c.name = name;
+    size_t k = 0;
+    for (int p = 0; p < 4; ++p) {
+        if (n_rel[p] < 0) return fail(PC_ERR_INVALID, "negative displacement count");
+        for (int j = 0; j < n_rel[p]; ++j, ++k)
+            c.rel[p].push_back({rel_vecs[3 * k], rel_vecs[3 * k + 1], rel_vecs[3 * k + 2]});
+    }
+    for (int i = 0; i < 9; ++i) c.J[i] = J[i];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) c.Jt[3 * a + b] = J[3 * b + a];
+    sys->specs.push_back(std::move(c));
+    return PC_OK;
+}
+
+int pc_set_coupling_matrix(pc_system* sys, int spec, const double* J) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (spec < 0 || spec >= int(sys->specs.size())) return fail(PC_ERR_INVALID, "spec index out of range");
+    Coupling& c = sys->specs[size_t(spec)];
+    for (int i = 0; i < 9; ++i) c.J[i] = J[i];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) c.Jt[3 * a + b] = J[3 * b + a];
+    rc = build_tables(sys, false, sys->tab_active);
+    if (rc) return rc;
+    rc = build_tables(sys, true, sys->tab_full);
+    if (rc) return rc;
+    const int old_colours = sys->n_colours;
+    rc = build_colours(sys);
+    if (rc) return rc;
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    PC_CK(cudaMemcpy(sys->d_tab_active.p, sys->tab_active, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
+    PC_CK(cudaMemcpy(sys->d_tab_full.p, sys->tab_full, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
+    if (sys->colouring != 0 || old_colours != sys->n_colours) return build_tiles(sys);
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_set_global_field(pc_system* sys, const double* B3) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    for (int i = 0; i < 3; ++i) sys->B[i] = B3[i];
+    sys->drop_graphs();
+    return PC_OK;
+}
+int pc_get_global_field(pc_system* sys, double* B3) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    for (int i = 0; i < 3; ++i) B3[i] = sys->B[i];
+    return PC_OK;
+}
+int pc_set_T_ref(pc_system* sys, double T_ref) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (!(T_ref > 0)) return fail(PC_ERR_INVALID, "T_ref must be positive");
+    sys->T_ref = T_ref;
+    sys->drop_graphs();
+    return PC_OK;
+}
+int pc_set_overrelax_mode(pc_system* sys, int mode) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (mode != 0 && mode != 1) return fail(PC_ERR_INVALID, "overrelaxation mode must be 0 (rotation) or 1 (reflection)");
+    sys->or_mode = mode;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_set_colouring(pc_system* sys, int mode) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (sys->ready) return fail(PC_ERR_STATE, "colouring must be chosen before setup_lattice()");
+    if (mode != 0 && mode != 1) return fail(PC_ERR_INVALID, "colouring mode must be 0 (per sublattice) or 1 (fewest classes)");
+    sys->colouring = mode;
+    return PC_OK;
+}
+
+int pc_setup_lattice(pc_system* sys) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (sys->ready) return fail(PC_ERR_STATE, "setup_lattice() already called");
+    if (sys->specs.size() > 100) return fail(PC_ERR_UNSUPPORTED, "at most 100 coupling specs");
+    rc = build_tables(sys, false, sys->tab_active);
+    if (rc) return rc;
+    rc = build_tables(sys, true, sys->tab_full);
+    if (rc) return rc;
+    rc = build_colours(sys);
+    if (rc) return rc;
+    PC_CK(sys->d_tab_active.alloc(16));
+    PC_CK(sys->d_tab_full.alloc(16));
+    PC_CK(cudaMemcpy(sys->d_tab_active.p, sys->tab_active, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
+    PC_CK(cudaMemcpy(sys->d_tab_full.p, sys->tab_full, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
+    rc = build_tiles(sys);
+    if (rc) return rc;
+    sys->ready = true;
+    return PC_OK;
+}
+
+int pc_pyrochlore_displacements(int kind, int pyro_sl, int64_t* out, int max_n, int* n) {
+    if (pyro_sl < 0 || pyro_sl > 3) return fail(PC_ERR_INVALID, "pyro_sl must be 0..3");
+    const bool pair = kind >= 10 && kind <= 13;
+    if (!pair && (kind < 1 || kind > 4)) return fail(PC_ERR_INVALID, "unknown displacement table kind");
+    const int64_t r2 = (kind == 2) ? 24 : (kind == 1 || pair) ? 8 : 32;
+    const std::array<int64_t, 3> x0 = {kLink[pyro_sl][0], kLink[pyro_sl][1], kLink[pyro_sl][2]};
+    int cnt = 0;
+    for (int64_t dx = -4; dx <= 4; ++dx)
+        for (int64_t dy = -4; dy <= 4; ++dy)
+            for (int64_t dz = -4; dz <= 4; ++dz) {
+                if (dx * dx + dy * dy + dz * dz != r2) continue;
+                const std::array<int64_t, 3> x = {x0[0] + dx, x0[1] + dy, x0[2] + dz};
+                const int sl2 = sl_at(x);
+                if (sl2 < 0) continue;
+                if (kind == 3 || kind == 4) {
+                    const bool mid = sl_at({x0[0] + dx / 2, x0[1] + dy / 2, x0[2] + dz / 2}) >= 0;
+                    if ((kind == 3) != mid) continue;
+                }
+                if (pair && sl2 % 4 != kind - 10) continue;
+                if (cnt >= max_n) return fail(PC_ERR_INVALID, "max_n too small");
+                out[3 * cnt] = dx;
+                out[3 * cnt + 1] = dy;
+                out[3 * cnt + 2] = dz;
+                ++cnt;
+            }
+    *n = cnt;
+    return PC_OK;
+}
+
+int pc_num_replicas(pc_system* sys, int* n) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    *n = sys->R;
+    return PC_OK;
+}
+int pc_num_spins(pc_system* sys, int replica, int64_t* n) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    *n = sys->N(replica);
+    return PC_OK;
+}
+int pc_colours(pc_system* sys, int* n_colours, int32_t* colour_of_sl) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    *n_colours = sys->n_colours;
+    if (colour_of_sl)
+        for (int i = 0; i < 16; ++i) colour_of_sl[i] = sys->colour_of_sl[i];
+    return PC_OK;
+}
+
+int pc_neighbour_table(pc_system* sys, int replica, int spec, int max_nb, int32_t* out) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    if (spec < 0 || spec >= int(sys->specs.size())) return fail(PC_ERR_INVALID, "spec index out of range");
+    const Coupling& c = sys->specs[size_t(spec)];
+    const int L = sys->L[size_t(replica)];
+    const int64_t Nc = sys->Nc(replica);
+    for (int p = 0; p < 4; ++p)
+        if (int(c.rel[p].size()) > max_nb) return fail(PC_ERR_INVALID, "max_nb too small");
+    for (int sl = 0; sl < 16; ++sl) {
+        const auto r = r_sl(sl);
+        const auto& rel = c.rel[sl % 4];
+        for (int64_t cell = 0; cell < Nc; ++cell) {
+            const int64_t cx = cell % L, cy = (cell / L) % L, cz = cell / (int64_t(L) * L);
+            int32_t* row = out + (size_t(sl) * Nc + cell) * size_t(max_nb);
+            for (int j = 0; j < max_nb; ++j) row[j] = -1;
+            for (size_t j = 0; j < rel.size(); ++j) {
+                const std::array<int64_t, 3> x = {8 * cx + r[0] + rel[j][0], 8 * cy + r[1] + rel[j][1],
+                                                  8 * cz + r[2] + rel[j][2]};
+                const int sl2 = sl_at(x);
+                if (sl2 < 0) return fail(PC_ERR_INVALID, "displacement does not land on a site");
+                const auto r2 = r_sl(sl2);
+                const int64_t nx = pmod((x[0] - r2[0]) / 8, L), ny = pmod((x[1] - r2[1]) / 8, L),
+                              nz = pmod((x[2] - r2[2]) / 8, L);
+                row[j] = int32_t(int64_t(sl2) * Nc + nx + L * (ny + int64_t(L) * nz));
+            }
+        }
+    }
+    return PC_OK;
+}
+
+int pc_site_positions(pc_system* sys, int replica, int64_t* pos, int32_t* sl_out) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    const int L = sys->L[size_t(replica)];
+    const int64_t Nc = sys->Nc(replica);
+    for (int sl = 0; sl < 16; ++sl) {
+        const auto r = r_sl(sl);
+        for (int64_t cell = 0; cell < Nc; ++cell) {
+            const int64_t c[3] = {cell % L, (cell / L) % L, cell / (int64_t(L) * L)};
+            const size_t i = size_t(sl) * size_t(Nc) + size_t(cell);
+            for (int a = 0; a < 3; ++a) pos[3 * i + a] = pmod(8 * c[a] + r[a], 8 * int64_t(L));
+            if (sl_out) sl_out[i] = sl;
+        }
+    }
+    return PC_OK;
+}
+
+int pc_launch_count(pc_system* sys, uint64_t* n) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    *n = sys->launches;
+    return PC_OK;
+}
+
+int pc_set_spins(pc_system* sys, int replica, const double* S) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    const int64_t n = sys->N(replica);
+    std::vector<float4> buf(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i)
+        buf[size_t(i)] = make_float4(float(S[3 * i]), float(S[3 * i + 1]), float(S[3 * i + 2]), 0.f);
+    PC_CK(cudaMemcpyAsync(sys->d_spins.p + sys->off[size_t(replica)], buf.data(), sizeof(float4) * size_t(n),
+                          cudaMemcpyHostToDevice, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+int pc_get_spins(pc_system* sys, int replica, double* S) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    const int64_t n = sys->N(replica);
+    std::vector<float4> buf(static_cast<size_t>(n));
+    PC_CK(cudaMemcpyAsync(buf.data(), sys->d_spins.p + sys->off[size_t(replica)], sizeof(float4) * size_t(n),
+                          cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    for (int64_t i = 0; i < n; ++i) {
+        S[3 * i] = buf[size_t(i)].x;
+        S[3 * i + 1] = buf[size_t(i)].y;
+        S[3 * i + 2] = buf[size_t(i)].z;
+    }
+    return PC_OK;
+}
+int pc_set_spins_f4(pc_system* sys, int replica, const float* S4) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    PC_CK(cudaMemcpyAsync(sys->d_spins.p + sys->off[size_t(replica)], S4, sizeof(float4) * size_t(sys->N(replica)),
+                          cudaMemcpyHostToDevice, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+int pc_get_spins_f4(pc_system* sys, int replica, float* S4) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    PC_CK(cudaMemcpyAsync(S4, sys->d_spins.p + sys->off[size_t(replica)], sizeof(float4) * size_t(sys->N(replica)),
+                          cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+int pc_random_spins(pc_system* sys, uint64_t seed) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    pc::launch_random_spins(sys->d_spins.p, sys->d_reps.p, sys->d_all_tiles.p, sys->n_all_tiles, seed, sys->threads,
+                            sys->stream);
+    PC_LAUNCH_CK();
+    sys->launches++;
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+int pc_spins_device(pc_system* sys, int replica, void** dev_ptr) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    *dev_ptr = sys->d_spins.p + sys->off[size_t(replica)];
+    return PC_OK;
+}
+int pc_get_sweep_counter(pc_system* sys, int replica, uint64_t* sweep) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    PC_CK(cudaMemcpy(sweep, sys->d_sweep.p, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    return PC_OK;
+}
+int pc_set_sweep_counter(pc_system* sys, int replica, uint64_t sweep) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    PC_CK(cudaMemcpy(sys->d_sweep.p, &sweep, sizeof(uint64_t), cudaMemcpyHostToDevice));
+    sys->host_sweep = sweep;
+    return PC_OK;
+}
+
+int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uint64_t* accepted) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!T) return fail(PC_ERR_INVALID, "null temperature array");
+    if (n_sweeps < 0 || n_overrelax < 0 || n_overrelax > 200) return fail(PC_ERR_INVALID, "bad sweep counts");
+    for (int r = 0; r < sys->R; ++r)
+        if (!(T[r] > 0)) return fail(PC_ERR_INVALID, "temperatures must be positive");
+    PC_CK(cudaMemcpyAsync(sys->d_T.p, T, sizeof(double) * size_t(sys->R), cudaMemcpyHostToDevice, sys->stream));
+    PC_CK(cudaMemsetAsync(sys->d_acc.p, 0, sizeof(unsigned long long) * size_t(sys->R), sys->stream));
+    rc = run_sweeps(sys, n_sweeps, n_overrelax);
+    if (rc) return rc;
+    if (accepted) {
+        PC_CK(cudaMemcpyAsync(accepted, sys->d_acc.p, sizeof(uint64_t) * size_t(sys->R), cudaMemcpyDeviceToHost,
+                              sys->stream));
+        PC_CK(cudaStreamSynchronize(sys->stream));
+    }
+    return PC_OK;
+}
+
+int pc_overrelax_theta(pc_system* sys, int replica, const double* theta) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    const int64_t n = sys->N(replica);
+    if (theta) {
+        PC_CK(sys->d_theta.alloc(size_t(n)));
+        PC_CK(cudaMemcpy(sys->d_theta.p, theta, sizeof(double) * size_t(n), cudaMemcpyHostToDevice));
+    }
+    for (int c = 0; c < sys->n_colours; ++c) {
+        pc::PassArgs a = pass_args(sys, c, 0, 0);
+        a.theta = sys->d_theta.p;
+        a.theta_replica = replica;
+        // only the requested replica's tiles: the theta array is per site of it
+        std::vector<Tile> tiles;
+        const auto& sls = sys->colour_sls[size_t(c)];
+        for (size_t k = 0; k < sls.size(); ++k)
+            for (int64_t c0 = 0; c0 < sys->Nc(replica); c0 += sys->threads)
+                tiles.push_back(make_int4(replica, int(k << 8) | sls[k], int(c0),
+                                          int(std::min<int64_t>(sys->threads, sys->Nc(replica) - c0))));
+        DevBuf<Tile> dt;
+        PC_CK(dt.alloc(tiles.size()));
+        PC_CK(cudaMemcpy(dt.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
+        a.tiles = dt.p;
+        a.n_tiles = int(tiles.size());
+        pc::launch_colour_pass(theta ? pc::kOverrelaxTheta : pc::kOverrelaxReflect, a, grid_for(sys, a.n_tiles),
+                               sys->threads, sys->stream);
+        PC_LAUNCH_CK();
+        sys->launches++;
+        PC_CK(cudaStreamSynchronize(sys->stream));
+        dt.release();
+    }
+    return PC_OK;
+}
+
+int pc_energy(pc_system* sys, double* e_per_cell, double* mag) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    rc = enqueue_energy(sys);
+    if (rc) return rc;
+    PC_CK(cudaMemcpyAsync(e_per_cell, sys->d_e.p, sizeof(double) * size_t(sys->R), cudaMemcpyDeviceToHost, sys->stream));
+    if (mag)
+        PC_CK(cudaMemcpyAsync(mag, sys->d_mag.p, sizeof(double) * 3 * size_t(sys->R), cudaMemcpyDeviceToHost,
+                              sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+
+int pc_local_field(pc_system* sys, int replica, double* h) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    if (sys->d_field.n != size_t(sys->N_tot)) PC_CK(sys->d_field.alloc(size_t(sys->N_tot)));
+    pc::FieldArgs a;
+    a.spins = sys->d_spins.p;
+    a.reps = sys->d_reps.p;
+    a.tables = sys->d_tab_active.p;
+    a.tiles = sys->d_all_tiles.p + sys->tile_begin[size_t(replica)];
+    a.n_tiles = sys->tile_end[size_t(replica)] - sys->tile_begin[size_t(replica)];
+    a.h_out = sys->d_field.p;
+    pc::launch_local_field(a, sys->threads, sys->stream);
+    PC_LAUNCH_CK();
+    sys->launches++;
+    const int64_t n = sys->N(replica);
+    std::vector<float4> buf(static_cast<size_t>(n));
+    PC_CK(cudaMemcpyAsync(buf.data(), sys->d_field.p + sys->off[size_t(replica)], sizeof(float4) * size_t(n),
+                          cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    for (int64_t i = 0; i < n; ++i) {
+        h[3 * i] = buf[size_t(i)].x;
+        h[3 * i + 1] = buf[size_t(i)].y;
+        h[3 * i + 2] = buf[size_t(i)].z;
+    }
+    return PC_OK;
+}
+
+// ------------------------------------------------------------------- SSF
+int pc_ssf_configure(pc_system* sys, const char* const* names, int n_corr, int n_slots, const int32_t* L_of_slot) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (n_corr < 1 || n_corr > 9) return fail(PC_ERR_INVALID, "ssf_manager: between 1 and 9 correlators");
+    if (n_slots < 0) return fail(PC_ERR_INVALID, "negative slot count");
+    // ssf_manager.hpp:176-193
+    auto axis = [](char c) -> int { return c == 'x' ? 0 : c == 'y' ? 1 : c == 'z' ? 2 : -1; };
+    for (int c = 0; c < n_corr; ++c) {
+        const std::string nm = names[c] ? names[c] : "";
+        if (nm.size() != 2) return fail(PC_ERR_INVALID, "ssf_manager: correlator name must be 2 chars: " + nm);
+        for (int k = 0; k < 2; ++k)
+            if (axis(nm[size_t(k)]) < 0)
+                return fail(PC_ERR_INVALID, std::string("ssf_manager: unknown spin component '") + nm[size_t(k)] + "'");
+        sys->corr_a[c] = axis(nm[0]);
+        sys->corr_b[c] = axis(nm[1]);
+    }
+    rc = ensure_groups(sys);
+    if (rc) return rc;
+    sys->n_corr = n_corr;
+    sys->n_slots = n_slots;
+    sys->L_of_slot.assign(L_of_slot, L_of_slot + n_slots);
+    int64_t max_nk = 1;
+    for (int sl = 0; sl < n_slots; ++sl) {
+        bool found = false;
+        for (auto& g : sys->groups) found = found || (g.L == L_of_slot[sl]);
+        if (!found) return fail(PC_ERR_INVALID, "slot size matches no replica");
+        max_nk = std::max<int64_t>(max_nk, int64_t(L_of_slot[sl]) * L_of_slot[sl] * L_of_slot[sl]);
+    }
+    sys->slot_stride = int64_t(n_corr) * max_nk * 2;
+    PC_CK(sys->d_ssf_sum.alloc(size_t(std::max(1, n_slots)) * size_t(sys->slot_stride)));
+    PC_CK(sys->d_ssf_sq.alloc(size_t(std::max(1, n_slots)) * size_t(sys->slot_stride)));
+    PC_CK(cudaMemset(sys->d_ssf_sum.p, 0, sizeof(double) * sys->d_ssf_sum.n));
+    PC_CK(cudaMemset(sys->d_ssf_sq.p, 0, sizeof(double) * sys->d_ssf_sq.n));
+    PC_CK(sys->d_slot_of_rep.alloc(size_t(sys->R)));
+    sys->ssf_n.assign(size_t(n_slots), 0);
+    sys->ssf_ready = true;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_ssf_sample(pc_system* sys, const int32_t* slot_of_replica) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    for (int r = 0; r < sys->R; ++r) {
+        const int s = slot_of_replica[r];
+        if (s >= sys->n_slots) return fail(PC_ERR_INVALID, "slot index out of range");
+        if (s >= 0 && sys->L_of_slot[size_t(s)] != sys->L[size_t(r)])
+            return fail(PC_ERR_INVALID, "slot size differs from replica size");
+    }
+    PC_CK(cudaMemcpyAsync(sys->d_slot_of_rep.p, slot_of_replica, sizeof(int32_t) * size_t(sys->R),
+                          cudaMemcpyHostToDevice, sys->stream));
+    for (auto& g : sys->groups) {
+        std::vector<int32_t> sel;
+        for (int r : g.reps)
+            if (slot_of_replica[r] >= 0) sel.push_back(r);
+        g.n_sel = int(sel.size());
+        if (!sel.empty())  // pageable source: the call returns once the data is staged
+            PC_CK(cudaMemcpyAsync(g.d_sel_index.p, sel.data(), sizeof(int32_t) * sel.size(), cudaMemcpyHostToDevice,
+                                  sys->stream));
+    }
+    pc::SsfOut o = ssf_out_base(sys);
+    o.acc_sum = sys->d_ssf_sum.p;
+    o.acc_sq = sys->d_ssf_sq.p;
+    o.slot_of_rep = sys->d_slot_of_rep.p;
+    rc = enqueue_ssf(sys, o, true);
+    if (rc) return rc;
+    for (int r = 0; r < sys->R; ++r)
+        if (slot_of_replica[r] >= 0) sys->ssf_n[size_t(slot_of_replica[r])]++;
+    return PC_OK;
+}
+
+int pc_ssf_read(pc_system* sys, int slot, double* sum, double* sq, uint64_t* n_samples) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    if (slot < 0 || slot >= sys->n_slots) return fail(PC_ERR_INVALID, "slot index out of range");
+    const int L = sys->L_of_slot[size_t(slot)];
+    const size_t n = size_t(sys->n_corr) * size_t(L) * L * L * 2;
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    if (sum)
+        PC_CK(cudaMemcpy(sum, sys->d_ssf_sum.p + size_t(slot) * sys->slot_stride, sizeof(double) * n,
+                         cudaMemcpyDeviceToHost));
+    if (sq)
+        PC_CK(cudaMemcpy(sq, sys->d_ssf_sq.p + size_t(slot) * sys->slot_stride, sizeof(double) * n,
+                         cudaMemcpyDeviceToHost));
+    if (n_samples) *n_samples = sys->ssf_n[size_t(slot)];
+    return PC_OK;
+}
+
+int pc_ssf_clear(pc_system* sys, int slot) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    if (slot < 0 || slot >= sys->n_slots) return fail(PC_ERR_INVALID, "slot index out of range");
+    PC_CK(cudaMemsetAsync(sys->d_ssf_sum.p + size_t(slot) * sys->slot_stride, 0, sizeof(double) * sys->slot_stride,
+                          sys->stream));
+    PC_CK(cudaMemsetAsync(sys->d_ssf_sq.p + size_t(slot) * sys->slot_stride, 0, sizeof(double) * sys->slot_stride,
+                          sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    sys->ssf_n[size_t(slot)] = 0;
+    return PC_OK;
+}
+
+int pc_ssf_forward(pc_system* sys, void* out_dev) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    // out_dev is [R][n_corr][n_k][2] with replicas in index order; the kernel
+    // indexes by position inside each size group, so offset per group.
+    size_t base = 0;
+    for (auto& g : sys->groups) {
+        const size_t nk = size_t(g.L) * g.L * g.L;
+        // groups must be replica-contiguous for the packed layout
+        for (size_t i = 0; i < g.reps.size(); ++i)
+            if (g.reps[i] != g.reps[0] + int(i)) return fail(PC_ERR_UNSUPPORTED, "ssf forward needs size-sorted replicas");
+        pc::SsfOut o = ssf_out_base(sys);
+        size_t off = 0;
+        for (int r = 0; r < g.reps[0]; ++r) off += size_t(sys->n_corr) * size_t(sys->Nc(r)) * 2;
+        o.val = static_cast<double*>(out_dev) + off;
+        pc::SsfGeom geom{g.L, g.P, g.Q, int(g.reps.size()), g.d_rep_index.p};
+        pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, g.d_G.p, sys->stream);
+        PC_LAUNCH_CK();
+        pc::launch_ssf_z(geom, g.d_G.p, o, sys->stream);
+        PC_LAUNCH_CK();
+        sys->launches += 2;
+        base += g.reps.size() * nk;
+    }
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+
+int pc_ssf_backward(pc_system* sys, const void* grad_out_dev, void* grad_S_dev) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    PC_CK(cudaMemsetAsync(grad_S_dev, 0, sizeof(float4) * size_t(sys->N_tot), sys->stream));
+    for (auto& g : sys->groups) {
+        for (size_t i = 0; i < g.reps.size(); ++i)
+            if (g.reps[i] != g.reps[0] + int(i))
+                return fail(PC_ERR_UNSUPPORTED, "ssf backward needs size-sorted replicas");
+        const size_t nk = size_t(g.L) * g.L * g.L;
+        if (g.d_amp.n != g.reps.size() * 3 * nk) PC_CK(g.d_amp.alloc(g.reps.size() * 3 * nk));
+        pc::SsfGeom geom{g.L, g.P, g.Q, int(g.reps.size()), g.d_rep_index.p};
+        pc::SsfOut o = ssf_out_base(sys);
+        o.amp = g.d_amp.p;
+        // recompute the forward amplitudes
+        pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, g.d_G.p, sys->stream);
+        PC_LAUNCH_CK();
+        pc::launch_ssf_z(geom, g.d_G.p, o, sys->stream);
+        PC_LAUNCH_CK();
+        size_t off = 0;
+        for (int r = 0; r < g.reps[0]; ++r) off += size_t(sys->n_corr) * size_t(sys->Nc(r)) * 2;
+        const double* dval = static_cast<const double*>(grad_out_dev) + off;
+        pc::launch_ssf_adjoint(geom, o, dval, g.d_amp.p, g.d_G.p, static_cast<float4*>(grad_S_dev), sys->d_reps.p,
+                               sys->stream);
+        PC_LAUNCH_CK();
+        sys->launches += 4;
+    }
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+
+int pc_ssf_current(pc_system* sys, int replica, double* out) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    const size_t n = size_t(sys->n_corr) * size_t(sys->Nc(replica)) * 2;
+    DevBuf<double> val;
+    PC_CK(val.alloc(n));
+    for (auto& g : sys->groups) {
+        if (g.L != sys->L[size_t(replica)]) continue;
+        DevBuf<int32_t> idx;
+        PC_CK(idx.alloc(1));
+        PC_CK(cudaMemcpy(idx.p, &replica, sizeof(int32_t), cudaMemcpyHostToDevice));
+        pc::SsfGeom geom{g.L, g.P, g.Q, 1, idx.p};
+        pc::SsfOut o = ssf_out_base(sys);
+        o.val = val.p;
+        pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, g.d_G.p, sys->stream);
+        PC_LAUNCH_CK();
+        pc::launch_ssf_z(geom, g.d_G.p, o, sys->stream);
+        PC_LAUNCH_CK();
+        sys->launches += 2;
+        PC_CK(cudaStreamSynchronize(sys->stream));
+        idx.release();
+    }
+    PC_CK(cudaMemcpy(out, val.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    val.release();
+    return PC_OK;
+}
+
+// ------------------------------------------------------------- tempering
+int pc_pt_configure(pc_system* sys, const double* T) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    std::map<int, std::vector<int>> by_L;
+    for (int r = 0; r < sys->R; ++r) {
+        if (!(T[r] > 0)) return fail(PC_ERR_INVALID, "temperatures must be positive");
+        by_L[sys->L[size_t(r)]].push_back(r);
+    }
+    std::vector<int32_t> rep_of_slot, slot_of_rep(size_t(sys->R));
+    sys->ladder_begin.clear();
+    sys->T_slot.clear();
+    for (auto& kv : by_L) {
+        auto reps = kv.second;
+        std::stable_sort(reps.begin(), reps.end(), [&](int a, int b) { return T[a] > T[b]; });
+        sys->ladder_begin.push_back(int32_t(rep_of_slot.size()));
+        for (int r : reps) {
+            slot_of_rep[size_t(r)] = int32_t(rep_of_slot.size());
+            rep_of_slot.push_back(r);
+            sys->T_slot.push_back(T[r]);
+        }
+    }
+    sys->ladder_begin.push_back(int32_t(rep_of_slot.size()));
+    sys->n_ladders = int(by_L.size());
+    const size_t ns = rep_of_slot.size();
+    PC_CK(sys->d_ladder_begin.alloc(sys->ladder_begin.size()));
+    PC_CK(cudaMemcpy(sys->d_ladder_begin.p, sys->ladder_begin.data(), sizeof(int32_t) * sys->ladder_begin.size(),
+                     cudaMemcpyHostToDevice));
+    PC_CK(sys->d_rep_of_slot.alloc(ns));
+    PC_CK(cudaMemcpy(sys->d_rep_of_slot.p, rep_of_slot.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice));
+    PC_CK(sys->d_pt_slot_of_rep.alloc(ns));
+    PC_CK(cudaMemcpy(sys->d_pt_slot_of_rep.p, slot_of_rep.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice));
+    PC_CK(sys->d_T_slot.alloc(ns));
+    PC_CK(cudaMemcpy(sys->d_T_slot.p, sys->T_slot.data(), sizeof(double) * ns, cudaMemcpyHostToDevice));
+    PC_CK(cudaMemcpy(sys->d_T.p, T, sizeof(double) * ns, cudaMemcpyHostToDevice));
+    PC_CK(sys->d_E_sum.alloc(ns));
+    PC_CK(sys->d_E2_sum.alloc(ns));
+    PC_CK(sys->d_n_e.alloc(ns));
+    PC_CK(sys->d_att.alloc(ns));
+    PC_CK(sys->d_accn.alloc(ns));
+    PC_CK(cudaMemset(sys->d_E_sum.p, 0, sizeof(double) * ns));
+    PC_CK(cudaMemset(sys->d_E2_sum.p, 0, sizeof(double) * ns));
+    PC_CK(cudaMemset(sys->d_n_e.p, 0, sizeof(unsigned long long) * ns));
+    PC_CK(cudaMemset(sys->d_att.p, 0, sizeof(unsigned long long) * ns));
+    PC_CK(cudaMemset(sys->d_accn.p, 0, sizeof(unsigned long long) * ns));
+    PC_CK(sys->d_round.alloc(1));
+    PC_CK(cudaMemset(sys->d_round.p, 0, sizeof(uint64_t)));
+    sys->pt_sweeps_done = 0;
+    sys->pt_ready = true;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+namespace {
+int enqueue_pt_round(pc_system* s, int n_sweep, int ssf_every, uint64_t sweep_phase) {
+    for (int i = 0; i < n_sweep; ++i) {
+        int rc = enqueue_sweep(s, uint64_t(i), 1, false);
+        if (rc) return rc;
+        if (ssf_every > 0 && (sweep_phase + uint64_t(i) + 1) % uint64_t(ssf_every) == 0) {
+            pc::SsfOut o = ssf_out_base(s);
+            o.acc_sum = s->d_ssf_sum.p;
+            o.acc_sq = s->d_ssf_sq.p;
+            o.slot_of_rep = s->d_pt_slot_of_rep.p;
+            rc = enqueue_ssf(s, o, false);
+            if (rc) return rc;
+        }
+    }
+    pc::launch_advance_counter(s->d_sweep.p, uint64_t(n_sweep), s->stream);
+    PC_LAUNCH_CK();
+    s->launches++;
+    int rc = enqueue_energy(s);
+    if (rc) return rc;
+    pc::PtArgs a;
+    a.n_ladders = s->n_ladders;
+    a.ladder_begin = s->d_ladder_begin.p;
+    a.T_slot = s->d_T_slot.p;
+    a.rep_of_slot = s->d_rep_of_slot.p;
+    a.slot_of_rep = s->d_pt_slot_of_rep.p;
+    a.T_rep = s->d_T.p;
+    a.e_rep = s->d_e.p;
+    a.reps = s->d_reps.p;
+    a.E_sum = s->d_E_sum.p;
+    a.E2_sum = s->d_E2_sum.p;
+    a.n_e = s->d_n_e.p;
+    a.attempts = s->d_att.p;
+    a.accepts = s->d_accn.p;
+    a.round = s->d_round.p;
+    a.seed = s->seed;
+    a.n_slots = int(s->T_slot.size());
+    pc::launch_pt_exchange(a, s->stream);
+    PC_LAUNCH_CK();
+    s->launches++;
+    return PC_OK;
+}
+}  // namespace
+
+int pc_pt_run(pc_system* sys, int n_rounds, int n_sweep, int ssf_every) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->pt_ready) return fail(PC_ERR_STATE, "tempering not configured");
+    if (n_rounds < 0 || n_sweep < 1 || ssf_every < 0) return fail(PC_ERR_INVALID, "bad tempering schedule");
+    if (ssf_every > 0) {
+        if (!sys->ssf_ready || sys->n_slots != int(sys->T_slot.size()))
+            return fail(PC_ERR_STATE, "tempering SSF needs pc_ssf_configure with one slot per replica");
+        for (size_t sl = 0; sl < sys->T_slot.size(); ++sl) {
+            int32_t r = -1;
+            PC_CK(cudaMemcpy(&r, sys->d_rep_of_slot.p + sl, sizeof(int32_t), cudaMemcpyDeviceToHost));
+            if (sys->L_of_slot[sl] != sys->L[size_t(r)])
+                return fail(PC_ERR_INVALID, "tempering SSF slot sizes must follow the ladders (ascending L)");
+        }
+    }
+    PC_CK(cudaMemsetAsync(sys->d_acc.p, 0, sizeof(unsigned long long) * size_t(sys->R), sys->stream));
+    const uint64_t period = ssf_every > 0 ? uint64_t(ssf_every) : 1;
+    for (int round = 0; round < n_rounds; ++round) {
+        const uint64_t phase = sys->pt_sweeps_done % period;
+        const auto key = std::make_pair(n_sweep, int(ssf_every > 0 ? phase : 0) + 100000 * ssf_every);
+        auto it = sys->pt_graphs.find(key);
+        if (it == sys->pt_graphs.end()) {
+            const uint64_t before = sys->launches;
+            PC_CK(cudaStreamBeginCapture(sys->stream, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_pt_round(sys, n_sweep, ssf_every, phase);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(sys->stream, &g);
+            if (rc) return rc;
+            if (e != cudaSuccess) return fail(PC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            cudaGraphExec_t x = nullptr;
+            PC_CK(cudaGraphInstantiate(&x, g, 0));
+            cudaGraphDestroy(g);
+            const int nodes = int(sys->launches - before);
+            sys->launches = before;
+            it = sys->pt_graphs.insert({key, {x, nodes}}).first;
+        }
+        PC_CK(cudaGraphLaunch(it->second.first, sys->stream));
+        sys->launches += uint64_t(it->second.second);
+        // host-side SSF sample counts (every slot samples together)
+        if (ssf_every > 0)
+            for (int i = 0; i < n_sweep; ++i)
+                if ((phase + uint64_t(i) + 1) % uint64_t(ssf_every) == 0)
+                    for (auto& n : sys->ssf_n) n++;
+        sys->pt_sweeps_done += uint64_t(n_sweep);
+        sys->host_sweep += uint64_t(n_sweep);
+    }
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+
+int pc_pt_reset_stats(pc_system* sys) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->pt_ready) return fail(PC_ERR_STATE, "tempering not configured");
+    const size_t ns = sys->T_slot.size();
+    PC_CK(cudaMemsetAsync(sys->d_E_sum.p, 0, sizeof(double) * ns, sys->stream));
+    PC_CK(cudaMemsetAsync(sys->d_E2_sum.p, 0, sizeof(double) * ns, sys->stream));
+    PC_CK(cudaMemsetAsync(sys->d_n_e.p, 0, sizeof(unsigned long long) * ns, sys->stream));
+    PC_CK(cudaMemsetAsync(sys->d_att.p, 0, sizeof(unsigned long long) * ns, sys->stream));
+    PC_CK(cudaMemsetAsync(sys->d_accn.p, 0, sizeof(unsigned long long) * ns, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+
+int pc_pt_read_energy(pc_system* sys, double* T, double* E, double* E2, uint64_t* n) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->pt_ready) return fail(PC_ERR_STATE, "tempering not configured");
+    const size_t ns = sys->T_slot.size();
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    if (T) std::memcpy(T, sys->T_slot.data(), sizeof(double) * ns);
+    if (E) PC_CK(cudaMemcpy(E, sys->d_E_sum.p, sizeof(double) * ns, cudaMemcpyDeviceToHost));
+    if (E2) PC_CK(cudaMemcpy(E2, sys->d_E2_sum.p, sizeof(double) * ns, cudaMemcpyDeviceToHost));
+    if (n) PC_CK(cudaMemcpy(n, sys->d_n_e.p, sizeof(uint64_t) * ns, cudaMemcpyDeviceToHost));
+    return PC_OK;
+}
+int pc_pt_read_exchange(pc_system* sys, uint64_t* attempts, uint64_t* accepts) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->pt_ready) return fail(PC_ERR_STATE, "tempering not configured");
+    const size_t ns = sys->T_slot.size();
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    PC_CK(cudaMemcpy(attempts, sys->d_att.p, sizeof(uint64_t) * ns, cudaMemcpyDeviceToHost));
+    PC_CK(cudaMemcpy(accepts, sys->d_accn.p, sizeof(uint64_t) * ns, cudaMemcpyDeviceToHost));
+    return PC_OK;
+}
+int pc_pt_slots(pc_system* sys, int32_t* slot_of_replica) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->pt_ready) return fail(PC_ERR_STATE, "tempering not configured");
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    PC_CK(cudaMemcpy(slot_of_replica, sys->d_pt_slot_of_rep.p, sizeof(int32_t) * size_t(sys->R), cudaMemcpyDeviceToHost));
+    return PC_OK;
+}
+
+// -------------------------------------------------------------- gradients
+int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* grad_S_dev, double* grad_J,
+                   double* grad_B) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    const int ns = int(sys->specs.size());
+    const int width = 4 + 9 * ns;
+    DevBuf<double> d_g, d_out;
+    PC_CK(d_g.alloc(size_t(sys->R)));
+    PC_CK(d_out.alloc(size_t(sys->R) * size_t(width)));
+    std::vector<double> ones(size_t(sys->R), 1.0);
+    PC_CK(cudaMemcpy(d_g.p, g ? g : ones.data(), sizeof(double) * size_t(sys->R), cudaMemcpyHostToDevice));
+    pc::GradArgs a;
+    a.spins = sys->d_spins.p;
+    a.reps = sys->d_reps.p;
+    a.tables = sys->d_tab_full.p;
+    a.tiles = sys->d_all_tiles.p;
+    a.n_tiles = sys->n_all_tiles;
+    a.n_spec = ns;
+    for (int i = 0; i < 3; ++i) a.B[i] = float(sys->B[i]);
+    a.g = d_g.p;
+    a.grad_S = static_cast<float4*>(grad_S_dev);
+    a.partial = sys->d_partial.p;
+    pc::launch_energy_grad_partials(a, sys->threads, sys->stream);
+    PC_LAUNCH_CK();
+    pc::launch_grad_finalize(sys->d_partial.p, width, sys->d_tile_begin.p, sys->d_tile_end.p, sys->R, d_out.p,
+                             sys->stream);
+    PC_LAUNCH_CK();
+    sys->launches += 2;
+    std::vector<double> out(size_t(sys->R) * size_t(width));
+    PC_CK(cudaMemcpyAsync(out.data(), d_out.p, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    d_g.release();
+    d_out.release();
+    for (int r = 0; r < sys->R; ++r) {
+        const double* o = out.data() + size_t(r) * size_t(width);
+        const double nc = double(sys->Nc(r));
+        const double gr = g ? g[r] : 1.0;
+        if (e_per_cell) e_per_cell[r] = o[0] / nc;
+        if (grad_B)
+            for (int a3 = 0; a3 < 3; ++a3) grad_B[3 * r + a3] = -gr * o[1 + a3] / nc;
+        if (grad_J)
+            for (int k = 0; k < 9 * ns; ++k) grad_J[size_t(r) * 9 * size_t(ns) + size_t(k)] = gr * o[4 + k] / nc;
+    }
+    return PC_OK;
+}
+
+// ---------------------------------------------------------------- tuning
+int pc_get_tile(pc_system* sys, int* threads, int* ctas_per_sm) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    *threads = sys->threads;
+    *ctas_per_sm = sys->ctas_per_sm;
+    return PC_OK;
+}
+int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (threads < 32 || threads > 512 || threads % 32 != 0) return fail(PC_ERR_INVALID, "threads must be 32..512, a multiple of 32");
+    if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(PC_ERR_INVALID, "ctas_per_sm must be 1..32");
+    sys->threads = threads;
+    sys->ctas_per_sm = ctas_per_sm;
+    if (sys->ready) return build_tiles(sys);
+    return PC_OK;
+}
+
+int pc_autotune(pc_system* sys) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    const size_t bytes = sizeof(float4) * size_t(sys->N_tot);
+    DevBuf<float4> saved;
+    PC_CK(saved.alloc(size_t(sys->N_tot)));
+    PC_CK(cudaMemcpyAsync(saved.p, sys->d_spins.p, bytes, cudaMemcpyDeviceToDevice, sys->stream));
+    uint64_t sweep0 = 0;
+    PC_CK(cudaMemcpyAsync(&sweep0, sys->d_sweep.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    std::vector<double> T(size_t(sys->R), 1.0);
+    PC_CK(cudaMemcpy(sys->d_T.p, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
+    const int cand_threads[3] = {128, 256, 512};
+    const int cand_ctas[3] = {2, 4, 8};
+    int best_t = sys->threads, best_c = sys->ctas_per_sm;
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    PC_CK(cudaEventCreate(&e0));
+    PC_CK(cudaEventCreate(&e1));
+    const bool timing = sys->timing;
+    sys->timing = false;
+    for (int ti = 0; ti < 3; ++ti)
+        for (int ci = 0; ci < 3; ++ci) {
+            sys->threads = cand_threads[ti];
+            sys->ctas_per_sm = cand_ctas[ci];
+            rc = build_tiles(sys);
+            if (rc) return rc;
+            rc = run_sweeps(sys, 2, 1);  // warm-up + graph instantiation
+            if (rc) return rc;
+            PC_CK(cudaEventRecord(e0, sys->stream));
+            rc = run_sweeps(sys, 5, 1);
+            if (rc) return rc;
+            PC_CK(cudaEventRecord(e1, sys->stream));
+            PC_CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PC_CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_t = cand_threads[ti];
+                best_c = cand_ctas[ci];
+            }
+        }
+    sys->timing = timing;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    sys->threads = best_t;
+    sys->ctas_per_sm = best_c;
+    rc = build_tiles(sys);
+    if (rc) return rc;
+    PC_CK(cudaMemcpyAsync(sys->d_spins.p, saved.p, bytes, cudaMemcpyDeviceToDevice, sys->stream));
+    PC_CK(cudaMemcpyAsync(sys->d_sweep.p, &sweep0, sizeof(uint64_t), cudaMemcpyHostToDevice, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    sys->host_sweep = sweep0;
+    saved.release();
+    return PC_OK;
+}
+
+// --------------------------------------------------------------- bench API
+int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, int n_sweep, int ssf_every,
+                 int ssf_slot, double* e_out, uint64_t* accepted) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!(T > 0)) return fail(PC_ERR_INVALID, "temperature must be positive");
+    if (n_sweep < 0 || ssf_every < 0) return fail(PC_ERR_INVALID, "bad sweep counts");
+    const bool do_ssf = ssf_slot >= 0 && ssf_every > 0;
+    if (do_ssf && (!sys->ssf_ready || ssf_slot >= sys->n_slots || sys->L_of_slot[size_t(ssf_slot)] != sys->L[0]))
+        return fail(PC_ERR_STATE, "ssf slot not configured for replica 0");
+    const size_t bytes = sizeof(float4) * size_t(sys->N(0));
+    PC_CK(cudaMemcpyAsync(sys->d_spins.p, S4_in, bytes, cudaMemcpyHostToDevice, sys->stream));
+    std::vector<double> Tv(size_t(sys->R), T);
+    PC_CK(cudaMemcpyAsync(sys->d_T.p, Tv.data(), sizeof(double) * Tv.size(), cudaMemcpyHostToDevice, sys->stream));
+    PC_CK(cudaMemsetAsync(sys->d_acc.p, 0, sizeof(unsigned long long) * size_t(sys->R), sys->stream));
+    SsfGroup* grp = nullptr;
+    if (do_ssf) {
+        std::vector<int32_t> slots(size_t(sys->R), -1);
+        slots[0] = ssf_slot;
+        PC_CK(cudaMemcpyAsync(sys->d_slot_of_rep.p, slots.data(), sizeof(int32_t) * slots.size(), cudaMemcpyHostToDevice,
+                              sys->stream));
+        for (auto& g : sys->groups)
+            if (g.L == sys->L[0]) grp = &g;
+    }
+    int done = 0;
+    while (done < n_sweep) {
+        const int chunk = do_ssf ? std::min(ssf_every, n_sweep - done) : n_sweep - done;
+        rc = run_sweeps(sys, chunk, 1);
+        if (rc) return rc;
+        done += chunk;
+        if (do_ssf && chunk == ssf_every) {
+            pc::SsfOut o = ssf_out_base(sys);
+            o.acc_sum = sys->d_ssf_sum.p;
+            o.acc_sq = sys->d_ssf_sq.p;
+            o.slot_of_rep = sys->d_slot_of_rep.p;
+            pc::SsfGeom geom{grp->L, grp->P, grp->Q, 1, grp->d_rep_index.p};
+            pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, grp->d_G.p, sys->stream);
+            PC_LAUNCH_CK();
+            pc::launch_ssf_z(geom, grp->d_G.p, o, sys->stream);
+            PC_LAUNCH_CK();
+            sys->launches += 2;
+            sys->ssf_n[size_t(ssf_slot)]++;
+        }
+    }
+    rc = enqueue_energy(sys);
+    if (rc) return rc;
+    PC_CK(cudaMemcpyAsync(S4_out, sys->d_spins.p, bytes, cudaMemcpyDeviceToHost, sys->stream));
+    if (e_out) PC_CK(cudaMemcpyAsync(e_out, sys->d_e.p, sizeof(double), cudaMemcpyDeviceToHost, sys->stream));
+    if (accepted)
+        PC_CK(cudaMemcpyAsync(accepted, sys->d_acc.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+
+int pc_set_kernel_timing(pc_system* sys, int on) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    sys->timing = on != 0;
+    sys->ev_used = 0;
+    return PC_OK;
+}
+
+int pc_last_kernel_times(pc_system* sys, double* metropolis_ms, double* overrelax_ms) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    double tot[2] = {0, 0};
+    int cnt[2] = {0, 0};
+    for (size_t i = 0; i < sys->ev_used; ++i) {
+        float ms = 0.f;
+        PC_CK(cudaEventElapsedTime(&ms, sys->ev_pool[i].first, sys->ev_pool[i].second));
+        tot[sys->ev_kind[i]] += ms;
+        cnt[sys->ev_kind[i]]++;
+    }
+    if (metropolis_ms) *metropolis_ms = cnt[0] ? tot[0] / cnt[0] : 0.0;
+    if (overrelax_ms) *overrelax_ms = cnt[1] ? tot[1] / cnt[1] : 0.0;
+    sys->ev_used = 0;
+    return PC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,282 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 oracle.
+
+Tolerances (FP32 spins and transforms against an FP64 oracle):
+  energy per cell, local fields, one overrelaxation pass, S(q): 1e-5 relative
+  to the scale of the quantity (max |value| over the array);
+  trajectories of a few sweeps: 1e-4 absolute per spin component;
+  integer tables: exact.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import pyro_cmc_b200 as pc
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-5
+
+COUPLINGS = [
+    dict(J1=1.0, J2=0.0, J3=0.0, Delta=1.0, B=(0.0, 0.0, 0.0)),
+    dict(J1=1.0, J2=-0.1, J3=0.05, Delta=1.0, B=(0.0, 0.0, 0.0)),
+    dict(J1=1.0, J2=0.1, J3=-0.05, Delta=0.5, B=(0.2, 0.0, 0.0)),
+    dict(J1=-0.7, J2=0.3, J3=0.02, Delta=1.3, B=(0.0, 0.1, 0.5)),
+]
+
+
+def pair(L, c, seed=0, colouring=0, **kw):
+    g = pc.pyrochlore_system(L, seed=seed, colouring=colouring, **c, **kw)
+    o = oracle.System(L, seed=seed, **c)
+    return g, o
+
+
+def unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def states(o, rng):
+    _, sl = o.positions()
+    pos, _ = o.positions()
+    z = np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], float) / np.sqrt(3)
+    q = 2 * np.pi * 3 / (8 * o.L)
+    spiral = np.stack([np.zeros(len(pos)), np.cos(q * pos[:, 2]), np.sin(q * pos[:, 2])], axis=1)
+    fm = np.tile([0.48, 0.6, 0.64], (o.N, 1))
+    return {"random": unit(rng, o.N), "fm": fm, "aiao": z[sl % 4], "spiral": spiral}
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 5])
+def test_neighbour_tables_bit_exact(L):
+    g, o = pair(L, COUPLINGS[1])
+    assert o.num_specs() == len(g.spec_names) == 9
+    for spec in range(9):
+        a = g.neighbour_table(spec, max_nb=16)
+        b = o.neighbours(spec, max_nb=16)
+        a = a[:, : b.shape[1]]
+        np.testing.assert_array_equal(np.sort(a, axis=1), np.sort(b, axis=1))
+
+
+def test_positions_match_oracle():
+    g, o = pair(3, COUPLINGS[0])
+    pg, sg = g.positions()
+    po, so = o.positions()
+    np.testing.assert_array_equal(pg, po % 24)
+    np.testing.assert_array_equal(sg, so)
+
+
+@pytest.mark.parametrize("L", [1, 2, 4, 8])
+@pytest.mark.parametrize("ci", range(len(COUPLINGS)))
+def test_energy_and_local_field(L, ci):
+    g, o = pair(L, COUPLINGS[ci])
+    rng = np.random.default_rng(100 * L + ci)
+    for name, S in states(o, rng).items():
+        o.set_spins(S)
+        g.set_spins(S)
+        S32 = g.spins()  # what the device holds (FP32)
+        o.set_spins(S32)
+        e_ref = o.energy()
+        h_ref = o.local_fields()
+        e, m = g.energy()
+        scale = 16 * (6 * abs(COUPLINGS[ci]["J1"]) + 12 * abs(COUPLINGS[ci]["J2"]) + 12 * abs(COUPLINGS[ci]["J3"]) + 1)
+        assert abs(e[0] - e_ref) <= REL * scale, (name, e[0], e_ref)
+        np.testing.assert_allclose(m[0], S32.sum(axis=0), atol=1e-6 * o.N)
+        h = g.local_field()
+        err = np.abs(h - h_ref).max() / max(1.0, np.abs(h_ref).max())
+        assert err <= REL, (name, err)
+
+
+def test_ferromagnet_energy_known_answer():
+    c = dict(J1=1.3, J2=-0.4, J3=0.25, Delta=1.0, B=(0.1, -0.2, 0.7))
+    g = pc.pyrochlore_system(4, **c)
+    n = np.array([0.48, 0.6, 0.64])
+    g.set_spins(np.tile(n, (g.N(), 1)))
+    e, _ = g.energy()
+    exact = 48 * 1.3 + 96 * -0.4 + 96 * 0.25 - 16 * np.dot([0.1, -0.2, 0.7], n)
+    assert e[0] == pytest.approx(exact, rel=1e-5)
+
+
+@pytest.mark.parametrize("colouring", [0, 1])
+@pytest.mark.parametrize("ci", [0, 2])
+def test_overrelax_pass_with_given_angles(colouring, ci):
+    g, o = pair(4, COUPLINGS[ci], colouring=colouring)
+    rng = np.random.default_rng(7)
+    S = unit(rng, o.N)
+    g.set_spins(S)
+    o.set_spins(g.spins())
+    _, col = g.colours()
+    theta = rng.uniform(0, 2 * np.pi, o.N)
+    e0 = o.energy()
+    g.overrelax_theta(theta)
+    o.overrelax(theta, colour_of_sl=col)
+    np.testing.assert_allclose(g.spins(), o.spins(), atol=1e-5)
+    e, _ = g.energy()
+    assert e[0] == pytest.approx(e0, abs=1e-4)
+    g.overrelax_theta(None)  # reflection
+    o.overrelax(None, colour_of_sl=col)
+    np.testing.assert_allclose(g.spins(), o.spins(), atol=1e-5)
+
+
+def test_colour_classes():
+    g = pc.pyrochlore_system(2, J1=1.0, J2=0.1, J3=0.0, colouring=1)
+    n, col = g.colours()
+    assert n == 4 and (col == np.arange(16) % 4).all()
+    g = pc.pyrochlore_system(2, J1=1.0, J2=0.1, J3=0.05, colouring=1)
+    n, col = g.colours()
+    assert n == 16
+    g = pc.pyrochlore_system(2, J1=1.0, colouring=0)
+    n, col = g.colours()
+    assert n == 16 and (col == np.arange(16)).all()
+
+
+@pytest.mark.parametrize("colouring", [0, 1])
+@pytest.mark.parametrize("T", [0.3, 2.0])
+def test_sweeps_follow_oracle_mirror(colouring, T):
+    c = COUPLINGS[2]
+    seed = 12345
+    g, o = pair(3, c, seed=seed, colouring=colouring)
+    rng = np.random.default_rng(3)
+    g.set_spins(unit(rng, o.N))
+    o.set_spins(g.spins())
+    _, col = g.colours()
+    for sweep in range(3):
+        acc_g = g.sweep(T, 1, 1)[0]
+        acc_o = o.sweep_philox(T, seed, 0, sweep, col, n_overrelax=1, or_mode=0)
+        Sg = g.spins()
+        So = o.spins()
+        assert int(acc_g) == int(acc_o)
+        np.testing.assert_allclose(Sg, So, atol=1e-4)
+        o.set_spins(Sg)  # re-sync to FP32 state
+    assert g.sweep_counter() == 3
+
+
+def test_sweep_reflection_mode_follows_oracle():
+    c = COUPLINGS[1]
+    seed = 99
+    g, o = pair(2, c, seed=seed, overrelax_mode=1)
+    rng = np.random.default_rng(5)
+    g.set_spins(unit(rng, o.N))
+    o.set_spins(g.spins())
+    _, col = g.colours()
+    acc_g = g.sweep(0.7, 1, 2)[0]
+    acc_o = o.sweep_philox(0.7, seed, 0, 0, col, n_overrelax=2, or_mode=1)
+    assert int(acc_g) == int(acc_o)
+    np.testing.assert_allclose(g.spins(), o.spins(), atol=1e-4)
+
+
+def test_batched_replicas_are_independent_streams():
+    c = COUPLINGS[1]
+    g = pc.pyrochlore_system(2, seed=5, n_replicas=3, **c)
+    rng = np.random.default_rng(1)
+    S = unit(rng, g.N())
+    for r in range(3):
+        g.set_spins(S, r)
+    g.sweep([0.5, 0.5, 0.5], 2, 1)
+    o = oracle.System(2, seed=5, **c)
+    for r in range(3):
+        o.set_spins(S.astype(np.float32).astype(np.float64))
+        o.sweep_philox(0.5, 5, r, 0, np.arange(16), 1)
+        o.sweep_philox(0.5, 5, r, 1, np.arange(16), 1)
+        np.testing.assert_allclose(g.spins(r), o.spins(), atol=2e-4)
+    assert np.abs(g.spins(0) - g.spins(1)).max() > 0.1
+
+
+def test_spins_stay_normalised_over_many_sweeps():
+    g = pc.pyrochlore_system(4, J1=1.0, J2=0.1, J3=0.05, B=(0, 0, 0.3))
+    g.random_spins(3)
+    g.sweep(0.1, 200, 1)
+    S = g.spins()
+    assert np.abs(np.linalg.norm(S, axis=1) - 1).max() < 1e-5
+
+
+def test_random_spins_uniform_on_sphere():
+    g = pc.pyrochlore_system(8, J1=1.0)
+    g.random_spins(42)
+    S = g.spins()
+    assert np.abs(np.linalg.norm(S, axis=1) - 1).max() < 1e-5
+    assert np.abs(S.mean(axis=0)).max() < 0.02
+    assert np.abs((S ** 2).mean(axis=0) - 1 / 3).max() < 0.02
+
+
+CORR9 = ["xx", "yy", "zz", "xy", "xz", "yz", "yx", "zx", "zy"]
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 4, 6, 8, 12])
+def test_ssf_matches_oracle(L):
+    g, o = pair(L, COUPLINGS[0])
+    g.ssf_configure(CORR9, 1)
+    rng = np.random.default_rng(L)
+    for name, S in states(o, rng).items():
+        g.set_spins(S)
+        o.set_spins(g.spins())
+        ref = o.ssf(CORR9, mode=0)
+        got = g.ssf_current()
+        scale = np.abs(ref).max()
+        assert np.abs(got - ref).max() <= REL * scale, (name, np.abs(got - ref).max() / scale)
+
+
+def test_ssf_accumulates_like_ssf_manager():
+    g, o = pair(4, COUPLINGS[0])
+    g.ssf_configure(["xx", "yy", "zz", "xy"], 2)
+    rng = np.random.default_rng(0)
+    refs = []
+    for k in range(3):
+        S = unit(rng, o.N)
+        g.set_spins(S)
+        o.set_spins(g.spins())
+        refs.append(o.ssf(["xx", "yy", "zz", "xy"]))
+        g.ssf_sample([1])
+    s, q, n = g.ssf_read(1)
+    assert n == 3
+    ref_s = sum(refs)
+    ref_q = sum(r ** 2 for r in refs)
+    assert np.abs(s - ref_s).max() <= REL * np.abs(ref_s).max()
+    assert np.abs(q - ref_q).max() <= 3 * REL * np.abs(ref_q).max()
+    s0, _, n0 = g.ssf_read(0)
+    assert n0 == 0 and not s0.any()
+    g.ssf_clear(1)
+    s, _, n = g.ssf_read(1)
+    assert n == 0 and not s.any()
+
+
+def test_ssf_spiral_byhand_peaks():
+    # spiral_byhand (test/spiral_byhand.cpp:100-107): S = (0, cos q.r, sin q.r)
+    L = 4
+    g = pc.pyrochlore_system(L, J1=-1.0, split_J1=False)
+    g.ssf_configure(["xx", "yy", "zz"], 1)
+    pos, _ = g.positions()
+    Q = np.array([1, 2, 0])
+    qv = 2 * np.pi * Q / (8 * L)
+    ph = pos @ qv
+    S = np.stack([np.zeros(len(ph)), np.cos(ph), np.sin(ph)], axis=1)
+    g.set_spins(S)
+    out = g.ssf_current()
+    tot = out[1, :, 0] + out[2, :, 0]
+    k_of = lambda K: ((K[0] % L) * L + (K[1] % L)) * L + (K[2] % L)
+    N = g.N()
+    # the helix puts N^2/2 into each of +Q and -Q
+    assert tot[k_of(Q)] == pytest.approx(N * N / 2, rel=1e-5)
+    assert tot[k_of(-Q)] == pytest.approx(N * N / 2, rel=1e-5)
+    assert np.abs(out[0]).max() < 1e-3 * N
+    mask = np.ones_like(tot, bool)
+    mask[[k_of(Q), k_of(-Q)]] = False
+    assert np.abs(tot[mask]).max() < 1e-3 * N * N
+    # energy against the oracle with the same single-J1 spec
+    o = oracle.System(L, J1=-1.0, j1_mode=1)
+    o.set_spins(g.spins())
+    e, _ = g.energy()
+    assert e[0] == pytest.approx(o.energy(), abs=1e-5 * 96)
+
+
+def test_invalid_correlator_names_raise():
+    g = pc.pyrochlore_system(2, J1=1.0)
+    with pytest.raises(pc.InvalidArgument, match="unknown spin component"):
+        g.ssf_configure(["xq"], 1)
+    with pytest.raises(pc.InvalidArgument, match="2 chars"):
+        g.ssf_configure(["xyz"], 1)
+
+
+def test_duplicate_coupling_name_raises():
+    g = pc.System(2)
+    g.define_pyrochlore(1.0)
+    with pytest.raises(pc.InvalidArgument, match="unique"):
+        g.define_coupling("J2", [[], [], [], []], np.eye(3))

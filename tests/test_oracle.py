@@ -1,0 +1,225 @@
+"""CPU tests of the oracle (the FP64 restatement of the reference MC path)
+against the reference's own artefacts (tests/golden/) and analytic known
+answers derived from the reference code. No GPU."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _geo():
+    return json.load(open(os.path.join(GOLD, "geometry_tables.json")))
+
+
+def _sets(rows):
+    return sorted(tuple(r) for r in rows)
+
+
+def test_oracle_displacement_tables_match_reference_tables():
+    g = _geo()
+    s = oracle.System(2, J1=1.0, J2=0.5, J3=0.25, j1_mode=0)
+    pairs = ["01", "02", "03", "12", "13", "23"]
+    for k, pr in enumerate(pairs):
+        for p in range(4):
+            assert _sets(s.spec_displacements(k, p)) == _sets(g["nn1_pair_" + pr][p])
+    for spec, name in ((6, "nn2_dist"), (7, "nn3a_dist"), (8, "nn3b_dist")):
+        for p in range(4):
+            got = s.spec_displacements(spec, p)
+            assert len(got) == len(g[name][p])
+            assert _sets(got) == _sets(g[name][p])
+    s1 = oracle.System(2, j1_mode=1)
+    for p in range(4):
+        assert _sets(s1.spec_displacements(0, p)) == _sets(g["nn1_dist"][p])
+
+
+def test_oracle_cell_matches_reference_cell():
+    g = _geo()
+    s = oracle.System(1)
+    pos, sl = s.positions()
+    R = np.array(g["PyroCubicCell_R_fcc"])
+    link = np.array(g["PyroCubicCell_link_positions"])
+    for i in range(16):
+        f, p = divmod(int(sl[i]), 4)
+        assert (pos[i] == R[f] + link[p]).all()
+    assert (np.array(g["pyro"]) == link).all() and (np.array(g["fcc_Dy"]) == R).all()
+
+
+def test_xoshiro_restatement_matches_reference_header():
+    rows = json.load(open(os.path.join(GOLD, "xoshiro_streams.json")))["draws"]
+    by = {}
+    for r in rows:
+        by.setdefault((r["seed"], r["kind"]), []).append((r["index"], r["value"]))
+    assert len(by) == 18
+    for (seed, kind), vals in by.items():
+        vals = [v for _, v in sorted(vals)]
+        got = oracle.xoshiro_draws(seed, kind, len(vals))
+        if kind == 0:
+            assert [int(x) for x in got] == vals
+        else:
+            np.testing.assert_array_equal(got, np.array(vals))
+
+
+def test_philox_known_answers():
+    kat = json.load(open(os.path.join(GOLD, "philox_kat.json")))["vectors"]
+    for v in kat:
+        assert oracle.philox(v["ctr"], v["key"]).tolist() == v["out"]
+
+
+def _numpy_energy(pos, S, L, specs):
+    """Independent bond-sum energy per cubic cell from positions and the golden
+    displacement tables: E = 1/2 sum_i sum_{j in nb(i)} S_i . M_ij S_j - B.S."""
+    index = {tuple(p % (8 * L)): i for i, p in enumerate(pos)}
+    E = 0.0
+    for disp_by_p, J, pyro_of in specs:
+        for i, p in enumerate(pos):
+            pi = pyro_of[i]
+            for d in disp_by_p[pi]:
+                j = index[tuple((p + np.array(d)) % (8 * L))]
+                M = J if pi <= pyro_of[j] else J.T
+                E += 0.5 * S[i] @ M @ S[j]
+    return E / L ** 3
+
+
+@pytest.mark.parametrize("L", [1, 2, 3])
+def test_energy_matches_independent_bond_sum(L):
+    g = _geo()
+    rng = np.random.default_rng(L)
+    J1, J2, J3, Delta = 1.0, -0.3, 0.2, 0.6
+    s = oracle.System(L, J1=J1, J2=J2, J3=J3, Delta=Delta)
+    S = rng.normal(size=(s.N, 3))
+    S /= np.linalg.norm(S, axis=1, keepdims=True)
+    s.set_spins(S)
+    pos, sl = s.positions()
+    pyro = sl % 4
+    z = np.array(g["pyro"], dtype=float) / np.sqrt(3)
+    specs = []
+    for pr in ["01", "02", "03", "12", "13", "23"]:
+        mu, nu = int(pr[0]), int(pr[1])
+        M = J1 * (np.eye(3) + (Delta - 1) * np.outer(z[mu], z[nu]))
+        specs.append((g["nn1_pair_" + pr], M, pyro))
+    specs += [(g["nn2_dist"], J2 * np.eye(3), pyro), (g["nn3a_dist"], J3 * np.eye(3), pyro),
+              (g["nn3b_dist"], J3 * np.eye(3), pyro)]
+    assert s.energy() == pytest.approx(_numpy_energy(pos, S, L, specs), rel=1e-12, abs=1e-12)
+
+
+def test_ferromagnet_known_answer():
+    # 6 J1, 12 J2, 6+6 J3 neighbours per site, 16 sites per cell (MC.cpp:305-312)
+    J1, J2, J3, B = 1.3, -0.4, 0.25, np.array([0.1, -0.2, 0.7])
+    s = oracle.System(3, J1=J1, J2=J2, J3=J3, B=B)
+    n = np.array([0.48, 0.6, 0.64])
+    s.set_spins(np.tile(n, (s.N, 1)))
+    assert s.energy() == pytest.approx(48 * J1 + 96 * J2 + 96 * J3 - 16 * B @ n, rel=1e-13)
+
+
+def test_zero_tetrahedron_sum_state_energy():
+    # all-in-all-out: S = z_p on pyro_sl p, zero total spin on every tetrahedron:
+    # e = -16 J1 per cubic cell (8 tetrahedra x -2 J1)
+    g = _geo()
+    s = oracle.System(2, J1=0.7)
+    _, sl = s.positions()
+    z = np.array(g["pyro"], dtype=float) / np.sqrt(3)
+    s.set_spins(z[sl % 4])
+    assert s.energy() == pytest.approx(-16 * 0.7, rel=1e-13)
+
+
+def test_overrelaxation_preserves_energy():
+    s = oracle.System(2, J1=1.0, J2=0.1, J3=0.05, Delta=0.7, B=(0, 0, 0.5), seed=3)
+    s.random_spins(11)
+    e0 = s.energy()
+    rng = np.random.default_rng(0)
+    s.overrelax(rng.uniform(0, 2 * np.pi, s.N))
+    assert s.energy() == pytest.approx(e0, rel=1e-12)
+    # reflection: mirror_about_vector regularises |h|^2 by 1e-10 (MC.cpp:99),
+    # so it preserves energy and |S| to that level only
+    s.overrelax(None)
+    assert s.energy() == pytest.approx(e0, rel=1e-8)
+    assert np.allclose(np.linalg.norm(s.spins(), axis=1), 1.0, atol=1e-8)
+
+
+def test_local_field_is_energy_gradient():
+    s = oracle.System(2, J1=1.0, J2=0.2, J3=-0.1, Delta=0.5, B=(0.3, 0, 0), seed=1)
+    s.random_spins(5)
+    S = s.spins()
+    h = s.local_fields()
+    B = np.array([0.3, 0, 0])
+    eps = 1e-6
+    for i in [0, 17, 100]:
+        for a in range(3):
+            Sp = S.copy()
+            Sp[i, a] += eps
+            s.set_spins(Sp)
+            ep = s.energy()
+            Sp[i, a] -= 2 * eps
+            s.set_spins(Sp)
+            em = s.energy()
+            fd = (ep - em) / (2 * eps) * s.Nc
+            assert fd == pytest.approx(h[i, a] - B[a], abs=1e-7)
+    s.set_spins(S)
+
+
+def test_coupling_grads_match_finite_differences():
+    J = dict(J1=1.0, J2=0.2, J3=-0.1, Delta=0.5)
+    s = oracle.System(2, **J, seed=1)
+    s.random_spins(9)
+    S = s.spins()
+    G = s.coupling_grads()  # dE_total/dJ_spec
+    # d e/d J2 through the J2 spec only: E is linear in the spec matrix
+    E_of = lambda **kw: _sys_energy(S, **kw) * 8
+    eps = 1e-6
+    fd = (E_of(**{**J, "J2": J["J2"] + eps}) - E_of(**{**J, "J2": J["J2"] - eps})) / (2 * eps)
+    assert fd == pytest.approx(np.trace(G[6]), rel=1e-7)
+    fd3 = (E_of(**{**J, "J3": J["J3"] + eps}) - E_of(**{**J, "J3": J["J3"] - eps})) / (2 * eps)
+    assert fd3 == pytest.approx(np.trace(G[7]) + np.trace(G[8]), rel=1e-7)
+
+
+def _sys_energy(S, **kw):
+    s = oracle.System(2, **kw)
+    s.set_spins(S)
+    return s.energy()
+
+
+@pytest.mark.parametrize("L", [1, 2])
+def test_ssf_direct_equals_reference_sublattice_contraction(L):
+    s = oracle.System(L, seed=2)
+    s.random_spins(21)
+    corr = ["xx", "yy", "zz", "xy", "xz", "yz", "zx", "yx", "zy"]
+    a = s.ssf(corr, mode=0)
+    b = s.ssf(corr, mode=1)
+    np.testing.assert_allclose(a, b, atol=1e-10 * np.abs(a).max())
+
+
+def test_ssf_ferromagnet_k0():
+    s = oracle.System(2)
+    n = np.array([0.0, 0.6, 0.8])
+    s.set_spins(np.tile(n, (s.N, 1)))
+    S = s.ssf(["xx", "yy", "zz", "yz"])
+    N = s.N
+    assert S[1, 0, 0] == pytest.approx((N * 0.6) ** 2)
+    assert S[2, 0, 0] == pytest.approx((N * 0.8) ** 2)
+    assert S[3, 0, 0] == pytest.approx(N * N * 0.48)
+
+
+def test_T_profile_restatement():
+    T, idx = oracle.T_profile(10.0, 0.05, [1.0, 0.1, 0.05], 100)
+    assert len(T) == 103
+    assert list(T[idx]) == [1.0, 0.1, 0.05]
+    assert all(np.diff(T) <= 0)
+    f = (0.05 / 10.0) ** (1 / 100)
+    sweep = [10.0 * f ** i for i in range(100)]
+    assert np.allclose(sorted(set(T) - {1.0, 0.1, 0.05}, reverse=True), sweep, rtol=1e-12)
+    assert min(sweep) > 0.05  # T_cold itself is not reached (cli_bits.hpp:254-259)
+
+
+def test_anneal_runs_and_cools():
+    s = oracle.System(2, J1=1.0, seed=7)
+    s.random_spins(3)
+    T, e, ssum, ssq = s.anneal(5.0, 0.05, [0.5], 20, 4, 4, 3, ["zz"])
+    assert len(e) == 21
+    assert e[-1] < e[0]
+    assert ssum.shape == (1, 1, 8, 2)
+    assert (ssq[..., 0] >= 0).all()
