@@ -91,6 +91,11 @@ int pc_set_overrelax_mode(pc_system* sys, int mode);
  * nonzero bond share a class: 4 pyro_sl classes when J3 = 0); a different,
  * equally valid visiting order with fewer launches. Call before setup. */
 int pc_set_colouring(pc_system* sys, int mode);
+/* Kernel path: 0 (default) uses the structured pyrochlore kernels whenever the
+ * couplings fit the fixed J1/J2/J3a/J3b neighbour structure, 1 forces the
+ * generic bond-table kernels. Reports the path in use via pc_kernel_path. */
+int pc_set_kernel_path(pc_system* sys, int force_generic);
+int pc_kernel_path(pc_system* sys, int* structured);
 /* MC_runner::setup_lattice (src/MC.cpp:15-52): builds the per-sublattice bond
  * shells, the colour classes and uploads them. Must follow all couplings. */
 int pc_setup_lattice(pc_system* sys);

@@ -40,6 +40,8 @@ _SIGNATURES = {
     "pc_set_T_ref": (_I, [_P, _D]),
     "pc_set_overrelax_mode": (_I, [_P, _I]),
     "pc_set_colouring": (_I, [_P, _I]),
+    "pc_set_kernel_path": (_I, [_P, _I]),
+    "pc_kernel_path": (_I, [_P, _IP]),
     "pc_setup_lattice": (_I, [_P]),
     "pc_num_replicas": (_I, [_P, _IP]),
     "pc_num_spins": (_I, [_P, _I, _I64P]),

@@ -101,6 +101,7 @@ class EnergyFunction(torch.autograd.Function):
         e, _ = system.energy()
         ctx.system = system
         ctx.has_params = params is not None
+        ctx.params_device = params.device if params is not None else None
         ctx.save_for_backward(spins)
         return torch.as_tensor(e, dtype=torch.float64, device=spins.device)
 
@@ -115,7 +116,7 @@ class EnergyFunction(torch.autograd.Function):
         gp = None
         if ctx.has_params:
             gp = torch.as_tensor(_param_grads(system, gJ.reshape(system.R, -1, 3, 3), gB).sum(axis=0),
-                                 dtype=torch.float64, device=spins.device)
+                                 dtype=torch.float64, device=ctx.params_device)
         return grad_spins, gp, None
 
 

@@ -38,7 +38,8 @@ using Tile = int4;
 struct ReplicaDev {
     int32_t L;
     int32_t Nc;
-    int64_t off;  // offset of the replica's spins in the global float4 array
+    int64_t off;    // offset of the replica's spins in the global float4 array
+    uint64_t divL;  // fast-division magic for L (pyro_struct.cuh)
 };
 
 // ---------------------------------------------------------------- Philox

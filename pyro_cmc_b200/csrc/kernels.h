@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "pyro_struct.cuh"
 
 namespace pc {
 
@@ -29,6 +30,8 @@ struct PassArgs {
     int or_pass;              // overrelaxation pass index (draw 2 + or_pass)
     const double* theta;      // kOverrelaxTheta: per-site angle of replica theta_replica (device)
     int theta_replica;
+    int structured;  // 1: couplings fit the pyrochlore structure, use `mats`
+    PyroMats mats;
 };
 
 void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st);
@@ -41,6 +44,8 @@ struct EnergyArgs {
     int n_tiles;
     float B[3];
     double* partial;  // [n_tiles][4]: sum (0.5 S.h - S.B), sum S
+    int structured;
+    PyroMats mats;
 };
 void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st);
 // Sums the tile partials of each replica in tile order: e[r] = sum/Nc, mag[r][3].

@@ -11,6 +11,8 @@
 // are staged once per CTA in shared memory; CTAs loop over tiles.
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -51,14 +53,177 @@ __device__ __forceinline__ float3 local_field(const float4* __restrict__ S, cons
     return make_float3(hx, hy, hz);
 }
 
+// Structured local field (compile-time neighbour offsets of sublattice SL,
+// pyro_struct.cuh): the wrapped neighbour coordinates are formed once, each
+// of the 30 neighbours is one add-and-load with offsets fixed at compile time,
+// groups with a zero matrix are skipped. Same sum as local_field() with the
+// shells grouped per target.
+struct Coords {
+    int x[3], y[3], z[3];  // wrapped cx-1, cx, cx+1 (y, z premultiplied by L, L^2)
+};
+
+template <int D>
+__device__ __forceinline__ int pick(const int (&v)[3]) {
+    if constexpr (D < 0)
+        return v[0];
+    else if constexpr (D > 0)
+        return v[2];
+    else
+        return v[1];
+}
+
+template <int SL, int E>
+__device__ __forceinline__ float4 load_nb(const float4* __restrict__ S, int Nc, const Coords& c) {
+    constexpr int s2 = nb_sl(SL, E), dx = nb_dx(SL, E), dy = nb_dy(SL, E), dz = nb_dz(SL, E);
+    return __ldg(&S[s2 * Nc + pick<dx>(c.x) + pick<dy>(c.y) + pick<dz>(c.z)]);
+}
+
+template <int SL, int G, int... K>
+__device__ __forceinline__ float3 group_sum(const float4* __restrict__ S, int Nc, const Coords& c,
+                                            std::integer_sequence<int, K...>) {
+    constexpr int B = grp_begin(SL, G);
+    const float4 v[sizeof...(K)] = {load_nb<SL, B + K>(S, Nc, c)...};
+    float3 t = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < int(sizeof...(K)); ++k) {
+        t.x += v[k].x;
+        t.y += v[k].y;
+        t.z += v[k].z;
+    }
+    return t;
+}
+
+template <int SL, int G>
+__device__ __forceinline__ void add_group(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
+                                          const PyroMats& mats) {
+    if (mats.active[SL] & (1u << G)) {
+        const float3 t = group_sum<SL, G>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
+        const float* J = mats.M[SL][G];
+        h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
+        h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
+        h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+    }
+}
+
+__device__ __forceinline__ Coords cell_coords(int cell, int L, uint64_t divL) {
+    const int q = fdiv(cell, divL);  // cy + L*cz
+    const int cx = cell - q * L;
+    const int cz = fdiv(q, divL);
+    const int cy = q - cz * L;
+    const int LL = L * L;
+    Coords c;
+    c.x[0] = cx == 0 ? L - 1 : cx - 1;
+    c.x[1] = cx;
+    c.x[2] = cx == L - 1 ? 0 : cx + 1;
+    c.y[0] = L * (cy == 0 ? L - 1 : cy - 1);
+    c.y[1] = L * cy;
+    c.y[2] = L * (cy == L - 1 ? 0 : cy + 1);
+    c.z[0] = LL * (cz == 0 ? L - 1 : cz - 1);
+    c.z[1] = LL * cz;
+    c.z[2] = LL * (cz == L - 1 ? 0 : cz + 1);
+    return c;
+}
+
+template <int SL>
+__device__ __forceinline__ float3 struct_field(const float4* __restrict__ S, const PyroMats& mats, int cell,
+                                               int L, int Nc, uint64_t divL) {
+    const Coords c = cell_coords(cell, L, divL);
+    float3 h = make_float3(0.f, 0.f, 0.f);
+    add_group<SL, 0>(h, S, Nc, c, mats);
+    add_group<SL, 1>(h, S, Nc, c, mats);
+    add_group<SL, 2>(h, S, Nc, c, mats);
+    add_group<SL, 3>(h, S, Nc, c, mats);
+    add_group<SL, 4>(h, S, Nc, c, mats);
+    add_group<SL, 5>(h, S, Nc, c, mats);
+    return h;
+}
+
+// The move at site i with local field h (global field not yet subtracted):
+// Metropolis (local_Metropolis, src/MC.cpp:111-130) or one overrelaxation
+// (overrelax_all, src/MC.cpp:145-153; mirror_about_vector :98-100). Returns
+// whether a Metropolis proposal was accepted.
 template <int MODE>
-__global__ void __launch_bounds__(512) colour_pass_kernel(const PassArgs a) {
+__device__ __forceinline__ bool apply_move(const PassArgs& a, float4* S, size_t i, float3 h, int r, uint64_t sweep) {
+    const float4 s0 = S[i];
+    h.x -= a.B[0];
+    h.y -= a.B[1];
+    h.z -= a.B[2];
+    if (MODE == kMetropolis) {
+        const double T = a.T_rep[r];
+        const float sigma = sqrtf(float(T) * a.inv_T_ref);
+        const float invT = float(1.0 / T);
+        const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
+        // Box-Muller on the top 24 bits of words (0,1) and (2,3)
+        const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
+        const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
+        float s_a, c_a, s_b, c_b;
+        sincospif(2.f * u24(w.y), &s_a, &c_a);
+        sincospif(2.f * u24(w.w), &s_b, &c_b);
+        float nx = s0.x + sigma * (r0 * c_a);
+        float ny = s0.y + sigma * (r0 * s_a);
+        float nz = s0.z + sigma * (r1 * c_b);
+        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+        nx *= inv;
+        ny *= inv;
+        nz *= inv;
+        const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
+        if (dE < 0.f || u24_lowbytes(w) < __expf(-dE * invT)) {
+            S[i] = make_float4(nx, ny, nz, 0.f);
+            return true;
+        }
+        return false;
+    }
+    const float n2 = h.x * h.x + h.y * h.y + h.z * h.z;
+    if (!(n2 > 1e-30f)) return false;
+    float nx, ny, nz;
+    const float av = h.x * s0.x + h.y * s0.y + h.z * s0.z;
+    if (MODE == kOverrelaxReflect) {
+        const float f = 2.f * av / (n2 + 1e-10f);
+        nx = -s0.x + f * h.x;
+        ny = -s0.y + f * h.y;
+        nz = -s0.z + f * h.z;
+    } else {
+        // rotate_about_vector (src/MC.cpp:102-109), theta = 2*pi*U
+        float sn, cs;
+        if (MODE == kOverrelaxTheta) {
+            sincosf(float(a.theta[i]), &sn, &cs);
+        } else {
+            const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
+            sincospif(2.f * u24(w.x), &sn, &cs);
+        }
+        const float f = (1.f - cs) * av / n2;
+        const float g = sn * rsqrtf(n2);
+        nx = cs * s0.x + f * h.x + g * (h.y * s0.z - h.z * s0.y);
+        ny = cs * s0.y + f * h.y + g * (h.z * s0.x - h.x * s0.z);
+        nz = cs * s0.z + f * h.z + g * (h.x * s0.y - h.y * s0.x);
+    }
+    // renormalise: keeps FP32 rounding from drifting |S| away from 1
+    const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+    S[i] = make_float4(nx * inv, ny * inv, nz * inv, 0.f);
+    return false;
+}
+
+__device__ __forceinline__ void count_accepted(const PassArgs& a, bool accepted, int r, unsigned int* warp_acc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned int c = __popc(__ballot_sync(0xffffffffu, accepted));
+    if (lane == 0) warp_acc[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int tot = 0;
+        for (int wi = 0; wi < int(blockDim.x >> 5); ++wi) tot += warp_acc[wi];
+        if (tot) atomicAdd(a.acc + r, (unsigned long long)tot);
+    }
+    __syncthreads();
+}
+
+// Generic colour pass: bond tables (any coupling set) staged in shared memory.
+template <int MODE>
+__global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant__ PassArgs a) {
     __shared__ SlTable tab[4];
     __shared__ unsigned int warp_acc[16];
     stage_tables(tab, a.tables, a.n_tab, a.tab_sl);
     __syncthreads();
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         const Tile tile = a.tiles[t];
         const int r = tile.x;
@@ -66,90 +231,77 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const PassArgs a) {
         const ReplicaDev rep = a.reps[r];
         const int L = rep.L, Nc = rep.Nc;
         float4* S = a.spins + rep.off;
-        const int cell = tile.z + int(threadIdx.x);
         bool accepted = false;
         if (int(threadIdx.x) < tile.w) {
+            const int cell = tile.z + int(threadIdx.x);
             const int cx = cell % L, cy = (cell / L) % L, cz = cell / (L * L);
-            const size_t i = size_t(sl) * Nc + cell;
-            const float4 s0 = S[i];
-            float3 h = local_field(S, tab[k], cx, cy, cz, L, Nc);
-            h.x -= a.B[0];
-            h.y -= a.B[1];
-            h.z -= a.B[2];
-            if (MODE == kMetropolis) {
-                const double T = a.T_rep[r];
-                const float sigma = sqrtf(float(T) * a.inv_T_ref);
-                const float invT = float(1.0 / T);
-                const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
-                // Box-Muller on the top 24 bits of words (0,1) and (2,3)
-                const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
-                const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
-                float s_a, c_a, s_b, c_b;
-                sincospif(2.f * u24(w.y), &s_a, &c_a);
-                sincospif(2.f * u24(w.w), &s_b, &c_b);
-                float nx = s0.x + sigma * (r0 * c_a);
-                float ny = s0.y + sigma * (r0 * s_a);
-                float nz = s0.z + sigma * (r1 * c_b);
-                const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
-                nx *= inv;
-                ny *= inv;
-                nz *= inv;
-                const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
-                if (dE < 0.f || u24_lowbytes(w) < __expf(-dE * invT)) {
-                    S[i] = make_float4(nx, ny, nz, 0.f);
-                    accepted = true;
-                }
-            } else {
-                const float n2 = h.x * h.x + h.y * h.y + h.z * h.z;
-                if (n2 > 1e-30f) {
-                    float nx, ny, nz;
-                    const float av = h.x * s0.x + h.y * s0.y + h.z * s0.z;
-                    if (MODE == kOverrelaxReflect) {
-                        // mirror_about_vector (src/MC.cpp:98-100)
-                        const float f = 2.f * av / (n2 + 1e-10f);
-                        nx = -s0.x + f * h.x;
-                        ny = -s0.y + f * h.y;
-                        nz = -s0.z + f * h.z;
-                    } else {
-                        // rotate_about_vector (src/MC.cpp:102-109), theta = 2*pi*U
-                        float sn, cs;
-                        if (MODE == kOverrelaxTheta) {
-                            sincosf(float(a.theta[i]), &sn, &cs);
-                        } else {
-                            const uint4 w =
-                                site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
-                            sincospif(2.f * u24(w.x), &sn, &cs);
-                        }
-                        const float f = (1.f - cs) * av / n2;
-                        const float g = sn * rsqrtf(n2);
-                        const float cx_ = h.y * s0.z - h.z * s0.y;
-                        const float cy_ = h.z * s0.x - h.x * s0.z;
-                        const float cz_ = h.x * s0.y - h.y * s0.x;
-                        nx = cs * s0.x + f * h.x + g * cx_;
-                        ny = cs * s0.y + f * h.y + g * cy_;
-                        nz = cs * s0.z + f * h.z + g * cz_;
-                    }
-                    // renormalise: keeps FP32 rounding from drifting |S| away from 1
-                    const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
-                    S[i] = make_float4(nx * inv, ny * inv, nz * inv, 0.f);
-                }
-            }
+            const float3 h = local_field(S, tab[k], cx, cy, cz, L, Nc);
+            accepted = apply_move<MODE>(a, S, size_t(sl) * Nc + cell, h, r, sweep);
         }
-        if (MODE == kMetropolis) {
-            const unsigned int c = __popc(__ballot_sync(0xffffffffu, accepted));
-            if (lane == 0) warp_acc[warp] = c;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                unsigned int tot = 0;
-                for (int wi = 0; wi < int(blockDim.x >> 5); ++wi) tot += warp_acc[wi];
-                if (tot) atomicAdd(a.acc + r, (unsigned long long)tot);
-            }
-            __syncthreads();
+        if (MODE == kMetropolis) count_accepted(a, accepted, r, warp_acc);
+    }
+}
+
+template <int MODE, int SL>
+__device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const ReplicaDev& rep, int r, int cell,
+                                            uint64_t sweep) {
+    const float3 h = struct_field<SL>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
+    return apply_move<MODE>(a, S, size_t(SL) * rep.Nc + cell, h, r, sweep);
+}
+
+#define PC_SL_SWITCH(sl, CALL) \
+    switch (sl) {              \
+        case 0: CALL(0); break;   \
+        case 1: CALL(1); break;   \
+        case 2: CALL(2); break;   \
+        case 3: CALL(3); break;   \
+        case 4: CALL(4); break;   \
+        case 5: CALL(5); break;   \
+        case 6: CALL(6); break;   \
+        case 7: CALL(7); break;   \
+        case 8: CALL(8); break;   \
+        case 9: CALL(9); break;   \
+        case 10: CALL(10); break; \
+        case 11: CALL(11); break; \
+        case 12: CALL(12); break; \
+        case 13: CALL(13); break; \
+        case 14: CALL(14); break; \
+        case 15: CALL(15); break; \
+        default: break;           \
+    }
+
+// Structured colour pass: pyrochlore neighbour offsets fixed at compile time,
+// coupling matrices per (sublattice, group) in the kernel parameters.
+template <int MODE>
+__global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant__ PassArgs a) {
+    __shared__ unsigned int warp_acc[8];
+    const uint64_t sweep = *a.sweep_base + a.sweep_offset;
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const Tile tile = a.tiles[t];
+        const int r = tile.x, sl = tile.y & 0xff;
+        const ReplicaDev rep = a.reps[r];
+        float4* S = a.spins + rep.off;
+        bool accepted = false;
+        if (int(threadIdx.x) < tile.w) {
+            const int cell = tile.z + int(threadIdx.x);
+#define PC_CALL(K) accepted = struct_site<MODE, K>(a, S, rep, r, cell, sweep)
+            PC_SL_SWITCH(sl, PC_CALL)
+#undef PC_CALL
         }
+        if (MODE == kMetropolis) count_accepted(a, accepted, r, warp_acc);
     }
 }
 
 void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st) {
+    if (a.structured && threads <= 256) {
+        switch (mode) {
+            case kMetropolis: struct_pass_kernel<kMetropolis><<<grid, threads, 0, st>>>(a); break;
+            case kOverrelaxRotate: struct_pass_kernel<kOverrelaxRotate><<<grid, threads, 0, st>>>(a); break;
+            case kOverrelaxReflect: struct_pass_kernel<kOverrelaxReflect><<<grid, threads, 0, st>>>(a); break;
+            case kOverrelaxTheta: struct_pass_kernel<kOverrelaxTheta><<<grid, threads, 0, st>>>(a); break;
+        }
+        return;
+    }
     switch (mode) {
         case kMetropolis: colour_pass_kernel<kMetropolis><<<grid, threads, 0, st>>>(a); break;
         case kOverrelaxRotate: colour_pass_kernel<kOverrelaxRotate><<<grid, threads, 0, st>>>(a); break;
@@ -190,7 +342,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
 // Energy terms per tile (total_energy_per_unit_cell, src/MC.cpp:305-312):
 // sum_i 0.5 S_i.h_i - S_i.B, plus sum_i S_i. Every sublattice of every
 // replica; tables staged per tile (one sublattice per tile).
-__global__ void __launch_bounds__(512) energy_partials_kernel(const EnergyArgs a) {
+__global__ void __launch_bounds__(512) energy_partials_kernel(const __grid_constant__ EnergyArgs a) {
     __shared__ SlTable tab;
     __shared__ double red[4 * 32];
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
@@ -220,12 +372,47 @@ __global__ void __launch_bounds__(512) energy_partials_kernel(const EnergyArgs a
     }
 }
 
+template <int SL>
+__device__ __forceinline__ float3 struct_field_e(const EnergyArgs& a, const float4* S, const ReplicaDev& rep, int cell) {
+    return struct_field<SL>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
+}
+
+__global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constant__ EnergyArgs a) {
+    __shared__ double red[4 * 32];
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+        const Tile tile = a.tiles[t];
+        const int r = tile.x, sl = tile.y & 0xff;
+        const ReplicaDev rep = a.reps[r];
+        const float4* S = a.spins + rep.off;
+        double v[4] = {0, 0, 0, 0};
+        if (int(threadIdx.x) < tile.w) {
+            const int cell = tile.z + int(threadIdx.x);
+            const float4 s0 = S[size_t(sl) * rep.Nc + cell];
+            float3 h = make_float3(0.f, 0.f, 0.f);
+#define PC_CALL(K) h = struct_field_e<K>(a, S, rep, cell)
+            PC_SL_SWITCH(sl, PC_CALL)
+#undef PC_CALL
+            v[0] = 0.5 * double(s0.x * h.x + s0.y * h.y + s0.z * h.z) -
+                   double(s0.x * a.B[0] + s0.y * a.B[1] + s0.z * a.B[2]);
+            v[1] = s0.x;
+            v[2] = s0.y;
+            v[3] = s0.z;
+        }
+        block_sum<4>(v, red);
+        if (threadIdx.x == 0)
+            for (int j = 0; j < 4; ++j) a.partial[size_t(t) * 4 + j] = v[j];
+    }
+}
+
 void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = a.n_tiles < sms * 4 ? a.n_tiles : sms * 4;
-    energy_partials_kernel<<<grid, threads, 0, st>>>(a);
+    if (a.structured && threads <= 256)
+        energy_struct_kernel<<<grid, threads, 0, st>>>(a);
+    else
+        energy_partials_kernel<<<grid, threads, 0, st>>>(a);
 }
 
 // One warp per replica: fixed-order sum of its tile partials (deterministic).

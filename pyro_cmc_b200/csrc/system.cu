@@ -21,6 +21,7 @@
 #include "../../include/pyrocmc.h"
 #include "common.cuh"
 #include "kernels.h"
+#include "pyro_struct.cuh"
 
 using pc::NbEntry;
 using pc::ReplicaDev;
@@ -133,6 +134,9 @@ struct pc_system {
 
     SlTable tab_active[16];
     SlTable tab_full[16];
+    bool structured = false;  // couplings fit the compile-time pyrochlore structure
+    bool force_generic = false;
+    pc::PyroMats mats;
     int n_colours = 0;
     int colour_of_sl[16];
     std::vector<std::vector<int>> colour_sls;
@@ -312,6 +316,58 @@ int build_tables(pc_system* s, bool keep_zero, SlTable* out) {
     return PC_OK;
 }
 
+// Maps the coupling specs onto the structural neighbour groups of
+// pyro_struct.cuh: for every sublattice and each of its 30 structural
+// neighbours, the effective matrix is the sum over specs containing that
+// displacement of J (source side) or J^T (target side), exactly the matrices
+// setup_lattice would attach. If every spec displacement is structural and
+// each group carries one matrix, the structured kernels apply.
+void build_struct(pc_system* s) {
+    s->structured = !s->force_generic;
+    std::memset(&s->mats, 0, sizeof(s->mats));
+    for (int sl = 0; sl < 16 && s->structured; ++sl) {
+        const pc::SStruct T = pc::make_struct(sl);
+        const int p = sl % 4;
+        const auto r = r_sl(sl);
+        double E[pc::kStructNb][9] = {};
+        for (const auto& c : s->specs)
+            for (const auto& v : c.rel[p]) {
+                const int g = pc::cs_group(sl, int(v[0]), int(v[1]), int(v[2]));
+                if (std::llabs(v[0]) > 4 || std::llabs(v[1]) > 4 || std::llabs(v[2]) > 4 || g < 0) {
+                    s->structured = false;
+                    break;
+                }
+                const std::array<int64_t, 3> x = {r[0] + v[0], r[1] + v[1], r[2] + v[2]};
+                const int sl2 = sl_at(x);
+                int e = -1;
+                for (int k = 0; k < pc::kStructNb; ++k) {
+                    const auto r2 = r_sl(T.nb[k].sl);
+                    if (T.nb[k].sl == sl2 && 8 * T.nb[k].dx + r2[0] == x[0] && 8 * T.nb[k].dy + r2[1] == x[1] &&
+                        8 * T.nb[k].dz + r2[2] == x[2])
+                        e = k;
+                }
+                if (e < 0) {
+                    s->structured = false;
+                    break;
+                }
+                const double* M = (p <= sl2 % 4) ? c.J : c.Jt;
+                for (int i = 0; i < 9; ++i) E[e][i] += M[i];
+            }
+        if (!s->structured) break;
+        for (int g = 0; g < pc::kGroups; ++g) {
+            const int b = T.gbegin[g], e1 = T.gbegin[g + 1];
+            bool nonzero = false;
+            for (int k = b; k < e1; ++k)
+                for (int i = 0; i < 9; ++i) {
+                    if (E[k][i] != E[b][i]) s->structured = false;
+                    nonzero = nonzero || E[k][i] != 0.0;
+                }
+            for (int i = 0; i < 9; ++i) s->mats.M[sl][g][i] = float(E[b][i]);
+            if (nonzero) s->mats.active[sl] |= 1u << g;
+        }
+    }
+}
+
 // Colour classes from the active bonds: sublattices joined by a nonzero bond
 // never share a class. Greedy in sublattice order, at most 4 sublattices per
 // class. With J1/J2 only this yields the 4 pyro_sl classes; J3 (which joins
@@ -410,6 +466,8 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.n_tiles = s->n_colour_tiles[size_t(colour)];
     a.acc = s->d_acc.p;
     a.or_pass = or_pass;
+    a.structured = s->structured ? 1 : 0;
+    a.mats = s->mats;
     return a;
 }
 
@@ -519,6 +577,8 @@ int enqueue_energy(pc_system* s) {
     a.n_tiles = s->n_all_tiles;
     for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
     a.partial = s->d_partial.p;
+    a.structured = s->structured ? 1 : 0;
+    a.mats = s->mats;
     pc::launch_energy_partials(a, s->threads, s->stream);
     PC_LAUNCH_CK();
     pc::launch_energy_finalize(s->d_partial.p, s->d_tile_begin.p, s->d_tile_end.p, s->d_reps.p, s->R, s->d_e.p,
@@ -615,7 +675,8 @@ int pc_create(int n_replicas, const int32_t* L, uint64_t seed, pc_system** out) 
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     std::vector<ReplicaDev> reps(static_cast<size_t>(n_replicas));
-    for (int r = 0; r < n_replicas; ++r) reps[size_t(r)] = {L[r], int32_t(s->Nc(r)), s->off[size_t(r)]};
+    for (int r = 0; r < n_replicas; ++r)
+        reps[size_t(r)] = {L[r], int32_t(s->Nc(r)), s->off[size_t(r)], pc::fastdiv_magic(L[r])};
     if (e == cudaSuccess) e = s->d_reps.alloc(size_t(n_replicas));
     if (e == cudaSuccess) e = cudaMemcpy(s->d_reps.p, reps.data(), sizeof(ReplicaDev) * reps.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = s->d_spins.alloc(size_t(s->N_tot));
@@ -691,6 +752,7 @@ int pc_set_coupling_matrix(pc_system* sys, int spec, const double* J) {
     const int old_colours = sys->n_colours;
     rc = build_colours(sys);
     if (rc) return rc;
+    build_struct(sys);
     PC_CK(cudaStreamSynchronize(sys->stream));
     PC_CK(cudaMemcpy(sys->d_tab_active.p, sys->tab_active, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
     PC_CK(cudaMemcpy(sys->d_tab_full.p, sys->tab_full, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
@@ -729,6 +791,22 @@ int pc_set_overrelax_mode(pc_system* sys, int mode) {
     return PC_OK;
 }
 
+int pc_set_kernel_path(pc_system* sys, int force_generic) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    sys->force_generic = force_generic != 0;
+    if (sys->ready) build_struct(sys);
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_kernel_path(pc_system* sys, int* structured) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    *structured = sys->structured ? 1 : 0;
+    return PC_OK;
+}
+
 int pc_set_colouring(pc_system* sys, int mode) {
     int rc = check_sys(sys, false);
     if (rc) return rc;
@@ -749,6 +827,7 @@ int pc_setup_lattice(pc_system* sys) {
     if (rc) return rc;
     rc = build_colours(sys);
     if (rc) return rc;
+    build_struct(sys);
     PC_CK(sys->d_tab_active.alloc(16));
     PC_CK(sys->d_tab_full.alloc(16));
     PC_CK(cudaMemcpy(sys->d_tab_active.p, sys->tab_active, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));

@@ -157,6 +157,16 @@ class System:
         reference's visiting order); 1: fewest classes."""
         call("pc_set_colouring", self._h, int(mode))
 
+    def set_kernel_path(self, force_generic: bool):
+        """Force the generic bond-table kernels (True) or allow the structured
+        pyrochlore kernels (False, default)."""
+        call("pc_set_kernel_path", self._h, int(bool(force_generic)))
+
+    def structured(self) -> bool:
+        v = C.c_int(0)
+        call("pc_kernel_path", self._h, C.byref(v))
+        return bool(v.value)
+
     def setup_lattice(self):
         call("pc_setup_lattice", self._h)
 
@@ -365,10 +375,11 @@ class System:
 
 
 def pyrochlore_system(L, J1=1.0, J2=0.0, J3=0.0, Delta=1.0, B=(0.0, 0.0, 0.0), T_ref=1.0, seed=0,
-                      n_replicas=None, split_J1=True, overrelax_mode=0, colouring=0) -> System:
+                      n_replicas=None, split_J1=True, overrelax_mode=0, colouring=0, generic=False) -> System:
     """build_J1J2J3_h (include/cli_bits.hpp:144-207) on the GPU engine."""
     s = System(L, seed=seed, n_replicas=n_replicas)
     s.set_colouring(colouring)
+    s.set_kernel_path(generic)
     s.define_pyrochlore(J1, J2, J3, Delta, split_J1=split_J1)
     s.set_global_field(B)
     s.set_T_ref(T_ref)

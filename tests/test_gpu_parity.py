@@ -26,6 +26,7 @@ COUPLINGS = [
 
 def pair(L, c, seed=0, colouring=0, **kw):
     g = pc.pyrochlore_system(L, seed=seed, colouring=colouring, **c, **kw)
+    assert g.structured() != bool(kw.get("generic", False))
     o = oracle.System(L, seed=seed, **c)
     return g, o
 
@@ -64,10 +65,11 @@ def test_positions_match_oracle():
     np.testing.assert_array_equal(sg, so)
 
 
+@pytest.mark.parametrize("generic", [False, True])
 @pytest.mark.parametrize("L", [1, 2, 4, 8])
 @pytest.mark.parametrize("ci", range(len(COUPLINGS)))
-def test_energy_and_local_field(L, ci):
-    g, o = pair(L, COUPLINGS[ci])
+def test_energy_and_local_field(L, ci, generic):
+    g, o = pair(L, COUPLINGS[ci], generic=generic)
     rng = np.random.default_rng(100 * L + ci)
     for name, S in states(o, rng).items():
         o.set_spins(S)
@@ -108,12 +110,23 @@ def test_overrelax_pass_with_given_angles(colouring, ci):
     e0 = o.energy()
     g.overrelax_theta(theta)
     o.overrelax(theta, colour_of_sl=col)
-    np.testing.assert_allclose(g.spins(), o.spins(), atol=1e-5)
+    _close_fp32(g.spins(), o.spins())
     e, _ = g.energy()
     assert e[0] == pytest.approx(e0, abs=1e-4)
     g.overrelax_theta(None)  # reflection
     o.overrelax(None, colour_of_sl=col)
-    np.testing.assert_allclose(g.spins(), o.spins(), atol=1e-5)
+    _close_fp32(g.spins(), o.spins())
+
+
+def _close_fp32(a, b):
+    """One FP32 overrelaxation pass against FP64: the rotation axis is the
+    local field, a sum of up to 30 unit vectors in FP32 (error ~1e-6 of the
+    sum's scale); where those nearly cancel (|h| << 1) the axis direction, and
+    with it the rotated spin, carries a larger relative error. Bound: 99.5% of
+    components within 1e-5, all within 2e-4."""
+    d = np.abs(a - b)
+    assert np.mean(d <= 1e-5) >= 0.995, np.sort(d.ravel())[-10:]
+    assert d.max() <= 2e-4
 
 
 def test_colour_classes():
@@ -128,12 +141,13 @@ def test_colour_classes():
     assert n == 16 and (col == np.arange(16)).all()
 
 
+@pytest.mark.parametrize("generic", [False, True])
 @pytest.mark.parametrize("colouring", [0, 1])
 @pytest.mark.parametrize("T", [0.3, 2.0])
-def test_sweeps_follow_oracle_mirror(colouring, T):
+def test_sweeps_follow_oracle_mirror(colouring, T, generic):
     c = COUPLINGS[2]
     seed = 12345
-    g, o = pair(3, c, seed=seed, colouring=colouring)
+    g, o = pair(3, c, seed=seed, colouring=colouring, generic=generic)
     rng = np.random.default_rng(3)
     g.set_spins(unit(rng, o.N))
     o.set_spins(g.spins())
@@ -210,7 +224,10 @@ def test_ssf_matches_oracle(L):
         o.set_spins(g.spins())
         ref = o.ssf(CORR9, mode=0)
         got = g.ssf_current()
-        scale = np.abs(ref).max()
+        # relative to the largest |S(q)|, and never below N (the size of S(q)
+        # of an uncorrelated state): states such as all-in-all-out have
+        # S(q) = 0 on the whole grid, where only an absolute bound means anything
+        scale = max(np.abs(ref).max(), o.N)
         assert np.abs(got - ref).max() <= REL * scale, (name, np.abs(got - ref).max() / scale)
 
 
@@ -253,12 +270,13 @@ def test_ssf_spiral_byhand_peaks():
     tot = out[1, :, 0] + out[2, :, 0]
     k_of = lambda K: ((K[0] % L) * L + (K[1] % L)) * L + (K[2] % L)
     N = g.N()
-    # the helix puts N^2/2 into each of +Q and -Q
+    # the helix puts N^2/2 at q = +Q; q = -Q is not on the K in [0,L)^3 grid
+    # (K = -Q mod L differs from -Q by a vector that is not a reciprocal
+    # vector of the site positions, so the sublattice phases do not repeat)
     assert tot[k_of(Q)] == pytest.approx(N * N / 2, rel=1e-5)
-    assert tot[k_of(-Q)] == pytest.approx(N * N / 2, rel=1e-5)
     assert np.abs(out[0]).max() < 1e-3 * N
     mask = np.ones_like(tot, bool)
-    mask[[k_of(Q), k_of(-Q)]] = False
+    mask[k_of(Q)] = False
     assert np.abs(tot[mask]).max() < 1e-3 * N * N
     # energy against the oracle with the same single-J1 spec
     o = oracle.System(L, J1=-1.0, j1_mode=1)
@@ -280,3 +298,14 @@ def test_duplicate_coupling_name_raises():
     g.define_pyrochlore(1.0)
     with pytest.raises(pc.InvalidArgument, match="unique"):
         g.define_coupling("J2", [[], [], [], []], np.eye(3))
+
+
+def test_nonstructural_coupling_uses_generic_path():
+    # an asymmetric J2 gives the J2 group two different matrices (J on the
+    # source side, J^T on the target side): the generic tables must take over
+    g = pc.System(2)
+    g.define_pyrochlore(1.0, 0.0, 0.0)
+    g.setup_lattice()
+    assert g.structured()
+    g.set_coupling_matrix(6, [[0.1, 0.05, 0.0], [0.0, 0.1, 0.0], [0.0, 0.0, 0.1]])
+    assert not g.structured()
