@@ -229,6 +229,7 @@ def main():
     s = pc.pyrochlore_system(WL["L"], J1=WL["J1"], J2=WL["J2"], J3=WL["J3"], B=WL["B"], seed=1000 + rank)
     s.set_stream(stream.cuda_stream)
     s.random_spins(17 + rank)
+    tile = s.autotune()
     s.ssf_configure(WL["corr"], 1)
     N = s.N()
     T = WL["T"]
@@ -297,6 +298,7 @@ def main():
 
     if rank == 0:
         cpu = None if (args.no_cpu or world > 1) else cpu_baseline_one_core()
+        CONFIG["tile"] = {"threads": tile[0], "ctas_per_sm": tile[1], "chosen_by": "pc_autotune"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
@@ -319,6 +321,7 @@ def run_extras(pc, torch, np):
     b = pc.pyrochlore_system(Ls, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=7)
     b.set_stream(stream.cuda_stream)
     b.random_spins(5)
+    btile = b.autotune()
     b.pt_configure(T)
     b.ssf_configure(["xx", "yy", "zz"], len(Ls), sorted(Ls))
     b.pt_run(8, 10, 16)  # warm-up and graph capture (80 sweeps)
@@ -349,7 +352,7 @@ def run_extras(pc, torch, np):
     out["batched"] = {"value": batched, "unit": UNIT,
                       "config": "parallel tempering, 128 replicas (L 8/12/16/24 x 32 T geometric in [0.02, 2]), "
                                 "J=(1,0,0.02), B=(0,0,0.1), exchange every 10 sweeps, S(q) xx/yy/zz every 16 sweeps",
-                      "ms_per_10_sweeps": ms / rounds, "exchange_accept": float(acc.sum()) / max(1.0, float(att.sum())),
+                      "ms_per_10_sweeps": ms / rounds, "tile": list(btile), "exchange_accept": float(acc.sum()) / max(1.0, float(att.sum())),
                       "plain_single_L8": plain_small, "batched_over_plain_L8": batched / plain_small}
     # gradient form: 256 x L=8 energy + S^zz(q) forward/backward
     from pyro_cmc_b200 import autograd as ag

@@ -64,6 +64,10 @@ int pc_destroy(pc_system* sys);
  * its own, e.g. the caller's framework stream; the caller keeps ownership. */
 int pc_set_stream(pc_system* sys, void* stream);
 
+/* Replaces the Philox key (MC_runner is constructed with its seed after the
+ * Lattice exists, include/MC.hpp:107). */
+int pc_set_seed(pc_system* sys, uint64_t seed);
+
 /* MC_runner::define_coupling (include/MC.hpp:121-124, src/MC.cpp:56-66).
  * rel_vecs: displacement vectors for pyro_sl 0..3 concatenated, n_rel[p] of
  * them for sublattice p, 3 int64 each. J: 3x3 row-major, applied by the source
@@ -150,6 +154,10 @@ int pc_set_sweep_counter(pc_system* sys, int replica, uint64_t sweep);
  * T[r] per replica (host array). accepted[r] (host, may be NULL) receives the
  * accepted Metropolis moves summed over the n_sweeps sweeps. */
 int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uint64_t* accepted);
+/* overrelax_all (src/MC.cpp:145-153) alone on every replica: one
+ * overrelaxation pass over the colour classes with Philox angles (draw 2 at
+ * the current sweep counter), then the counter advances by one. */
+int pc_overrelax_all(pc_system* sys);
 /* overrelax_all (src/MC.cpp:145-153) alone, with deterministic angles:
  * theta (host, N doubles for `replica`) or NULL for reflection. For parity
  * tests of one overrelaxation pass. */

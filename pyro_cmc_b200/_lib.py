@@ -33,6 +33,7 @@ _SIGNATURES = {
     "pc_create": (_I, [_I, _I32P, _U64, _PP]),
     "pc_destroy": (_I, [_P]),
     "pc_set_stream": (_I, [_P, _P]),
+    "pc_set_seed": (_I, [_P, _U64]),
     "pc_define_coupling": (_I, [_P, C.c_char_p, _I64P, _I32P, _DP]),
     "pc_set_coupling_matrix": (_I, [_P, _I, _DP]),
     "pc_set_global_field": (_I, [_P, _DP]),
@@ -58,6 +59,7 @@ _SIGNATURES = {
     "pc_get_sweep_counter": (_I, [_P, _I, _U64P]),
     "pc_set_sweep_counter": (_I, [_P, _I, _U64]),
     "pc_sweep": (_I, [_P, _DP, _I, _I, _U64P]),
+    "pc_overrelax_all": (_I, [_P]),
     "pc_overrelax_theta": (_I, [_P, _I, _DP]),
     "pc_energy": (_I, [_P, _DP, _DP]),
     "pc_local_field": (_I, [_P, _I, _DP]),

@@ -35,15 +35,40 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp",
-           *[os.path.join(CSRC, f) for f in SOURCES], "-lcudart"]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
+    if force or needs_build():
+        cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp",
+               *[os.path.join(CSRC, f) for f in SOURCES], "-lcudart"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        os.replace(LIB + ".tmp", LIB)
+    build_host(force=force, verbose=verbose)
     return LIB
+
+
+HOST = os.path.join(HERE, "host")
+BIN = os.path.join(HERE, "bin")
+HOST_LIB_SOURCES = ["MC.cpp", "managers.cpp", "h5out.cpp"]
+HOST_HEADERS = ["MC.hpp", "managers.hpp", "h5out.hpp", "cli_bits.hpp", "vec3.hpp"]
+DRIVERS = ["anneal", "fieldcool", "temper", "spiral_byhand"]
+
+
+def build_host(force: bool = False, verbose: bool = False) -> None:
+    """The C++ drivers (the reference's executables) over libpyrocmc.so,
+    built with g++ into pyro_cmc_b200/bin/."""
+    os.makedirs(BIN, exist_ok=True)
+    deps = [os.path.join(HOST, f) for f in HOST_LIB_SOURCES + HOST_HEADERS] + [LIB]
+    for d in DRIVERS:
+        exe = os.path.join(BIN, d)
+        src = os.path.join(HOST, d + ".cpp")
+        if not force and os.path.exists(exe) and all(os.path.getmtime(x) <= os.path.getmtime(exe) for x in deps + [src]):
+            continue
+        cmd = ["g++", "-O2", "-std=c++20", "-Wall", "-I", os.path.join(REPO, "include"), "-o", exe, src,
+               *[os.path.join(HOST, f) for f in HOST_LIB_SOURCES], "-L", HERE, "-lpyrocmc",
+               "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
 
 
 if __name__ == "__main__":

@@ -174,7 +174,9 @@ __device__ __forceinline__ bool apply_move(const PassArgs& a, float4* S, size_t 
         return false;
     }
     const float n2 = h.x * h.x + h.y * h.y + h.z * h.z;
-    if (!(n2 > 1e-30f)) return false;
+    // a zero local field leaves the spin as it is; so does a zero spin (the
+    // reference's default-constructed state, which rotation keeps at zero)
+    if (!(n2 > 1e-30f) || !(s0.x * s0.x + s0.y * s0.y + s0.z * s0.z > 0.f)) return false;
     float nx, ny, nz;
     const float av = h.x * s0.x + h.y * s0.y + h.z * s0.z;
     if (MODE == kOverrelaxReflect) {
@@ -203,9 +205,15 @@ __device__ __forceinline__ bool apply_move(const PassArgs& a, float4* S, size_t 
     return false;
 }
 
-__device__ __forceinline__ void count_accepted(const PassArgs& a, bool accepted, int r, unsigned int* warp_acc) {
+// Accepted-move counting: each thread keeps a running count while its block
+// works through tiles of one replica and the block flushes it (one atomic)
+// when the replica changes and at the end. Tiles are replica-contiguous, so
+// a single-replica pass costs one atomic per block.
+__device__ __forceinline__ void flush_accepted(const PassArgs& a, unsigned int& mine, int r, unsigned int* warp_acc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned int c = __popc(__ballot_sync(0xffffffffu, accepted));
+    unsigned int c = mine;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
     if (lane == 0) warp_acc[warp] = c;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -214,6 +222,7 @@ __device__ __forceinline__ void count_accepted(const PassArgs& a, bool accepted,
         if (tot) atomicAdd(a.acc + r, (unsigned long long)tot);
     }
     __syncthreads();
+    mine = 0;
 }
 
 // Generic colour pass: bond tables (any coupling set) staged in shared memory.
@@ -224,22 +233,27 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
     stage_tables(tab, a.tables, a.n_tab, a.tab_sl);
     __syncthreads();
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
+    unsigned int mine = 0;
+    int r_cur = -1;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         const Tile tile = a.tiles[t];
         const int r = tile.x;
+        if (MODE == kMetropolis && r != r_cur) {
+            if (r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
+            r_cur = r;
+        }
         const int k = tile.y >> 8, sl = tile.y & 0xff;
         const ReplicaDev rep = a.reps[r];
         const int L = rep.L, Nc = rep.Nc;
         float4* S = a.spins + rep.off;
-        bool accepted = false;
         if (int(threadIdx.x) < tile.w) {
             const int cell = tile.z + int(threadIdx.x);
             const int cx = cell % L, cy = (cell / L) % L, cz = cell / (L * L);
             const float3 h = local_field(S, tab[k], cx, cy, cz, L, Nc);
-            accepted = apply_move<MODE>(a, S, size_t(sl) * Nc + cell, h, r, sweep);
+            mine += apply_move<MODE>(a, S, size_t(sl) * Nc + cell, h, r, sweep) ? 1u : 0u;
         }
-        if (MODE == kMetropolis) count_accepted(a, accepted, r, warp_acc);
     }
+    if (MODE == kMetropolis && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
 }
 
 template <int MODE, int SL>
@@ -276,20 +290,27 @@ template <int MODE>
 __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant__ PassArgs a) {
     __shared__ unsigned int warp_acc[8];
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
+    unsigned int mine = 0;
+    int r_cur = -1;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         const Tile tile = a.tiles[t];
         const int r = tile.x, sl = tile.y & 0xff;
+        if (MODE == kMetropolis && r != r_cur) {
+            if (r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
+            r_cur = r;
+        }
         const ReplicaDev rep = a.reps[r];
         float4* S = a.spins + rep.off;
-        bool accepted = false;
         if (int(threadIdx.x) < tile.w) {
             const int cell = tile.z + int(threadIdx.x);
+            bool accepted = false;
 #define PC_CALL(K) accepted = struct_site<MODE, K>(a, S, rep, r, cell, sweep)
             PC_SL_SWITCH(sl, PC_CALL)
 #undef PC_CALL
+            mine += accepted ? 1u : 0u;
         }
-        if (MODE == kMetropolis) count_accepted(a, accepted, r, warp_acc);
     }
+    if (MODE == kMetropolis && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
 }
 
 void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st) {

@@ -715,6 +715,14 @@ int pc_set_stream(pc_system* sys, void* stream) {
     return PC_OK;
 }
 
+int pc_set_seed(pc_system* sys, uint64_t seed) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    sys->seed = seed;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
 int pc_define_coupling(pc_system* sys, const char* name, const int64_t* rel_vecs, const int32_t* n_rel, const double* J) {
     int rc = check_sys(sys, false);
     if (rc) return rc;
@@ -1054,6 +1062,24 @@ int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uin
                               sys->stream));
         PC_CK(cudaStreamSynchronize(sys->stream));
     }
+    return PC_OK;
+}
+
+int pc_overrelax_all(pc_system* sys) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    const pc::PassMode om = sys->or_mode == 1 ? pc::kOverrelaxReflect : pc::kOverrelaxRotate;
+    for (int c = 0; c < sys->n_colours; ++c) {
+        const pc::PassArgs a = pass_args(sys, c, 0, 0);
+        pc::launch_colour_pass(om, a, grid_for(sys, a.n_tiles), sys->threads, sys->stream);
+        PC_LAUNCH_CK();
+        sys->launches++;
+    }
+    pc::launch_advance_counter(sys->d_sweep.p, 1, sys->stream);
+    PC_LAUNCH_CK();
+    sys->launches++;
+    sys->host_sweep++;
+    PC_CK(cudaStreamSynchronize(sys->stream));
     return PC_OK;
 }
 
@@ -1598,8 +1624,10 @@ int pc_autotune(pc_system* sys) {
     PC_CK(cudaStreamSynchronize(sys->stream));
     std::vector<double> T(size_t(sys->R), 1.0);
     PC_CK(cudaMemcpy(sys->d_T.p, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
+    // candidate tile shapes: threads per CTA x resident CTAs per SM (the
+    // structured kernels run at most 256 threads per CTA)
     const int cand_threads[3] = {128, 256, 512};
-    const int cand_ctas[3] = {2, 4, 8};
+    const int cand_ctas[6] = {2, 3, 4, 5, 6, 8};
     int best_t = sys->threads, best_c = sys->ctas_per_sm;
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;
@@ -1608,7 +1636,8 @@ int pc_autotune(pc_system* sys) {
     const bool timing = sys->timing;
     sys->timing = false;
     for (int ti = 0; ti < 3; ++ti)
-        for (int ci = 0; ci < 3; ++ci) {
+        for (int ci = 0; ci < 6; ++ci) {
+            if (sys->structured && cand_threads[ti] > 256) continue;
             sys->threads = cand_threads[ti];
             sys->ctas_per_sm = cand_ctas[ci];
             rc = build_tiles(sys);

@@ -241,6 +241,10 @@ class System:
         call("pc_sweep", self._h, _dp(Tv), int(n_sweeps), int(n_overrelax), acc.ctypes.data_as(_U64P))
         return acc
 
+    def overrelax_all(self):
+        """One overrelaxation pass on every replica (Philox angles)."""
+        call("pc_overrelax_all", self._h)
+
     def overrelax_theta(self, theta=None, replica: int = 0):
         if theta is None:
             call("pc_overrelax_theta", self._h, replica, None)
