@@ -9,7 +9,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpyrocmc.so")
 SOURCES = ["system.cu", "sweep.cu", "ssf.cu", "pt.cu"]
-HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh", "struct_field.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

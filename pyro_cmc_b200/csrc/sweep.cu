@@ -15,6 +15,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "struct_field.cuh"
 
 namespace pc {
 
@@ -51,91 +52,6 @@ __device__ __forceinline__ float3 local_field(const float4* __restrict__ S, cons
         hz += J[6] * tx + J[7] * ty + J[8] * tz;
     }
     return make_float3(hx, hy, hz);
-}
-
-// Structured local field (compile-time neighbour offsets of sublattice SL,
-// pyro_struct.cuh): the wrapped neighbour coordinates are formed once, each
-// of the 30 neighbours is one add-and-load with offsets fixed at compile time,
-// groups with a zero matrix are skipped. Same sum as local_field() with the
-// shells grouped per target.
-struct Coords {
-    int x[3], y[3], z[3];  // wrapped cx-1, cx, cx+1 (y, z premultiplied by L, L^2)
-};
-
-template <int D>
-__device__ __forceinline__ int pick(const int (&v)[3]) {
-    if constexpr (D < 0)
-        return v[0];
-    else if constexpr (D > 0)
-        return v[2];
-    else
-        return v[1];
-}
-
-template <int SL, int E>
-__device__ __forceinline__ float4 load_nb(const float4* __restrict__ S, int Nc, const Coords& c) {
-    constexpr int s2 = nb_sl(SL, E), dx = nb_dx(SL, E), dy = nb_dy(SL, E), dz = nb_dz(SL, E);
-    return __ldg(&S[s2 * Nc + pick<dx>(c.x) + pick<dy>(c.y) + pick<dz>(c.z)]);
-}
-
-template <int SL, int G, int... K>
-__device__ __forceinline__ float3 group_sum(const float4* __restrict__ S, int Nc, const Coords& c,
-                                            std::integer_sequence<int, K...>) {
-    constexpr int B = grp_begin(SL, G);
-    const float4 v[sizeof...(K)] = {load_nb<SL, B + K>(S, Nc, c)...};
-    float3 t = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-    for (int k = 0; k < int(sizeof...(K)); ++k) {
-        t.x += v[k].x;
-        t.y += v[k].y;
-        t.z += v[k].z;
-    }
-    return t;
-}
-
-template <int SL, int G>
-__device__ __forceinline__ void add_group(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
-                                          const PyroMats& mats) {
-    if (mats.active[SL] & (1u << G)) {
-        const float3 t = group_sum<SL, G>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
-        const float* J = mats.M[SL][G];
-        h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
-        h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
-        h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
-    }
-}
-
-__device__ __forceinline__ Coords cell_coords(int cell, int L, uint64_t divL) {
-    const int q = fdiv(cell, divL);  // cy + L*cz
-    const int cx = cell - q * L;
-    const int cz = fdiv(q, divL);
-    const int cy = q - cz * L;
-    const int LL = L * L;
-    Coords c;
-    c.x[0] = cx == 0 ? L - 1 : cx - 1;
-    c.x[1] = cx;
-    c.x[2] = cx == L - 1 ? 0 : cx + 1;
-    c.y[0] = L * (cy == 0 ? L - 1 : cy - 1);
-    c.y[1] = L * cy;
-    c.y[2] = L * (cy == L - 1 ? 0 : cy + 1);
-    c.z[0] = LL * (cz == 0 ? L - 1 : cz - 1);
-    c.z[1] = LL * cz;
-    c.z[2] = LL * (cz == L - 1 ? 0 : cz + 1);
-    return c;
-}
-
-template <int SL>
-__device__ __forceinline__ float3 struct_field(const float4* __restrict__ S, const PyroMats& mats, int cell,
-                                               int L, int Nc, uint64_t divL) {
-    const Coords c = cell_coords(cell, L, divL);
-    float3 h = make_float3(0.f, 0.f, 0.f);
-    add_group<SL, 0>(h, S, Nc, c, mats);
-    add_group<SL, 1>(h, S, Nc, c, mats);
-    add_group<SL, 2>(h, S, Nc, c, mats);
-    add_group<SL, 3>(h, S, Nc, c, mats);
-    add_group<SL, 4>(h, S, Nc, c, mats);
-    add_group<SL, 5>(h, S, Nc, c, mats);
-    return h;
 }
 
 // The move at site i with local field h (global field not yet subtracted):
