@@ -234,6 +234,26 @@ int pc_ssf_forward(pc_system* sys, void* out_dev);
  * device). Recomputes the forward transform instead of storing it. */
 int pc_ssf_backward(pc_system* sys, const void* grad_out_dev, void* grad_S_dev);
 
+/* ------------------------------------------------------ allocation-free */
+
+/* No counterpart in the reference. Energy per cubic cell and magnetisation of
+ * one pyrochlore lattice for callers that may not allocate device memory (a
+ * thread capturing a CUDA graph in global mode, a program whose memory belongs
+ * to a framework's caching allocator, a loop that cannot absorb the device-wide
+ * synchronisation of cudaFree). Nothing is allocated: the reduction's partial
+ * sums live in a 512 KiB array compiled into the library, shared by all calls
+ * on a device and kept until the process exits.
+ *   spins_dev  device, float4[16 L^3] in this library's site order
+ *   L          1..64 (larger L is rejected with PC_ERR_INVALID before any work)
+ *   params     host, 7 doubles: J1, J2, J3, Delta, Bx, By, Bz (the coupling set
+ *              of build_J1J2J3_h)
+ *   out_dev    device, 4 doubles: energy per cubic cell, sum_i S_i (x, y, z)
+ *   stream     cudaStream_t to launch on (NULL: the default stream)
+ * Asynchronous on `stream`. The first call on a device looks up the scratch
+ * array's address; make it before any stream capture. Calls that overlap on
+ * the GPU (e.g. on two streams) race on the shared array. */
+int pc_energy_noalloc(const void* spins_dev, int L, const double* params, void* out_dev, void* stream);
+
 /* ------------------------------------------------------------------ tuning */
 
 /* Times the sweep kernel over the candidate tile shapes on this system and

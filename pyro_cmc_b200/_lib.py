@@ -77,6 +77,7 @@ _SIGNATURES = {
     "pc_energy_grad": (_I, [_P, _DP, _DP, _P, _DP, _DP]),
     "pc_ssf_forward": (_I, [_P, _P]),
     "pc_ssf_backward": (_I, [_P, _P, _P]),
+    "pc_energy_noalloc": (_I, [_P, _I, _DP, _P, _P]),
     "pc_autotune": (_I, [_P]),
     "pc_get_tile": (_I, [_P, _IP, _IP]),
     "pc_set_tile": (_I, [_P, _I, _I]),

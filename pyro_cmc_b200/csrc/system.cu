@@ -114,6 +114,11 @@ void split_PQ(int L, int* P, int* Q) {
 
 }  // namespace
 
+namespace pc {
+// lets the other translation units of the library report through pc_last_error()
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace pc
+
 struct pc_system {
     int device = 0;
     int sms = 148;
