@@ -45,11 +45,13 @@ if REPO not in sys.path:
 METRIC = "spin-updates/s on 1 B200 (plain/batched/grad) at matched ⟨E⟩,C_v,S(q) vs CPU"
 UNIT = "spin-updates/s"
 WL = dict(L=64, J1=1.0, J2=0.1, J3=0.05, B=(0.0, 0.0, 0.5), T=0.5, n_sweep=32, ssf_every=16,
-          corr=["xx", "yy", "zz", "xy", "xz", "yz", "yx", "zx", "zy"])
+          corr=["xx", "yy", "zz", "xy", "xz", "yz", "yx", "zx", "zy"], schedule=1)
 CONFIG = {"workload": "fieldcool L=64 sampling step (32 sweeps + 2 S(q) samples x 9 correlators + energy)",
           "L": 64, "n_spins": 16 * 64 ** 3, "J": [1.0, 0.1, 0.05], "B": [0.0, 0.0, 0.5], "T": 0.5,
           "n_sweep": 32, "ssf_every": 16, "n_corr": 9, "spins": "fp32", "accumulators": "fp64",
-          "l2": "lattice (67 MB) fits in L2; no flush between steps", "parallelism": "replicas"}
+          "l2": "lattice (67 MB) fits in L2; no flush between steps", "parallelism": "replicas",
+          "schedule": "fused: per colour class, each site's Metropolis move then its overrelaxation move with one "
+                      "local field (pc_set_sweep_schedule 1); same moves per sweep as the reference's order"}
 
 
 def env_int(name, default):
@@ -83,7 +85,7 @@ def profile_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -98,7 +100,7 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -226,7 +228,8 @@ def main():
 
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    s = pc.pyrochlore_system(WL["L"], J1=WL["J1"], J2=WL["J2"], J3=WL["J3"], B=WL["B"], seed=1000 + rank)
+    s = pc.pyrochlore_system(WL["L"], J1=WL["J1"], J2=WL["J2"], J3=WL["J3"], B=WL["B"], seed=1000 + rank,
+                             schedule=WL["schedule"])
     s.set_stream(stream.cuda_stream)
     s.random_spins(17 + rank)
     tile = s.autotune()
@@ -259,6 +262,21 @@ def main():
     ms_max = max_over_ranks(ms)
     value = world * N * WL["n_sweep"] / (ms_max * 1e-3)
 
+    # the same steps in the reference's move order (Metropolis pass, then the
+    # overrelaxation pass), for comparison
+    s.set_sweep_schedule(0)
+    for _ in range(2):
+        device_step()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        device_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_ref_order = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    s.set_sweep_schedule(WL["schedule"])
+    device_step()
+
     # kernel durations of the colour passes (events around every launch)
     s.set_kernel_timing(True)
     device_step()
@@ -285,7 +303,7 @@ def main():
     alg_bytes = 32.0 * s.Nc()  # one colour pass: one sublattice, float4 read + write per site
     achieved = alg_bytes / (t_met * 1e-3) / 1e9 if t_met > 0 else None
     traffic = profile_traffic()
-    roofline = {"bound": "hbm", "kernel": "colour_pass_kernel<Metropolis>", "achieved": achieved, "peak": peak,
+    roofline = {"bound": "hbm", "kernel": "struct_pass_kernel (fused Metropolis + overrelaxation colour pass)", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                 "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "launch_ms": t_met,
                 "overrelax_launch_ms": t_or,
@@ -298,12 +316,15 @@ def main():
 
     if rank == 0:
         cpu = None if (args.no_cpu or world > 1) else cpu_baseline_one_core()
-        CONFIG["tile"] = {"threads": tile[0], "ctas_per_sm": tile[1], "chosen_by": "pc_autotune"}
+        CONFIG["tile"] = {"threads": tile[0], "ctas_per_sm": tile[1], "load_variant": tile[2],
+                          "chosen_by": "pc_autotune"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
                 "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clk}
+        line["value_reference_order"] = {"value": world * N * WL["n_sweep"] / (ms_ref_order * 1e-3), "unit": UNIT,
+                                          "ms_per_step": ms_ref_order, "schedule": "pc_set_sweep_schedule 0"}
         line.update(extras)
         print(json.dumps(line), flush=True)
     del s
@@ -318,7 +339,7 @@ def run_extras(pc, torch, np):
     Ls = [8] * 32 + [12] * 32 + [16] * 32 + [24] * 32
     Tl = np.geomspace(2.0, 0.02, 32)
     T = np.concatenate([Tl] * 4)
-    b = pc.pyrochlore_system(Ls, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=7)
+    b = pc.pyrochlore_system(Ls, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=7, schedule=WL["schedule"])
     b.set_stream(stream.cuda_stream)
     b.random_spins(5)
     btile = b.autotune()
@@ -338,7 +359,7 @@ def run_extras(pc, torch, np):
     att, acc = b.pt_exchange_stats()
     del b
     # plain single small replica (L=8), the comparison point for batching
-    p1 = pc.pyrochlore_system(8, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=9)
+    p1 = pc.pyrochlore_system(8, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=9, schedule=WL["schedule"])
     p1.set_stream(stream.cuda_stream)
     p1.random_spins(1)
     p1.sweep(0.5, 20, 1, count=False)

@@ -95,6 +95,16 @@ int pc_set_overrelax_mode(pc_system* sys, int mode);
  * nonzero bond share a class: 4 pyro_sl classes when J3 = 0); a different,
  * equally valid visiting order with fewer launches. Call before setup. */
 int pc_set_colouring(pc_system* sys, int mode);
+/* Sweep schedule. 0 (default): the reference's order -- a Metropolis pass
+ * over all colour classes, then n_overrelax overrelaxation passes
+ * (src/MC.cpp:155-163). 1 (fused): each colour pass applies the Metropolis
+ * move and then the first overrelaxation move to every site of the class,
+ * both with the site's local field, which no move of the pass changes; the
+ * remaining n_overrelax - 1 passes follow as in schedule 0. Both moves keep the
+ * Boltzmann distribution invariant, so the fused sweep samples the same
+ * ensemble with one local-field evaluation per site instead of two. The
+ * Philox draws per site are those of schedule 0. */
+int pc_set_sweep_schedule(pc_system* sys, int schedule);
 /* Kernel path: 0 (default) uses the structured pyrochlore kernels whenever the
  * couplings fit the fixed J1/J2/J3a/J3b neighbour structure, 1 forces the
  * generic bond-table kernels. Reports the path in use via pc_kernel_path. */
@@ -256,9 +266,14 @@ int pc_energy_noalloc(const void* spins_dev, int L, const double* params, void* 
 
 /* ------------------------------------------------------------------ tuning */
 
-/* Times the sweep kernel over the candidate tile shapes on this system and
- * keeps the fastest (spin state is saved and restored). */
+/* Times the sweep over the candidate tile shapes (threads per CTA x CTAs per
+ * SM) and neighbour-load variants on this system and keeps the fastest (spin
+ * state and sweep counter are saved and restored). */
 int pc_autotune(pc_system* sys);
+/* How the structured kernels issue the 30 neighbour loads of a site:
+ * 0 group by group (fewest registers), 1 all at once, 2 in two batches. */
+int pc_set_load_variant(pc_system* sys, int variant);
+int pc_get_load_variant(pc_system* sys, int* variant);
 /* Current tile shape (threads per CTA, CTAs per SM). */
 int pc_get_tile(pc_system* sys, int* threads, int* ctas_per_sm);
 int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm);

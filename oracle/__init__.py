@@ -71,7 +71,7 @@ def lib():
         l.orc_sweep.restype = _U64
         l.orc_sweep.argtypes = [_P, _D, _I, _I]
         l.orc_sweep_philox.restype = _U64
-        l.orc_sweep_philox.argtypes = [_P, _D, _U64, _U32, _U64, _I, _I32P, _I]
+        l.orc_sweep_philox.argtypes = [_P, _D, _U64, _U32, _U64, _I, _I32P, _I, _I]
         l.orc_overrelax.argtypes = [_P, _DP, _I32P]
         l.orc_ssf.argtypes = [_P, _I32P, _I, _I, _DP, _DP]
         l.orc_T_profile.argtypes = [_D, _D, _DP, _I, _I, _DP, _I32P, _I]
@@ -189,10 +189,10 @@ class System:
     def sweep(self, T, n_sweeps=1, n_overrelax=1):
         return lib().orc_sweep(self._h, T, n_sweeps, n_overrelax)
 
-    def sweep_philox(self, T, seed, replica, sweep, colour_of_sl, n_overrelax=1, or_mode=0):
+    def sweep_philox(self, T, seed, replica, sweep, colour_of_sl, n_overrelax=1, or_mode=0, fused=False):
         col = _arr(colour_of_sl, np.int32)
         return lib().orc_sweep_philox(self._h, T, seed, replica, sweep, n_overrelax,
-                                      col.ctypes.data_as(_I32P), or_mode)
+                                      col.ctypes.data_as(_I32P), or_mode, int(bool(fused)))
 
     def overrelax(self, theta=None, colour_of_sl=None):
         col = None if colour_of_sl is None else _arr(colour_of_sl, np.int32)

@@ -398,10 +398,13 @@ struct Runner {
     // so the order inside a class is immaterial), then n_or overrelaxation
     // passes over the same classes, with Philox draws per site. The update
     // formulas are those of local_Metropolis / overrelax_all above.
+    // fused: the first overrelaxation move of each site follows its Metropolis
+    // move inside the same colour class, with the same local field.
     size_t sweep_philox(double T, uint64_t seed, uint32_t replica, uint64_t sweep, int n_or,
-                        const std::vector<std::vector<int>>& colour_sls, int or_mode) {
+                        const std::vector<std::vector<int>>& colour_sls, int or_mode, bool fused = false) {
         size_t acc = 0;
         const double sigma = std::sqrt(T / T_ref);
+        const bool fuse = fused && n_or >= 1;
         for (const auto& cls : colour_sls)
             for (int sl : cls)
                 for (int cell = 0; cell < lat->Nc; ++cell) {
@@ -422,8 +425,17 @@ struct Runner {
                         spin->S = nS;
                         ++acc;
                     }
+                    if (fuse && dot(h, h) >= 1e-30) {
+                        if (or_mode == 1) {
+                            mirror_about_vector(spin->S, h);
+                        } else {
+                            uint32_t wo[4];
+                            philox_site(seed, replica, sweep, 2, site, wo);
+                            rotate_about_vector(spin->S, h, 2 * M_PI * u24(wo[0]));
+                        }
+                    }
                 }
-        for (int k = 0; k < n_or; ++k)
+        for (int k = fuse ? 1 : 0; k < n_or; ++k)
             for (const auto& cls : colour_sls)
                 for (int sl : cls)
                     for (int cell = 0; cell < lat->Nc; ++cell) {
@@ -750,13 +762,13 @@ uint64_t orc_sweep(void* h, double T, int n_sweeps, int n_overrelax) {
 // colour_of_sl[16]: colour index per sublattice; colours visited 0..n_colours-1,
 // sublattices inside a colour in increasing order.
 uint64_t orc_sweep_philox(void* h, double T, uint64_t seed, uint32_t replica, uint64_t sweep, int n_overrelax,
-                          const int32_t* colour_of_sl, int or_mode) {
+                          const int32_t* colour_of_sl, int or_mode, int fused) {
     auto* s = static_cast<System*>(h);
     int nc = 0;
     for (int i = 0; i < 16; ++i) nc = std::max(nc, colour_of_sl[i] + 1);
     std::vector<std::vector<int>> cls(static_cast<size_t>(nc));
     for (int i = 0; i < 16; ++i) cls[size_t(colour_of_sl[i])].push_back(i);
-    return s->mc.sweep_philox(T, seed, replica, sweep, n_overrelax, cls, or_mode);
+    return s->mc.sweep_philox(T, seed, replica, sweep, n_overrelax, cls, or_mode, fused != 0);
 }
 
 // One overrelaxation pass with caller-supplied angles (theta[i] per site) or

@@ -42,6 +42,7 @@ _SIGNATURES = {
     "pc_set_overrelax_mode": (_I, [_P, _I]),
     "pc_set_colouring": (_I, [_P, _I]),
     "pc_set_kernel_path": (_I, [_P, _I]),
+    "pc_set_sweep_schedule": (_I, [_P, _I]),
     "pc_kernel_path": (_I, [_P, _IP]),
     "pc_setup_lattice": (_I, [_P]),
     "pc_num_replicas": (_I, [_P, _IP]),
@@ -79,6 +80,8 @@ _SIGNATURES = {
     "pc_ssf_backward": (_I, [_P, _P, _P]),
     "pc_energy_noalloc": (_I, [_P, _I, _DP, _P, _P]),
     "pc_autotune": (_I, [_P]),
+    "pc_set_load_variant": (_I, [_P, _I]),
+    "pc_get_load_variant": (_I, [_P, _IP]),
     "pc_get_tile": (_I, [_P, _IP, _IP]),
     "pc_set_tile": (_I, [_P, _I, _I]),
     "pc_step_host": (_I, [_P, _FP, _FP, _D, _I, _I, _I, _DP, _U64P]),

@@ -45,7 +45,7 @@ def anneal_batch(K: int, L: int, J1: float, J2: float = 0.0, J3: float = 0.0, B=
                  Delta: float = 1.0, T_hot: float = 10.0, T_cold: float | None = None, T_sample=(0.1,),
                  n_steps: int = 100, n_sweep: int = 16, n_burn_in: int = 16, n_sample: int = 64,
                  corr=("xx", "yy", "zz", "xy", "xz", "yz"), T_ref: float = 1.0, seed: int = 0,
-                 init_seed: int | None = None):
+                 init_seed: int | None = None, schedule: int = 0):
     """The anneal protocol for K seeds at once: burn-in at T_hot, then for each
     T of the profile n_sweep sweeps and one energy sample; at the sample
     temperatures, n_sample x (n_sweep sweeps + one S(q) sample).
@@ -55,7 +55,8 @@ def anneal_batch(K: int, L: int, J1: float, J2: float = 0.0, J3: float = 0.0, B=
     if T_cold is None:
         T_cold = min(T_sample)
     T_grid, S_idx = generate_T_profile(T_hot, T_cold, T_sample, n_steps)
-    s = pyrochlore_system(L, J1=J1, J2=J2, J3=J3, Delta=Delta, B=B, T_ref=T_ref, seed=seed, n_replicas=K)
+    s = pyrochlore_system(L, J1=J1, J2=J2, J3=J3, Delta=Delta, B=B, T_ref=T_ref, seed=seed, n_replicas=K,
+                          schedule=schedule)
     s.random_spins(seed if init_seed is None else init_seed)
     nTs = len(S_idx)
     s.ssf_configure(list(corr), max(1, K * nTs), [L] * max(1, K * nTs))
@@ -88,11 +89,11 @@ def anneal_batch(K: int, L: int, J1: float, J2: float = 0.0, J3: float = 0.0, B=
 
 def temper(L_list, T, J1: float, J2: float = 0.0, J3: float = 0.0, B=(0.0, 0.0, 0.0), Delta: float = 1.0,
            n_burn_in_rounds: int = 10, n_rounds: int = 100, n_sweep: int = 10, ssf_every: int = 0,
-           corr=("xx", "yy", "zz"), seed: int = 0):
+           corr=("xx", "yy", "zz"), seed: int = 0, schedule: int = 0):
     """Batched parallel tempering: replica r of size L_list[r] starts at T[r];
     replicas of equal L form one ladder. Returns per-slot (T, <e>, <e^2>,
     n samples), exchange statistics and the system (for SSF reads)."""
-    s = pyrochlore_system(list(L_list), J1=J1, J2=J2, J3=J3, Delta=Delta, B=B, seed=seed)
+    s = pyrochlore_system(list(L_list), J1=J1, J2=J2, J3=J3, Delta=Delta, B=B, seed=seed, schedule=schedule)
     s.random_spins(seed)
     s.pt_configure(T)
     if ssf_every:

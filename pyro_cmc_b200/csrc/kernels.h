@@ -10,7 +10,17 @@
 
 namespace pc {
 
-enum PassMode { kMetropolis = 0, kOverrelaxRotate = 1, kOverrelaxReflect = 2, kOverrelaxTheta = 3 };
+// kFused*: the Metropolis move and then one overrelaxation move of the same
+// site in one pass, both with the site's local field (which no move of this
+// pass changes).
+enum PassMode {
+    kMetropolis = 0,
+    kOverrelaxRotate = 1,
+    kOverrelaxReflect = 2,
+    kOverrelaxTheta = 3,
+    kFusedRotate = 4,
+    kFusedReflect = 5
+};
 
 struct PassArgs {
     float4* spins;
@@ -30,7 +40,8 @@ struct PassArgs {
     int or_pass;              // overrelaxation pass index (draw 2 + or_pass)
     const double* theta;      // kOverrelaxTheta: per-site angle of replica theta_replica (device)
     int theta_replica;
-    int structured;  // 1: couplings fit the pyrochlore structure, use `mats`
+    int structured;    // 1: couplings fit the pyrochlore structure, use `mats`
+    int load_variant;  // structured path: how neighbour loads are batched (0, 1, 2)
     PyroMats mats;
 };
 

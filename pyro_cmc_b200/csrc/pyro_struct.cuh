@@ -141,6 +141,11 @@ __host__ __device__ constexpr int nb_dx(int sl, int e) { return kStruct.t[sl].nb
 __host__ __device__ constexpr int nb_dy(int sl, int e) { return kStruct.t[sl].nb[e].dy; }
 __host__ __device__ constexpr int nb_dz(int sl, int e) { return kStruct.t[sl].nb[e].dz; }
 __host__ __device__ constexpr int grp_begin(int sl, int g) { return kStruct.t[sl].gbegin[g]; }
+__host__ __device__ constexpr int group_of(int sl, int e) {
+    int g = 0;
+    while (g + 1 < kGroups && kStruct.t[sl].gbegin[g + 1] <= e) ++g;
+    return g;
+}
 __host__ __device__ constexpr int grp_size(int sl, int g) { return kStruct.t[sl].gbegin[g + 1] - kStruct.t[sl].gbegin[g]; }
 
 // Group matrices per sublattice (row-major 3x3) and the groups with a nonzero

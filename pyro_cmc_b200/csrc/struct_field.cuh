@@ -83,6 +83,48 @@ __device__ __forceinline__ Coords cell_coords(int cell, int L, uint64_t divL) {
     return c;
 }
 
+// All 30 neighbour loads issued at once (a group with a zero matrix loads
+// nothing: the loads are predicated, not branched around), so one memory round
+// trip covers the whole site instead of one per group.
+template <int SL, int OFF, int... E>
+__device__ __forceinline__ void load_range(float4 (&v)[kStructNb], const float4* __restrict__ S, int Nc,
+                                           const Coords& c, uint32_t act, std::integer_sequence<int, E...>) {
+    ((v[OFF + E] = (act & (1u << group_of(SL, OFF + E))) ? load_nb<SL, OFF + E>(S, Nc, c)
+                                                          : make_float4(0.f, 0.f, 0.f, 0.f)),
+     ...);
+}
+// neighbours [B, E) of sublattice SL into v[B..E)
+template <int SL, int B, int E>
+__device__ __forceinline__ void load_nbs(float4 (&v)[kStructNb], const float4* __restrict__ S, int Nc, const Coords& c,
+                                         uint32_t act) {
+    load_range<SL, B>(v, S, Nc, c, act, std::make_integer_sequence<int, E - B>{});
+}
+
+template <int SL, int G>
+__device__ __forceinline__ void add_group_v(float3& h, const float4 (&v)[kStructNb], const PyroMats& mats) {
+    constexpr int B = grp_begin(SL, G), E = grp_begin(SL, G + 1);
+    float3 t = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = B; k < E; ++k) {
+        t.x += v[k].x;
+        t.y += v[k].y;
+        t.z += v[k].z;
+    }
+    const float* J = mats.M[SL][G];
+    h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
+    h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
+    h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+}
+
+// h += sum of the group matrices times the group sums, groups [G0, G1)
+template <int SL, int G0, int G1>
+__device__ __forceinline__ void field_groups(float3& h, const float4 (&v)[kStructNb], const PyroMats& mats) {
+    if constexpr (G0 < G1) {
+        add_group_v<SL, G0>(h, v, mats);
+        field_groups<SL, G0 + 1, G1>(h, v, mats);
+    }
+}
+
 template <int SL>
 __device__ __forceinline__ float3 struct_field(const float4* __restrict__ S, const PyroMats& mats, int cell,
                                                int L, int Nc, uint64_t divL) {

@@ -58,67 +58,95 @@ __device__ __forceinline__ float3 local_field(const float4* __restrict__ S, cons
 // Metropolis (local_Metropolis, src/MC.cpp:111-130) or one overrelaxation
 // (overrelax_all, src/MC.cpp:145-153; mirror_about_vector :98-100). Returns
 // whether a Metropolis proposal was accepted.
-template <int MODE>
-__device__ __forceinline__ bool apply_move(const PassArgs& a, float4* S, size_t i, float3 h, int r, uint64_t sweep) {
-    const float4 s0 = S[i];
-    h.x -= a.B[0];
-    h.y -= a.B[1];
-    h.z -= a.B[2];
-    if (MODE == kMetropolis) {
-        const double T = a.T_rep[r];
-        const float sigma = sqrtf(float(T) * a.inv_T_ref);
-        const float invT = float(1.0 / T);
-        const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
-        // Box-Muller on the top 24 bits of words (0,1) and (2,3)
-        const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
-        const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
-        float s_a, c_a, s_b, c_b;
-        sincospif(2.f * u24(w.y), &s_a, &c_a);
-        sincospif(2.f * u24(w.w), &s_b, &c_b);
-        float nx = s0.x + sigma * (r0 * c_a);
-        float ny = s0.y + sigma * (r0 * s_a);
-        float nz = s0.z + sigma * (r1 * c_b);
-        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
-        nx *= inv;
-        ny *= inv;
-        nz *= inv;
-        const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
-        if (dE < 0.f || u24_lowbytes(w) < __expf(-dE * invT)) {
-            S[i] = make_float4(nx, ny, nz, 0.f);
-            return true;
-        }
-        return false;
-    }
+// The overrelaxation of spin s0 about the effective field h (global field
+// already subtracted): rotate_about_vector by the given angle (src/MC.cpp:102-109)
+// or mirror_about_vector (:98-100), renormalised against FP32 drift. Returns
+// false (spin unchanged) for a zero field or a zero spin.
+template <bool REFLECT>
+__device__ __forceinline__ bool overrelax_spin(float4 s0, float3 h, float sn, float cs, float4& out) {
     const float n2 = h.x * h.x + h.y * h.y + h.z * h.z;
     // a zero local field leaves the spin as it is; so does a zero spin (the
     // reference's default-constructed state, which rotation keeps at zero)
     if (!(n2 > 1e-30f) || !(s0.x * s0.x + s0.y * s0.y + s0.z * s0.z > 0.f)) return false;
-    float nx, ny, nz;
     const float av = h.x * s0.x + h.y * s0.y + h.z * s0.z;
-    if (MODE == kOverrelaxReflect) {
+    float nx, ny, nz;
+    if (REFLECT) {
         const float f = 2.f * av / (n2 + 1e-10f);
         nx = -s0.x + f * h.x;
         ny = -s0.y + f * h.y;
         nz = -s0.z + f * h.z;
     } else {
-        // rotate_about_vector (src/MC.cpp:102-109), theta = 2*pi*U
-        float sn, cs;
-        if (MODE == kOverrelaxTheta) {
-            sincosf(float(a.theta[i]), &sn, &cs);
-        } else {
-            const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
-            sincospif(2.f * u24(w.x), &sn, &cs);
-        }
         const float f = (1.f - cs) * av / n2;
         const float g = sn * rsqrtf(n2);
         nx = cs * s0.x + f * h.x + g * (h.y * s0.z - h.z * s0.y);
         ny = cs * s0.y + f * h.y + g * (h.z * s0.x - h.x * s0.z);
         nz = cs * s0.z + f * h.z + g * (h.x * s0.y - h.y * s0.x);
     }
-    // renormalise: keeps FP32 rounding from drifting |S| away from 1
     const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
-    S[i] = make_float4(nx * inv, ny * inv, nz * inv, 0.f);
+    out = make_float4(nx * inv, ny * inv, nz * inv, 0.f);
+    return true;
+}
+
+// Metropolis proposal of local_Metropolis (src/MC.cpp:111-130) at site i with
+// effective field h: returns whether it is accepted; `out` holds the new spin.
+__device__ __forceinline__ bool metropolis_spin(const PassArgs& a, float4 s0, float3 h, int r, uint64_t sweep, size_t i,
+                                                float4& out) {
+    const double T = a.T_rep[r];
+    const float sigma = sqrtf(float(T) * a.inv_T_ref);
+    const float invT = float(1.0 / T);
+    const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
+    // Box-Muller on the top 24 bits of words (0,1) and (2,3)
+    const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
+    const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
+    float s_a, c_a, s_b, c_b;
+    sincospif(2.f * u24(w.y), &s_a, &c_a);
+    sincospif(2.f * u24(w.w), &s_b, &c_b);
+    float nx = s0.x + sigma * (r0 * c_a);
+    float ny = s0.y + sigma * (r0 * s_a);
+    float nz = s0.z + sigma * (r1 * c_b);
+    const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+    nx *= inv;
+    ny *= inv;
+    nz *= inv;
+    const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
+    if (dE < 0.f || u24_lowbytes(w) < __expf(-dE * invT)) {
+        out = make_float4(nx, ny, nz, 0.f);
+        return true;
+    }
+    out = s0;
     return false;
+}
+
+// The move at site i with local field h (global field not yet subtracted).
+// Returns whether a Metropolis proposal was accepted.
+template <int MODE>
+__device__ __forceinline__ bool apply_move(const PassArgs& a, float4* S, size_t i, float3 h, int r, uint64_t sweep) {
+    const float4 s0 = S[i];
+    h.x -= a.B[0];
+    h.y -= a.B[1];
+    h.z -= a.B[2];
+    bool acc = false;
+    float4 s1 = s0;
+    if (MODE == kMetropolis || MODE == kFusedRotate || MODE == kFusedReflect)
+        acc = metropolis_spin(a, s0, h, r, sweep, i, s1);
+    if (MODE == kMetropolis) {
+        if (acc) S[i] = s1;
+        return acc;
+    }
+    float sn = 0.f, cs = 1.f;
+    if (MODE == kOverrelaxRotate || MODE == kFusedRotate) {
+        const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
+        sincospif(2.f * u24(w.x), &sn, &cs);
+    } else if (MODE == kOverrelaxTheta) {
+        sincosf(float(a.theta[i]), &sn, &cs);
+    }
+    float4 s2;
+    const bool moved = overrelax_spin<MODE == kOverrelaxReflect || MODE == kFusedReflect>(s1, h, sn, cs, s2);
+    if (moved)
+        S[i] = s2;
+    else if (acc)
+        S[i] = s1;
+    return acc;
 }
 
 // Accepted-move counting: each thread keeps a running count while its block
@@ -154,7 +182,7 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         const Tile tile = a.tiles[t];
         const int r = tile.x;
-        if (MODE == kMetropolis && r != r_cur) {
+        if ((MODE == kMetropolis || MODE >= kFusedRotate) && r != r_cur) {
             if (r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
             r_cur = r;
         }
@@ -169,14 +197,113 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
             mine += apply_move<MODE>(a, S, size_t(sl) * Nc + cell, h, r, sweep) ? 1u : 0u;
         }
     }
-    if (MODE == kMetropolis && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
+    if ((MODE == kMetropolis || MODE >= kFusedRotate) && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
 }
 
-template <int MODE, int SL>
+// One site of the structured pass. How the 30 neighbour loads are issued is
+// chosen by the autotuner (more loads in flight per thread costs registers,
+// hence resident warps):
+//   VAR 0: group by group (six short load batches, fewest registers);
+//   VAR 1: all 30 at once, before the Philox draw and the proposal (which do
+//          not depend on the local field) are computed;
+//   VAR 2: J1 + J2 neighbours (18) before the draw, J3 (12) after it.
+template <int SL, int VAR>
+__device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const PassArgs& a, const ReplicaDev& rep,
+                                             const Coords& c, float4 (&v)[kStructNb], int phase) {
+    constexpr int kJ3 = grp_begin(SL, 4);
+    float3 h = make_float3(0.f, 0.f, 0.f);
+    if constexpr (VAR == 0) {
+        if (phase == 1) {
+            add_group<SL, 0>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 1>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 2>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 3>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 4>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 5>(h, S, rep.Nc, c, a.mats);
+        }
+    } else if constexpr (VAR == 1) {
+        if (phase == 0)
+            load_nbs<SL, 0, kStructNb>(v, S, rep.Nc, c, a.mats.active[SL]);
+        else
+            field_groups<SL, 0, kGroups>(h, v, a.mats);
+    } else {
+        if (phase == 0) {
+            load_nbs<SL, 0, kJ3>(v, S, rep.Nc, c, a.mats.active[SL]);
+        } else {
+            field_groups<SL, 0, 4>(h, v, a.mats);
+            load_nbs<SL, kJ3, kStructNb>(v, S, rep.Nc, c, a.mats.active[SL]);
+            field_groups<SL, 4, kGroups>(h, v, a.mats);
+        }
+    }
+    return h;
+}
+
+template <int MODE, int SL, int VAR>
 __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const ReplicaDev& rep, int r, int cell,
                                             uint64_t sweep) {
-    const float3 h = struct_field<SL>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
-    return apply_move<MODE>(a, S, size_t(SL) * rep.Nc + cell, h, r, sweep);
+    const Coords c = cell_coords(cell, rep.L, rep.divL);
+    float4 v[kStructNb];
+    site_field<SL, VAR>(S, a, rep, c, v, 0);  // issue loads (VAR 1, 2)
+    const size_t i = size_t(SL) * rep.Nc + cell;
+    const float4 s0 = S[i];
+    constexpr bool kMet = MODE == kMetropolis || MODE == kFusedRotate || MODE == kFusedReflect;
+    constexpr bool kRot = MODE == kOverrelaxRotate || MODE == kFusedRotate;
+    // draws first: they do not depend on the local field, so they overlap the loads
+    uint4 w = make_uint4(0, 0, 0, 0);
+    float sigma = 0.f, invT = 0.f;
+    if (kMet) {
+        const double T = a.T_rep[r];
+        sigma = sqrtf(float(T) * a.inv_T_ref);
+        invT = float(1.0 / T);
+        w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
+    }
+    float sn = 0.f, cs = 1.f;
+    if (kRot) {
+        const uint4 wo = site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
+        sincospif(2.f * u24(wo.x), &sn, &cs);
+    } else if (MODE == kOverrelaxTheta) {
+        sincosf(float(a.theta[i]), &sn, &cs);
+    }
+    float4 s1 = s0;
+    float nx = 0.f, ny = 0.f, nz = 0.f, u = 0.f;
+    if (kMet) {
+        const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
+        const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
+        float s_a, c_a, s_b, c_b;
+        sincospif(2.f * u24(w.y), &s_a, &c_a);
+        sincospif(2.f * u24(w.w), &s_b, &c_b);
+        nx = s0.x + sigma * (r0 * c_a);
+        ny = s0.y + sigma * (r0 * s_a);
+        nz = s0.z + sigma * (r1 * c_b);
+        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+        nx *= inv;
+        ny *= inv;
+        nz *= inv;
+        u = u24_lowbytes(w);
+    }
+    float3 h = site_field<SL, VAR>(S, a, rep, c, v, 1);
+    h.x -= a.B[0];
+    h.y -= a.B[1];
+    h.z -= a.B[2];
+    bool acc = false;
+    if (kMet) {
+        const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
+        if (dE < 0.f || u < __expf(-dE * invT)) {
+            s1 = make_float4(nx, ny, nz, 0.f);
+            acc = true;
+        }
+        if (MODE == kMetropolis) {
+            if (acc) S[i] = s1;
+            return acc;
+        }
+    }
+    float4 s2;
+    const bool moved = overrelax_spin<MODE == kOverrelaxReflect || MODE == kFusedReflect>(s1, h, sn, cs, s2);
+    if (moved)
+        S[i] = s2;
+    else if (acc)
+        S[i] = s1;
+    return acc;
 }
 
 #define PC_SL_SWITCH(sl, CALL) \
@@ -202,7 +329,7 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
 
 // Structured colour pass: pyrochlore neighbour offsets fixed at compile time,
 // coupling matrices per (sublattice, group) in the kernel parameters.
-template <int MODE>
+template <int MODE, int VAR>
 __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant__ PassArgs a) {
     __shared__ unsigned int warp_acc[8];
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
@@ -211,7 +338,7 @@ __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant_
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
         const Tile tile = a.tiles[t];
         const int r = tile.x, sl = tile.y & 0xff;
-        if (MODE == kMetropolis && r != r_cur) {
+        if ((MODE == kMetropolis || MODE >= kFusedRotate) && r != r_cur) {
             if (r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
             r_cur = r;
         }
@@ -220,23 +347,35 @@ __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant_
         if (int(threadIdx.x) < tile.w) {
             const int cell = tile.z + int(threadIdx.x);
             bool accepted = false;
-#define PC_CALL(K) accepted = struct_site<MODE, K>(a, S, rep, r, cell, sweep)
+#define PC_CALL(K) accepted = struct_site<MODE, K, VAR>(a, S, rep, r, cell, sweep)
             PC_SL_SWITCH(sl, PC_CALL)
 #undef PC_CALL
             mine += accepted ? 1u : 0u;
         }
     }
-    if (MODE == kMetropolis && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
+    if ((MODE == kMetropolis || MODE >= kFusedRotate) && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
+}
+
+template <int VAR>
+static void launch_struct(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st) {
+    switch (mode) {
+        case kMetropolis: struct_pass_kernel<kMetropolis, VAR><<<grid, threads, 0, st>>>(a); break;
+        case kOverrelaxRotate: struct_pass_kernel<kOverrelaxRotate, VAR><<<grid, threads, 0, st>>>(a); break;
+        case kOverrelaxReflect: struct_pass_kernel<kOverrelaxReflect, VAR><<<grid, threads, 0, st>>>(a); break;
+        case kOverrelaxTheta: struct_pass_kernel<kOverrelaxTheta, VAR><<<grid, threads, 0, st>>>(a); break;
+        case kFusedRotate: struct_pass_kernel<kFusedRotate, VAR><<<grid, threads, 0, st>>>(a); break;
+        case kFusedReflect: struct_pass_kernel<kFusedReflect, VAR><<<grid, threads, 0, st>>>(a); break;
+    }
 }
 
 void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st) {
     if (a.structured && threads <= 256) {
-        switch (mode) {
-            case kMetropolis: struct_pass_kernel<kMetropolis><<<grid, threads, 0, st>>>(a); break;
-            case kOverrelaxRotate: struct_pass_kernel<kOverrelaxRotate><<<grid, threads, 0, st>>>(a); break;
-            case kOverrelaxReflect: struct_pass_kernel<kOverrelaxReflect><<<grid, threads, 0, st>>>(a); break;
-            case kOverrelaxTheta: struct_pass_kernel<kOverrelaxTheta><<<grid, threads, 0, st>>>(a); break;
-        }
+        if (a.load_variant == 1)
+            launch_struct<1>(mode, a, grid, threads, st);
+        else if (a.load_variant == 2)
+            launch_struct<2>(mode, a, grid, threads, st);
+        else
+            launch_struct<0>(mode, a, grid, threads, st);
         return;
     }
     switch (mode) {
@@ -244,6 +383,8 @@ void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads,
         case kOverrelaxRotate: colour_pass_kernel<kOverrelaxRotate><<<grid, threads, 0, st>>>(a); break;
         case kOverrelaxReflect: colour_pass_kernel<kOverrelaxReflect><<<grid, threads, 0, st>>>(a); break;
         case kOverrelaxTheta: colour_pass_kernel<kOverrelaxTheta><<<grid, threads, 0, st>>>(a); break;
+        case kFusedRotate: colour_pass_kernel<kFusedRotate><<<grid, threads, 0, st>>>(a); break;
+        case kFusedReflect: colour_pass_kernel<kFusedReflect><<<grid, threads, 0, st>>>(a); break;
     }
 }
 
@@ -352,17 +493,20 @@ void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st) {
         energy_partials_kernel<<<grid, threads, 0, st>>>(a);
 }
 
-// One warp per replica: fixed-order sum of its tile partials (deterministic).
-__global__ void energy_finalize_kernel(const double* partial, const int32_t* tb, const int32_t* te,
-                                       const ReplicaDev* reps, int R, double* e, double* mag) {
+// One block per replica: each thread sums a fixed strided subset of the
+// replica's tile partials, then a fixed-shape tree combines them, so the
+// result does not depend on scheduling (deterministic).
+__global__ void __launch_bounds__(256) energy_finalize_kernel(const double* partial, const int32_t* tb,
+                                                              const int32_t* te, const ReplicaDev* reps, int R,
+                                                              double* e, double* mag) {
+    __shared__ double red[4 * 32];
     const int r = blockIdx.x;
     if (r >= R) return;
-    const int lane = threadIdx.x;
     double v[4] = {0, 0, 0, 0};
-    for (int t = tb[r] + lane; t < te[r]; t += 32)
+    for (int t = tb[r] + int(threadIdx.x); t < te[r]; t += blockDim.x)
         for (int j = 0; j < 4; ++j) v[j] += partial[size_t(t) * 4 + j];
-    for (int j = 0; j < 4; ++j) v[j] = warp_sum(v[j]);
-    if (lane == 0) {
+    block_sum<4>(v, red);
+    if (threadIdx.x == 0) {
         e[r] = v[0] / double(reps[r].Nc);
         if (mag)
             for (int j = 0; j < 3; ++j) mag[3 * r + j] = v[1 + j];
@@ -371,7 +515,7 @@ __global__ void energy_finalize_kernel(const double* partial, const int32_t* tb,
 
 void launch_energy_finalize(const double* partial, const int32_t* tile_begin, const int32_t* tile_end,
                             const ReplicaDev* reps, int R, double* e, double* mag, cudaStream_t st) {
-    energy_finalize_kernel<<<R, 32, 0, st>>>(partial, tile_begin, tile_end, reps, R, e, mag);
+    energy_finalize_kernel<<<R, 256, 0, st>>>(partial, tile_begin, tile_end, reps, R, e, mag);
 }
 
 __global__ void __launch_bounds__(512) local_field_kernel(const FieldArgs a) {

@@ -134,6 +134,7 @@ struct pc_system {
     double B[3] = {0, 0, 0};
     int or_mode = 0;
     int colouring = 0;
+    int schedule = 0;  // 0: Metropolis pass then overrelaxation passes; 1: fused
     std::vector<Coupling> specs;
     bool ready = false;
 
@@ -148,6 +149,7 @@ struct pc_system {
 
     int threads = 256;
     int ctas_per_sm = 4;
+    int load_variant = 0;  // structured kernels: neighbour-load batching
 
     DevBuf<ReplicaDev> d_reps;
     DevBuf<float4> d_spins;
@@ -165,6 +167,7 @@ struct pc_system {
     DevBuf<double> d_e, d_mag;
     DevBuf<double> d_theta;
     DevBuf<float4> d_field;
+    DevBuf<double> d_grad_g, d_grad_out;  // energy-gradient upstream scalars and results
 
     uint64_t host_sweep = 0;
     uint64_t launches = 0;
@@ -228,6 +231,8 @@ struct pc_system {
         d_field.release();
         d_ssf_sum.release();
         d_ssf_sq.release();
+        d_grad_g.release();
+        d_grad_out.release();
         for (auto& g : groups) {
             g.d_rep_index.release();
             g.d_sel_index.release();
@@ -472,6 +477,7 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.acc = s->d_acc.p;
     a.or_pass = or_pass;
     a.structured = s->structured ? 1 : 0;
+    a.load_variant = s->load_variant;
     a.mats = s->mats;
     return a;
 }
@@ -498,18 +504,21 @@ int enqueue_sweep(pc_system* s, uint64_t off, int n_or, bool record_events) {
         }
         return PC_OK;
     };
+    const bool fused = s->schedule == 1 && n_or >= 1;
+    const pc::PassMode mm =
+        fused ? (s->or_mode == 1 ? pc::kFusedReflect : pc::kFusedRotate) : pc::kMetropolis;
     for (int c = 0; c < s->n_colours; ++c) {
         const pc::PassArgs a = pass_args(s, c, off, 0);
         int rc = record(0, true);
         if (rc) return rc;
-        pc::launch_colour_pass(pc::kMetropolis, a, grid_for(s, a.n_tiles), s->threads, s->stream);
+        pc::launch_colour_pass(mm, a, grid_for(s, a.n_tiles), s->threads, s->stream);
         PC_LAUNCH_CK();
         rc = record(0, false);
         if (rc) return rc;
         s->launches++;
     }
     const pc::PassMode om = s->or_mode == 1 ? pc::kOverrelaxReflect : pc::kOverrelaxRotate;
-    for (int k = 0; k < n_or; ++k)
+    for (int k = fused ? 1 : 0; k < n_or; ++k)
         for (int c = 0; c < s->n_colours; ++c) {
             const pc::PassArgs a = pass_args(s, c, off, k);
             int rc = record(1, true);
@@ -800,6 +809,15 @@ int pc_set_overrelax_mode(pc_system* sys, int mode) {
     if (rc) return rc;
     if (mode != 0 && mode != 1) return fail(PC_ERR_INVALID, "overrelaxation mode must be 0 (rotation) or 1 (reflection)");
     sys->or_mode = mode;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_set_sweep_schedule(pc_system* sys, int schedule) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (schedule != 0 && schedule != 1) return fail(PC_ERR_INVALID, "sweep schedule must be 0 (reference order) or 1 (fused)");
+    sys->schedule = schedule;
     sys->drop_graphs();
     return PC_OK;
 }
@@ -1558,11 +1576,14 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
     if (rc) return rc;
     const int ns = int(sys->specs.size());
     const int width = 4 + 9 * ns;
-    DevBuf<double> d_g, d_out;
-    PC_CK(d_g.alloc(size_t(sys->R)));
-    PC_CK(d_out.alloc(size_t(sys->R) * size_t(width)));
+    if (sys->d_grad_g.n != size_t(sys->R)) PC_CK(sys->d_grad_g.alloc(size_t(sys->R)));
+    if (sys->d_grad_out.n != size_t(sys->R) * size_t(width))
+        PC_CK(sys->d_grad_out.alloc(size_t(sys->R) * size_t(width)));
+    DevBuf<double>& d_g = sys->d_grad_g;
+    DevBuf<double>& d_out = sys->d_grad_out;
     std::vector<double> ones(size_t(sys->R), 1.0);
-    PC_CK(cudaMemcpy(d_g.p, g ? g : ones.data(), sizeof(double) * size_t(sys->R), cudaMemcpyHostToDevice));
+    PC_CK(cudaMemcpyAsync(d_g.p, g ? g : ones.data(), sizeof(double) * size_t(sys->R), cudaMemcpyHostToDevice,
+                          sys->stream));
     pc::GradArgs a;
     a.spins = sys->d_spins.p;
     a.reps = sys->d_reps.p;
@@ -1583,8 +1604,6 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
     std::vector<double> out(size_t(sys->R) * size_t(width));
     PC_CK(cudaMemcpyAsync(out.data(), d_out.p, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, sys->stream));
     PC_CK(cudaStreamSynchronize(sys->stream));
-    d_g.release();
-    d_out.release();
     for (int r = 0; r < sys->R; ++r) {
         const double* o = out.data() + size_t(r) * size_t(width);
         const double nc = double(sys->Nc(r));
@@ -1617,6 +1636,21 @@ int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm) {
     return PC_OK;
 }
 
+int pc_set_load_variant(pc_system* sys, int variant) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (variant < 0 || variant > 2) return fail(PC_ERR_INVALID, "load variant must be 0, 1 or 2");
+    sys->load_variant = variant;
+    sys->drop_graphs();
+    return PC_OK;
+}
+int pc_get_load_variant(pc_system* sys, int* variant) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    *variant = sys->load_variant;
+    return PC_OK;
+}
+
 int pc_autotune(pc_system* sys) {
     int rc = check_sys(sys);
     if (rc) return rc;
@@ -1629,44 +1663,49 @@ int pc_autotune(pc_system* sys) {
     PC_CK(cudaStreamSynchronize(sys->stream));
     std::vector<double> T(size_t(sys->R), 1.0);
     PC_CK(cudaMemcpy(sys->d_T.p, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
-    // candidate tile shapes: threads per CTA x resident CTAs per SM (the
-    // structured kernels run at most 256 threads per CTA)
+    // candidates: neighbour-load variant x threads per CTA x resident CTAs per
+    // SM (the structured kernels run at most 256 threads per CTA)
     const int cand_threads[3] = {128, 256, 512};
     const int cand_ctas[6] = {2, 3, 4, 5, 6, 8};
-    int best_t = sys->threads, best_c = sys->ctas_per_sm;
+    int best_t = sys->threads, best_c = sys->ctas_per_sm, best_v = sys->load_variant;
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;
     PC_CK(cudaEventCreate(&e0));
     PC_CK(cudaEventCreate(&e1));
     const bool timing = sys->timing;
     sys->timing = false;
-    for (int ti = 0; ti < 3; ++ti)
-        for (int ci = 0; ci < 6; ++ci) {
-            if (sys->structured && cand_threads[ti] > 256) continue;
-            sys->threads = cand_threads[ti];
-            sys->ctas_per_sm = cand_ctas[ci];
-            rc = build_tiles(sys);
-            if (rc) return rc;
-            rc = run_sweeps(sys, 2, 1);  // warm-up + graph instantiation
-            if (rc) return rc;
-            PC_CK(cudaEventRecord(e0, sys->stream));
-            rc = run_sweeps(sys, 5, 1);
-            if (rc) return rc;
-            PC_CK(cudaEventRecord(e1, sys->stream));
-            PC_CK(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            PC_CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best_ms) {
-                best_ms = ms;
-                best_t = cand_threads[ti];
-                best_c = cand_ctas[ci];
+    const int n_var = sys->structured ? 3 : 1;
+    for (int vi = 0; vi < n_var; ++vi)
+        for (int ti = 0; ti < 3; ++ti)
+            for (int ci = 0; ci < 6; ++ci) {
+                if (sys->structured && cand_threads[ti] > 256) continue;
+                sys->load_variant = vi;
+                sys->threads = cand_threads[ti];
+                sys->ctas_per_sm = cand_ctas[ci];
+                rc = build_tiles(sys);
+                if (rc) return rc;
+                rc = run_sweeps(sys, 2, 1);  // warm-up + graph instantiation
+                if (rc) return rc;
+                PC_CK(cudaEventRecord(e0, sys->stream));
+                rc = run_sweeps(sys, 5, 1);
+                if (rc) return rc;
+                PC_CK(cudaEventRecord(e1, sys->stream));
+                PC_CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                PC_CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best_t = cand_threads[ti];
+                    best_c = cand_ctas[ci];
+                    best_v = vi;
+                }
             }
-        }
     sys->timing = timing;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     sys->threads = best_t;
     sys->ctas_per_sm = best_c;
+    sys->load_variant = best_v;
     rc = build_tiles(sys);
     if (rc) return rc;
     PC_CK(cudaMemcpyAsync(sys->d_spins.p, saved.p, bytes, cudaMemcpyDeviceToDevice, sys->stream));

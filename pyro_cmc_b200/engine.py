@@ -157,6 +157,12 @@ class System:
         reference's visiting order); 1: fewest classes."""
         call("pc_set_colouring", self._h, int(mode))
 
+    def set_sweep_schedule(self, schedule: int):
+        """0: the reference's order (Metropolis pass, then overrelaxation
+        passes); 1: fused (Metropolis then overrelaxation per site in one
+        colour pass, sharing the local field)."""
+        call("pc_set_sweep_schedule", self._h, int(schedule))
+
     def set_kernel_path(self, force_generic: bool):
         """Force the generic bond-table kernels (True) or allow the structured
         pyrochlore kernels (False, default)."""
@@ -346,8 +352,18 @@ class System:
 
     # ---------------------------------------------------------------- tuning
     def autotune(self):
+        """Picks the fastest tile shape and neighbour-load variant by timing
+        sweeps on this system; returns (threads, ctas_per_sm, load_variant)."""
         call("pc_autotune", self._h)
-        return self.tile()
+        return (*self.tile(), self.load_variant())
+
+    def load_variant(self) -> int:
+        v = C.c_int(0)
+        call("pc_get_load_variant", self._h, C.byref(v))
+        return v.value
+
+    def set_load_variant(self, v: int):
+        call("pc_set_load_variant", self._h, int(v))
 
     def tile(self):
         t = C.c_int(0)
@@ -379,11 +395,13 @@ class System:
 
 
 def pyrochlore_system(L, J1=1.0, J2=0.0, J3=0.0, Delta=1.0, B=(0.0, 0.0, 0.0), T_ref=1.0, seed=0,
-                      n_replicas=None, split_J1=True, overrelax_mode=0, colouring=0, generic=False) -> System:
+                      n_replicas=None, split_J1=True, overrelax_mode=0, colouring=0, generic=False,
+                      schedule=0) -> System:
     """build_J1J2J3_h (include/cli_bits.hpp:144-207) on the GPU engine."""
     s = System(L, seed=seed, n_replicas=n_replicas)
     s.set_colouring(colouring)
     s.set_kernel_path(generic)
+    s.set_sweep_schedule(schedule)
     s.define_pyrochlore(J1, J2, J3, Delta, split_J1=split_J1)
     s.set_global_field(B)
     s.set_T_ref(T_ref)

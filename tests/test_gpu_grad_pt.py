@@ -187,15 +187,17 @@ def _stats_compare(a_mean, a_err, b_mean, b_err, what):
     return z
 
 
-def test_pt_equilibrium_matches_reference_tempering():
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_pt_equilibrium_matches_reference_tempering(schedule):
     """Batched GPU tempering vs the oracle's temper.cpp emulation (equilibrium
-    <e>(T) per slot, batch-mean errors over K independent runs)."""
+    <e>(T) per slot, batch-mean errors over K independent runs); for both
+    sweep schedules."""
     L, T = 2, [2.0, 1.2, 0.8, 0.5, 0.3]
     c = dict(J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1))
     K = 16
     gpu_means = []
     for k in range(K):
-        s = pc.pyrochlore_system(L, n_replicas=len(T), seed=100 + k, **c)
+        s = pc.pyrochlore_system(L, n_replicas=len(T), seed=100 + k, schedule=schedule, **c)
         s.random_spins(k)
         s.pt_configure(T)
         s.pt_run(40, 5)  # burn-in
@@ -215,7 +217,8 @@ def test_pt_equilibrium_matches_reference_tempering():
                    cpu_means.std(0, ddof=1) / np.sqrt(K), "pt <e>")
 
 
-def test_anneal_config1_statistical_parity():
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_anneal_config1_statistical_parity(schedule):
     """The plain anneal of config 1 (L=4, J1=1, T 10 -> 0.05 over 100 log steps,
     16 sweeps per step, S(q) xx/yy/zz at T in {1, 0.1, 0.05} from 64 samples,
     16 burn-in sweeps, uniform start): <e>(T), the cross-seed C_v and S(q) of K
@@ -226,7 +229,7 @@ def test_anneal_config1_statistical_parity():
     K = 32
     args = dict(L=4, J1=1.0, J2=0.0, J3=0.0, B=(0, 0, 0), T_hot=10.0, T_cold=0.05, T_sample=[1.0, 0.1, 0.05],
                 n_steps=100, n_sweep=16, n_burn_in=16, n_sample=64, corr=["xx", "yy", "zz"])
-    res = anneal_batch(K=K, seed=0xdeadbeef, **args)
+    res = anneal_batch(K=K, seed=0xdeadbeef, schedule=schedule, **args)
     e_gpu = res["e"]  # [K, n_T]
 
     def run(k):

@@ -141,20 +141,23 @@ def test_colour_classes():
     assert n == 16 and (col == np.arange(16)).all()
 
 
-@pytest.mark.parametrize("generic", [False, True])
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("path", ["generic", "v0", "v1", "v2"])
 @pytest.mark.parametrize("colouring", [0, 1])
 @pytest.mark.parametrize("T", [0.3, 2.0])
-def test_sweeps_follow_oracle_mirror(colouring, T, generic):
+def test_sweeps_follow_oracle_mirror(colouring, T, path, schedule):
     c = COUPLINGS[2]
     seed = 12345
-    g, o = pair(3, c, seed=seed, colouring=colouring, generic=generic)
+    g, o = pair(3, c, seed=seed, colouring=colouring, generic=(path == "generic"), schedule=schedule)
+    if path != "generic":
+        g.set_load_variant(int(path[1]))
     rng = np.random.default_rng(3)
     g.set_spins(unit(rng, o.N))
     o.set_spins(g.spins())
     _, col = g.colours()
     for sweep in range(3):
         acc_g = g.sweep(T, 1, 1)[0]
-        acc_o = o.sweep_philox(T, seed, 0, sweep, col, n_overrelax=1, or_mode=0)
+        acc_o = o.sweep_philox(T, seed, 0, sweep, col, n_overrelax=1, or_mode=0, fused=bool(schedule))
         Sg = g.spins()
         So = o.spins()
         assert int(acc_g) == int(acc_o)
@@ -163,16 +166,17 @@ def test_sweeps_follow_oracle_mirror(colouring, T, generic):
     assert g.sweep_counter() == 3
 
 
-def test_sweep_reflection_mode_follows_oracle():
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_sweep_reflection_mode_follows_oracle(schedule):
     c = COUPLINGS[1]
     seed = 99
-    g, o = pair(2, c, seed=seed, overrelax_mode=1)
+    g, o = pair(2, c, seed=seed, overrelax_mode=1, schedule=schedule)
     rng = np.random.default_rng(5)
     g.set_spins(unit(rng, o.N))
     o.set_spins(g.spins())
     _, col = g.colours()
     acc_g = g.sweep(0.7, 1, 2)[0]
-    acc_o = o.sweep_philox(0.7, seed, 0, 0, col, n_overrelax=2, or_mode=1)
+    acc_o = o.sweep_philox(0.7, seed, 0, 0, col, n_overrelax=2, or_mode=1, fused=bool(schedule))
     assert int(acc_g) == int(acc_o)
     # two reflections about FP32 local fields: each roughly doubles the axis
     # error of sites whose field nearly cancels
