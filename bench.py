@@ -8,8 +8,9 @@ T=0.5: 32 Metropolis+overrelaxation sweeps, an S(q) sample of all nine
 correlators after every 16 sweeps, one energy sample. A spin-update is one
 Metropolis proposal at one site (each sweep also overrelaxes every site), so a
 step is 32 * N spin-updates. Inputs are synthetic (uniform on S^2, device
-Philox). The lattice (67 MB) is smaller than L2, so the timed loop streams it
-from L2 as production runs do; between timed steps nothing is flushed.
+Philox). The lattice (67 MB) is smaller than L2 (126 MB), so a 256 MiB buffer
+is written between timed steps (outside the per-step CUDA events) and every
+step starts with a cold L2.
 
   value   device-timed steps, spins resident in HBM (CUDA events on the
           system's stream, max over ranks)
@@ -49,7 +50,7 @@ WL = dict(L=64, J1=1.0, J2=0.1, J3=0.05, B=(0.0, 0.0, 0.5), T=0.5, n_sweep=32, s
 CONFIG = {"workload": "fieldcool L=64 sampling step (32 sweeps + 2 S(q) samples x 9 correlators + energy)",
           "L": 64, "n_spins": 16 * 64 ** 3, "J": [1.0, 0.1, 0.05], "B": [0.0, 0.0, 0.5], "T": 0.5,
           "n_sweep": 32, "ssf_every": 16, "n_corr": 9, "spins": "fp32", "accumulators": "fp64",
-          "l2": "lattice (67 MB) fits in L2; no flush between steps", "parallelism": "replicas",
+          "l2": "L2 flushed between timed steps (256 MiB buffer written outside the per-step events)", "parallelism": "replicas",
           "schedule": "fused: per colour class, each site's Metropolis move then its overrelaxation move with one "
                       "local field (pc_set_sweep_schedule 1); same moves per sweep as the reference's order"}
 
@@ -104,6 +105,11 @@ class ClockSampler:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # wait (at most 3 s) for the first sample, so the timed region is covered
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def stop(self):
         if not self.proc:
@@ -170,6 +176,34 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args):
+    """One step of the workload (32 fused sweeps, two 9-correlator S(q)
+    samples, one energy) on a fresh system with a fixed tile: the launch
+    sequence is random_spins, then per sweep one struct_pass launch per colour
+    class (16), the S(q) kernels after sweeps 16 and 32, the energy kernels."""
+    import torch
+
+    import pyro_cmc_b200 as pc
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    s = pc.pyrochlore_system(WL["L"], J1=WL["J1"], J2=WL["J2"], J3=WL["J3"], B=WL["B"], seed=1000,
+                             schedule=WL["schedule"])
+    s.set_stream(stream.cuda_stream)
+    s.set_tile(args.tile[0], args.tile[1])
+    s.set_load_variant(args.tile[2])
+    s.random_spins(17)
+    s.ssf_configure(WL["corr"], 1)
+    l0 = s.launch_count()
+    for _ in range(WL["n_sweep"] // WL["ssf_every"]):
+        s.sweep(WL["T"], WL["ssf_every"], 1, count=False)
+        s.ssf_sample([0])
+    e, _ = s.energy()
+    torch.cuda.synchronize()
+    print(f"profile case: L={WL['L']} tile={args.tile} launches={s.launch_count() - l0} e={e[0]:.6f}", flush=True)
+    del s
+
+
 def cpu_baseline_one_core():
     import oracle
     b = oracle.Bench(WL["L"], WL["J1"], WL["J2"], WL["J3"], WL["B"], 1, seed=3)
@@ -185,11 +219,16 @@ def cpu_baseline_one_core():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and gradient forms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run one step of the workload with a fixed tile and no autotuning or warm-up, for ncu "
+                         "captures (prints a launch summary, no JSON line)")
+    ap.add_argument("--tile", type=int, nargs=3, default=[128, 6, 0], metavar=("THREADS", "CTAS", "VARIANT"),
+                    help="tile for --profile-case")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -199,6 +238,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.profile_case:
+        run_profile_case(args)
         return
 
     import numpy as np
@@ -243,21 +285,30 @@ def main():
             s.ssf_sample([0])
         s.energy()
 
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+
+    def timed_steps():
+        """K steps, each bracketed by CUDA events on the system's stream, L2
+        flushed before each; returns the mean step time in ms."""
+        for i in range(args.steps):
+            flush_buf.zero_()
+            starts[i].record(stream)
+            device_step()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / args.steps
+
     for _ in range(args.warmup):
         device_step()
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
     l0 = s.launch_count()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        device_step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
+    ms = timed_steps()
     launches = s.launch_count() - l0
-    ms = ev0.elapsed_time(ev1) / args.steps
+    barrier()
     clk = clocks.stop()
     ms_max = max_over_ranks(ms)
     value = world * N * WL["n_sweep"] / (ms_max * 1e-3)
@@ -268,12 +319,7 @@ def main():
     for _ in range(2):
         device_step()
     torch.cuda.synchronize()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        device_step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    ms_ref_order = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    ms_ref_order = max_over_ranks(timed_steps())
     s.set_sweep_schedule(WL["schedule"])
     device_step()
 
@@ -290,11 +336,14 @@ def main():
     for _ in range(args.warmup):
         s.step_host(S4_in, S4_out, T, WL["n_sweep"], WL["ssf_every"], 0)
     barrier()
-    t0 = time.perf_counter()
+    e2e_s = 0.0
     for _ in range(args.steps):
-        s.step_host(S4_in, S4_out, T, WL["n_sweep"], WL["ssf_every"], 0)
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    e2e_s = max_over_ranks(e2e_s)
+        flush_buf.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.step_host(S4_in, S4_out, T, WL["n_sweep"], WL["ssf_every"], 0)  # returns after the D2H copy
+        e2e_s += time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s / args.steps)
     e2e = {"value": world * N * WL["n_sweep"] / e2e_s, "unit": UNIT, "h2d_bytes_per_step": N * 16,
            "d2h_bytes_per_step": N * 16 + 8, "ms_per_step": e2e_s * 1e3,
            "call": "pc_step_host (pinned host spins in/out)"}
@@ -375,6 +424,33 @@ def run_extras(pc, torch, np):
                                 "J=(1,0,0.02), B=(0,0,0.1), exchange every 10 sweeps, S(q) xx/yy/zz every 16 sweeps",
                       "ms_per_10_sweeps": ms / rounds, "tile": list(btile), "exchange_accept": float(acc.sum()) / max(1.0, float(att.sum())),
                       "plain_single_L8": plain_small, "batched_over_plain_L8": batched / plain_small}
+    # plain single replica of the L=16 anneal: one sampling step = 16 sweeps +
+    # one S(q) sample of the anneal's six correlators
+    a = pc.pyrochlore_system(16, J1=1.0, J2=-0.1, J3=0.05, B=(0, 0, 0), seed=21, schedule=WL["schedule"])
+    a.set_stream(stream.cuda_stream)
+    a.random_spins(2)
+    atile = a.autotune()
+    a.ssf_configure(["xx", "yy", "zz", "xy", "xz", "yz"], 1)
+
+    def a_step():
+        a.sweep(0.5, 16, 1, count=False)
+        a.ssf_sample([0])
+
+    for _ in range(5):
+        a_step()
+    torch.cuda.synchronize()
+    n_a = 50
+    e0.record(stream)
+    for _ in range(n_a):
+        a_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    a_ms = e0.elapsed_time(e1) / n_a
+    out["plain_L16"] = {"value": a.N() * 16 / (a_ms * 1e-3), "unit": UNIT,
+                        "config": "anneal L=16 (65,536 spins), J=(1,-0.1,0.05), B=0, T=0.5; step = 16 sweeps + "
+                                  "one S(q) sample (xx,yy,zz,xy,xz,yz)",
+                        "ms_per_step": a_ms, "tile": list(atile)}
+    del a
     # gradient form: 256 x L=8 energy + S^zz(q) forward/backward
     from pyro_cmc_b200 import autograd as ag
     B = 256

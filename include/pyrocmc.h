@@ -274,7 +274,8 @@ int pc_autotune(pc_system* sys);
  * 0 group by group (fewest registers), 1 all at once, 2 in two batches. */
 int pc_set_load_variant(pc_system* sys, int variant);
 int pc_get_load_variant(pc_system* sys, int* variant);
-/* Current tile shape (threads per CTA, CTAs per SM). */
+/* Current tile shape (threads per CTA, CTAs per SM). CTAs per SM = 0 launches
+ * one CTA per tile instead of a grid of SMs x CTAs striding over the tiles. */
 int pc_get_tile(pc_system* sys, int* threads, int* ctas_per_sm);
 int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm);
 
@@ -292,6 +293,12 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
 int pc_last_kernel_times(pc_system* sys, double* metropolis_ms, double* overrelax_ms);
 /* Enables per-kernel CUDA-event timing (off by default). */
 int pc_set_kernel_timing(pc_system* sys, int on);
+/* Launch overlap of consecutive colour passes (on by default): each pass is
+ * launched with programmatic dependent launch and waits in-kernel for the
+ * previous kernel's completion before reading spins, so its launch overlaps
+ * the previous pass's tail. 0 launches them in plain stream order. Results are
+ * identical either way. No counterpart in the reference (a launch setting). */
+int pc_set_launch_overlap(pc_system* sys, int on);
 
 #ifdef __cplusplus
 }

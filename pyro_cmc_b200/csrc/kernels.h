@@ -45,7 +45,9 @@ struct PassArgs {
     PyroMats mats;
 };
 
-void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st);
+// pdl: launch with programmatic dependent launch (the kernel waits for the
+// previous kernel on the stream with griddepcontrol.wait before touching spins)
+void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl = false);
 
 struct EnergyArgs {
     const float4* spins;

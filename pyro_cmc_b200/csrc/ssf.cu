@@ -20,7 +20,10 @@
 // accumulators.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
+#include "dft.cuh"
 #include "kernels.h"
 
 namespace pc {
@@ -116,7 +119,7 @@ __device__ void ct_half(const float2* __restrict__ in, float2* __restrict__ out,
 
 // Full 1-D transform of all lines, result back in `a` (b is scratch).
 template <bool INV>
-__device__ __forceinline__ void dft_lines(float2* a, float2* b, int L, int P, int Q, int n_lines, int lstride,
+__device__ __forceinline__ void dft_lines_generic(float2* a, float2* b, int L, int P, int Q, int n_lines, int lstride,
                                           int estride, const float2* tw, bool line_fast) {
     ct_half<false, INV>(a, b, L, P, Q, n_lines, lstride, estride, tw, line_fast);
     __syncthreads();
@@ -124,7 +127,191 @@ __device__ __forceinline__ void dft_lines(float2* a, float2* b, int L, int P, in
     __syncthreads();
 }
 
-// ------------------------------------------------------------------ stage 1
+// ------------------------------------------------------- fast path, P, Q <= 8
+// Stage 1, one CTA per (replica, z plane, z group, pair of the group's
+// sublattices s0, s1). The six real planes of the pair become three complex
+// planes, A0 = Sx0 + i Sy0, A1 = Sx1 + i Sy1, Az = Sz0 + i Sz1, whose 2-D DFTs
+// are split again by Hermitian symmetry (F real => F(-K) = conj F(K)):
+//   X0 = (A0(K) + conj A0(-K)) / 2,  Y0 = (A0(K) - conj A0(-K)) / 2i, ...
+// Each component's X0 e^{-i q.r_s0} + X1 e^{-i q.r_s1} (x, y parts of the
+// phase) goes to its own half-group plane of G; stage 2 adds the two halves of
+// a group. G layout: [replica][component][2 gz + pair][nz][Ky][Kx].
+//
+// Plane layout in shared memory: element (x, y) at y L + sw(x, y). With L a
+// multiple of 16, sw swaps 8-element blocks by the parity of y and permutes
+// inside a block by the block index, so the row passes (one thread per 8-element
+// stretch) and the column passes (consecutive x) are free of bank conflicts at
+// L = 64.
+template <bool SWZ>
+__device__ __forceinline__ int plane_pos(int x, int y, int L) {
+    if constexpr (SWZ)
+        return y * L + ((((x >> 3) ^ (y & 1)) << 3) | ((x & 7) ^ ((x >> 3) & 7)));
+    else
+        return y * L + x;
+}
+
+__host__ __device__ __forceinline__ bool ssf_fast_path(int P, int Q) { return P <= kMaxRadix && Q <= kMaxRadix; }
+
+template <bool SWZ>
+__global__ void __launch_bounds__(512) ssf_plane_kernel(const SsfGeom g, const float4* __restrict__ spins,
+                                                        const ReplicaDev* __restrict__ reps, float2* __restrict__ G) {
+    extern __shared__ float2 sm[];
+    const int L = g.L, LL = L * L, P = g.P, Q = g.Q;
+    float2* tw = sm;
+    float2* ph = tw + L;
+    float2* buf = ph + 8 * L;  // planes A0, A1, Az
+    const int h = blockIdx.x & 7, gz = h >> 1, pr = h & 1;
+    const int nz = (blockIdx.x >> 3) % L;
+    const int rp = (blockIdx.x >> 3) / L;
+    const ReplicaDev rep = reps[g.rep_index[rp]];
+    const int s0 = c_zgroup[gz][2 * pr], s1 = c_zgroup[gz][2 * pr + 1];
+    const float4* p0 = spins + rep.off + size_t(s0) * rep.Nc + size_t(nz) * LL;
+    const float4* p1 = spins + rep.off + size_t(s1) * rep.Nc + size_t(nz) * LL;
+    fill_tables(tw, ph, L);
+    for (int i = threadIdx.x; i < LL; i += blockDim.x) {
+        const int y = i / L, x = i - y * L;
+        const float4 a = p0[i], b = p1[i];
+        const int q = plane_pos<SWZ>(x, y, L);
+        buf[q] = make_float2(a.x, a.y);
+        buf[LL + q] = make_float2(b.x, b.y);
+        buf[2 * LL + q] = make_float2(a.z, b.z);
+    }
+    __syncthreads();
+    const int lpr = max(1, int(kPassBItems * blockDim.x) / P);
+    auto row = [=](int l, int e) {  // line (plane b, row y), element x
+        const int b = l / L;
+        return b * LL + plane_pos<SWZ>(e, l - b * L, L);
+    };
+    dft_lines<false, false>(buf, P, Q, 3 * L, lpr, row, tw);
+    auto col = [=](int l, int e) {  // line (plane b, column x), element y
+        const int b = l / L;
+        return b * LL + plane_pos<SWZ>(l - b * L, e, L);
+    };
+    dft_lines<false, true>(buf, P, Q, 3 * L, lpr, col, tw);
+    const int rx0 = c_rsl[s0][0], ry0 = c_rsl[s0][1], rx1 = c_rsl[s1][0], ry1 = c_rsl[s1][1];
+    const size_t L3 = size_t(L) * LL;
+    float2* Gx = G + ((size_t(rp) * 3) * 8 + h) * L3 + size_t(nz) * LL;
+    float2* Gy = Gx + 8 * L3;
+    float2* Gz = Gy + 8 * L3;
+    for (int i = threadIdx.x; i < LL; i += blockDim.x) {
+        const int Ky = i / L, Kx = i - Ky * L;
+        const int q = plane_pos<SWZ>(Kx, Ky, L);
+        const int qm = plane_pos<SWZ>(Kx ? L - Kx : 0, Ky ? L - Ky : 0, L);
+        const float2 a = buf[q], am = buf[qm];
+        const float2 b = buf[LL + q], bm = buf[LL + qm];
+        const float2 z = buf[2 * LL + q], zm = buf[2 * LL + qm];
+        const float2 e0 = cmul(phase(ph, L, Kx * rx0), phase(ph, L, Ky * ry0));
+        const float2 e1 = cmul(phase(ph, L, Kx * rx1), phase(ph, L, Ky * ry1));
+        // (F + conj F-)/2 and (F - conj F-)/2i
+        const float2 X0 = make_float2(0.5f * (a.x + am.x), 0.5f * (a.y - am.y));
+        const float2 Y0 = make_float2(0.5f * (a.y + am.y), -0.5f * (a.x - am.x));
+        const float2 X1 = make_float2(0.5f * (b.x + bm.x), 0.5f * (b.y - bm.y));
+        const float2 Y1 = make_float2(0.5f * (b.y + bm.y), -0.5f * (b.x - bm.x));
+        const float2 Z0 = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+        const float2 Z1 = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+        const float2 u0 = cmul(X0, e0), u1 = cmul(X1, e1);
+        const float2 v0 = cmul(Y0, e0), v1 = cmul(Y1, e1);
+        const float2 w0 = cmul(Z0, e0), w1 = cmul(Z1, e1);
+        Gx[i] = make_float2(u0.x + u1.x, u0.y + u1.y);
+        Gy[i] = make_float2(v0.x + v1.x, v0.y + v1.y);
+        Gz[i] = make_float2(w0.x + w1.x, w0.y + w1.y);
+    }
+}
+
+__host__ __device__ __forceinline__ int ssf_chunk(int L) { return L < 16 ? L : 16; }
+
+// Stage 2, one CTA per (replica, Ky, chunk of C Kx values): the z-DFT of the
+// 12 (component, z group) line sets, the z part of the phase, the sum over
+// groups -> B^a(K), then the correlators and the FP64 accumulators. Shared
+// layout T[(a*4 + gz)][z][CP], CP = C + 1 (odd row stride: the per-K reads
+// with consecutive Kz hit distinct banks).
+__global__ void __launch_bounds__(512) ssf_line_kernel(const SsfGeom g, const float2* __restrict__ G, const SsfOut o) {
+    extern __shared__ float2 sm[];
+    const int L = g.L, LL = L * L, P = g.P, Q = g.Q;
+    const int C = ssf_chunk(L), CP = C + 1;
+    const int n_chunk = (L + C - 1) / C;
+    float2* tw = sm;
+    float2* ph = tw + L;
+    float2* T = ph + 8 * L;
+    const int chunk = blockIdx.x % n_chunk;
+    const int Ky = (blockIdx.x / n_chunk) % L;
+    const int rp = (blockIdx.x / n_chunk) / L;
+    const int Kx0 = chunk * C;
+    const int nc = min(C, L - Kx0);
+    const size_t L3 = size_t(L) * LL;
+    fill_tables(tw, ph, L);
+    for (int i = threadIdx.x; i < 12 * L * C; i += blockDim.x) {
+        const int c = i % C, zr = i / C;  // zr = (a*4 + gz) * L + z
+        const int ag = zr / L, z = zr - ag * L;
+        float2 v = make_float2(0.f, 0.f);
+        if (c < nc) {
+            const int a = ag >> 2, gz = ag & 3;
+            const float2* src = G + ((size_t(rp) * 3 + a) * 8 + 2 * gz) * L3 + size_t(z) * LL + size_t(Ky) * L + Kx0 + c;
+            const float2 u = src[0], w = src[L3];  // the group's two sublattice pairs
+            v = make_float2(u.x + w.x, u.y + w.y);
+        }
+        T[zr * CP + c] = v;
+    }
+    __syncthreads();
+    const int lpr = max(1, int(kPassBItems * blockDim.x) / P);
+    auto zl = [=](int l, int e) {  // line (a*4 + gz, c), element z
+        const int ag = l / C;
+        return (ag * L + e) * CP + (l - ag * C);
+    };
+    dft_lines<false, true>(T, P, Q, 12 * C, lpr, zl, tw);
+    const int rep_glob = g.rep_index[rp];
+    const int n_k = L * LL;
+    const int slot = o.acc_sum ? o.slot_of_rep[rep_glob] : -1;
+    for (int i = threadIdx.x; i < L * nc; i += blockDim.x) {
+        const int c = i / L, Kz = i - c * L;
+        float2 B[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int gz = 0; gz < 4; ++gz) {
+                const float2 v = cmul(T[((a * 4 + gz) * L + Kz) * CP + c], phase(ph, L, Kz * (2 * gz - 1)));
+                acc.x += v.x;
+                acc.y += v.y;
+            }
+            B[a] = acc;
+        }
+        const size_t k = (size_t(Kx0 + c) * L + Ky) * L + Kz;
+        if (o.amp)
+            for (int a = 0; a < 3; ++a) o.amp[(size_t(rp) * 3 + a) * n_k + k] = B[a];
+        if (o.val || slot >= 0)
+#pragma unroll
+            for (int cc = 0; cc < 9; ++cc) {  // unrolled: constant indices into the parameter arrays
+                if (cc >= o.n_corr) break;
+                const int ca = o.corr_a[cc], cb = o.corr_b[cc];  // selects keep B[] in registers
+                const float2 ba = ca == 0 ? B[0] : (ca == 1 ? B[1] : B[2]);
+                const float2 bb = cb == 0 ? B[0] : (cb == 1 ? B[1] : B[2]);
+                // conj(B^a) B^b
+                const double re = double(ba.x) * bb.x + double(ba.y) * bb.y;
+                const double im = double(ba.x) * bb.y - double(ba.y) * bb.x;
+                if (o.val) {
+                    double2* v = reinterpret_cast<double2*>(o.val + ((size_t(rp) * o.n_corr + cc) * n_k + k) * 2);
+                    *v = make_double2(re, im);
+                }
+                if (slot >= 0) {
+                    double2* s = reinterpret_cast<double2*>(o.acc_sum + size_t(slot) * o.slot_stride +
+                                                            (size_t(cc) * n_k + k) * 2);
+                    double2* q = reinterpret_cast<double2*>(o.acc_sq + size_t(slot) * o.slot_stride +
+                                                            (size_t(cc) * n_k + k) * 2);
+                    double2 sv = *s, qv = *q;
+                    sv.x += re;
+                    sv.y += im;
+                    qv.x += re * re;
+                    qv.y += im * im;
+                    *s = sv;
+                    *q = qv;
+                }
+            }
+    }
+}
+
+// ------------------------------------------------ generic path, P or Q > 8
+// stage 1: per (replica, z plane, z group), runtime-length DFT loops
 __global__ void __launch_bounds__(256) ssf_xy_kernel(const SsfGeom g, const float4* __restrict__ spins,
                                                      const ReplicaDev* reps, float2* __restrict__ G) {
     extern __shared__ float2 sm[];
@@ -151,8 +338,8 @@ __global__ void __launch_bounds__(256) ssf_xy_kernel(const SsfGeom g, const floa
                 w0[i] = make_float2(a == 0 ? v.x : (a == 1 ? v.y : v.z), 0.f);
             }
             __syncthreads();
-            dft_lines<false>(w0, w1, L, g.P, g.Q, L, L, 1, tw, false);  // along x (rows)
-            dft_lines<false>(w0, w1, L, g.P, g.Q, L, 1, L, tw, true);   // along y (columns)
+            dft_lines_generic<false>(w0, w1, L, g.P, g.Q, L, L, 1, tw, false);  // along x (rows)
+            dft_lines_generic<false>(w0, w1, L, g.P, g.Q, L, 1, L, tw, true);   // along y (columns)
             const int rx = c_rsl[sl][0], ry = c_rsl[sl][1];
             for (int i = threadIdx.x; i < LL; i += blockDim.x) {
                 const int Kx = i % L, Ky = i / L;
@@ -169,11 +356,23 @@ __global__ void __launch_bounds__(256) ssf_xy_kernel(const SsfGeom g, const floa
     }
 }
 
-__host__ __device__ __forceinline__ int ssf_chunk(int L) { return L < 16 ? L : 16; }
+int ssf_plane_threads(int L) { return std::min(512, std::max(64, (L * L / 8 + 31) / 32 * 32)); }
+int ssf_line_threads(int L, int P, int Q) {
+    const int items = 12 * ssf_chunk(L) * std::max(P, Q) / 4;
+    return std::min(512, std::max(64, (items + 31) / 32 * 32));
+}
 
 void launch_ssf_xy(const SsfGeom& g, const float4* spins, const ReplicaDev* reps, float2* G, cudaStream_t st) {
     const int L = g.L;
     const size_t smem = sizeof(float2) * (size_t(9) * L + 3 * size_t(L) * L);
+    if (ssf_fast_path(g.P, g.Q)) {
+        const int threads = ssf_plane_threads(L);
+        if (L % 16 == 0)
+            ssf_plane_kernel<true><<<g.n_rep * L * 8, threads, smem, st>>>(g, spins, reps, G);
+        else
+            ssf_plane_kernel<false><<<g.n_rep * L * 8, threads, smem, st>>>(g, spins, reps, G);
+        return;
+    }
     ssf_xy_kernel<<<g.n_rep * L * 4, 256, smem, st>>>(g, spins, reps, G);
 }
 
@@ -205,7 +404,7 @@ __global__ void __launch_bounds__(256) ssf_z_kernel(const SsfGeom g, const float
                 w0[i] = c < nc ? src[size_t(nz) * LL + c] : make_float2(0.f, 0.f);
             }
             __syncthreads();
-            dft_lines<false>(w0, w1, L, g.P, g.Q, C, 1, C, tw, true);  // along z
+            dft_lines_generic<false>(w0, w1, L, g.P, g.Q, C, 1, C, tw, true);  // along z
             const int rz = 2 * gz - 1;
             for (int i = threadIdx.x; i < L * C; i += blockDim.x) {
                 const int Kz = i / C;
@@ -259,6 +458,11 @@ __global__ void __launch_bounds__(256) ssf_z_kernel(const SsfGeom g, const float
 void launch_ssf_z(const SsfGeom& g, const float2* G, const SsfOut& o, cudaStream_t st) {
     const int L = g.L, C = ssf_chunk(L);
     const int n_chunk = (L + C - 1) / C;
+    if (ssf_fast_path(g.P, g.Q)) {
+        const size_t smem = sizeof(float2) * (size_t(9) * L + 12 * size_t(L) * (C + 1));
+        ssf_line_kernel<<<g.n_rep * L * n_chunk, ssf_line_threads(L, g.P, g.Q), smem, st>>>(g, G, o);
+        return;
+    }
     const size_t smem = sizeof(float2) * (size_t(9) * L + 5 * size_t(L) * C);
     ssf_z_kernel<<<g.n_rep * L * n_chunk, 256, smem, st>>>(g, G, o);
 }
@@ -316,7 +520,7 @@ __global__ void __launch_bounds__(256) ssf_adj_z_kernel(const SsfGeom g, const S
                 w0[i] = cmulc(Y[a * L * C + i], phase(ph, L, Kz * rz));  // times exp(+i qz rz)
             }
             __syncthreads();
-            dft_lines<true>(w0, w1, L, g.P, g.Q, C, 1, C, tw, true);
+            dft_lines_generic<true>(w0, w1, L, g.P, g.Q, C, 1, C, tw, true);
             float2* dst = H + ((size_t(rp) * 3 + a) * 4 + gz) * size_t(L) * LL + size_t(Ky) * L + Kx0;
             for (int i = threadIdx.x; i < L * nc; i += blockDim.x) {
                 const int c = i % nc, nz = i / nc;
@@ -356,8 +560,8 @@ __global__ void __launch_bounds__(256) ssf_adj_xy_kernel(const SsfGeom g, const 
                 w0[i] = cmulc(hp[i], p);
             }
             __syncthreads();
-            dft_lines<true>(w0, w1, L, g.P, g.Q, L, 1, L, tw, true);   // along y
-            dft_lines<true>(w0, w1, L, g.P, g.Q, L, L, 1, tw, false);  // along x
+            dft_lines_generic<true>(w0, w1, L, g.P, g.Q, L, 1, L, tw, true);   // along y
+            dft_lines_generic<true>(w0, w1, L, g.P, g.Q, L, L, 1, tw, false);  // along x
             float* dst = grad + 4 * (size_t(rep.off) + size_t(sl) * rep.Nc + size_t(nz) * LL) + a;
             for (int i = threadIdx.x; i < LL; i += blockDim.x) dst[4 * size_t(i)] = w0[i].x;
         }
@@ -365,6 +569,9 @@ __global__ void __launch_bounds__(256) ssf_adj_xy_kernel(const SsfGeom g, const 
 }
 
 void ssf_prepare() {
+    cudaFuncSetAttribute(ssf_plane_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(ssf_plane_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(ssf_line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(ssf_xy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(ssf_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(ssf_adj_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -169,12 +169,21 @@ __device__ __forceinline__ void flush_accepted(const PassArgs& a, unsigned int& 
     mine = 0;
 }
 
+// Programmatic dependent launch: let the next kernel on the stream start its
+// launch now, then wait until the previous kernel has finished and its writes
+// are visible (both are no-ops for a kernel launched without the attribute).
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Generic colour pass: bond tables (any coupling set) staged in shared memory.
 template <int MODE>
 __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant__ PassArgs a) {
     __shared__ SlTable tab[4];
     __shared__ unsigned int warp_acc[16];
-    stage_tables(tab, a.tables, a.n_tab, a.tab_sl);
+    stage_tables(tab, a.tables, a.n_tab, a.tab_sl);  // tables are never written by kernels
+    pdl_enter();
     __syncthreads();
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
     unsigned int mine = 0;
@@ -332,6 +341,7 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
 template <int MODE, int VAR>
 __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant__ PassArgs a) {
     __shared__ unsigned int warp_acc[8];
+    pdl_enter();
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
     unsigned int mine = 0;
     int r_cur = -1;
@@ -356,35 +366,50 @@ __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant_
     if ((MODE == kMetropolis || MODE >= kFusedRotate) && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
 }
 
+template <typename Kern>
+static void launch_pass(Kern k, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(threads));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, a);
+}
+
 template <int VAR>
-static void launch_struct(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st) {
+static void launch_struct(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl) {
     switch (mode) {
-        case kMetropolis: struct_pass_kernel<kMetropolis, VAR><<<grid, threads, 0, st>>>(a); break;
-        case kOverrelaxRotate: struct_pass_kernel<kOverrelaxRotate, VAR><<<grid, threads, 0, st>>>(a); break;
-        case kOverrelaxReflect: struct_pass_kernel<kOverrelaxReflect, VAR><<<grid, threads, 0, st>>>(a); break;
-        case kOverrelaxTheta: struct_pass_kernel<kOverrelaxTheta, VAR><<<grid, threads, 0, st>>>(a); break;
-        case kFusedRotate: struct_pass_kernel<kFusedRotate, VAR><<<grid, threads, 0, st>>>(a); break;
-        case kFusedReflect: struct_pass_kernel<kFusedReflect, VAR><<<grid, threads, 0, st>>>(a); break;
+        case kMetropolis: launch_pass(struct_pass_kernel<kMetropolis, VAR>, a, grid, threads, st, pdl); break;
+        case kOverrelaxRotate: launch_pass(struct_pass_kernel<kOverrelaxRotate, VAR>, a, grid, threads, st, pdl); break;
+        case kOverrelaxReflect: launch_pass(struct_pass_kernel<kOverrelaxReflect, VAR>, a, grid, threads, st, pdl); break;
+        case kOverrelaxTheta: launch_pass(struct_pass_kernel<kOverrelaxTheta, VAR>, a, grid, threads, st, pdl); break;
+        case kFusedRotate: launch_pass(struct_pass_kernel<kFusedRotate, VAR>, a, grid, threads, st, pdl); break;
+        case kFusedReflect: launch_pass(struct_pass_kernel<kFusedReflect, VAR>, a, grid, threads, st, pdl); break;
     }
 }
 
-void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st) {
+void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl) {
     if (a.structured && threads <= 256) {
         if (a.load_variant == 1)
-            launch_struct<1>(mode, a, grid, threads, st);
+            launch_struct<1>(mode, a, grid, threads, st, pdl);
         else if (a.load_variant == 2)
-            launch_struct<2>(mode, a, grid, threads, st);
+            launch_struct<2>(mode, a, grid, threads, st, pdl);
         else
-            launch_struct<0>(mode, a, grid, threads, st);
+            launch_struct<0>(mode, a, grid, threads, st, pdl);
         return;
     }
     switch (mode) {
-        case kMetropolis: colour_pass_kernel<kMetropolis><<<grid, threads, 0, st>>>(a); break;
-        case kOverrelaxRotate: colour_pass_kernel<kOverrelaxRotate><<<grid, threads, 0, st>>>(a); break;
-        case kOverrelaxReflect: colour_pass_kernel<kOverrelaxReflect><<<grid, threads, 0, st>>>(a); break;
-        case kOverrelaxTheta: colour_pass_kernel<kOverrelaxTheta><<<grid, threads, 0, st>>>(a); break;
-        case kFusedRotate: colour_pass_kernel<kFusedRotate><<<grid, threads, 0, st>>>(a); break;
-        case kFusedReflect: colour_pass_kernel<kFusedReflect><<<grid, threads, 0, st>>>(a); break;
+        case kMetropolis: launch_pass(colour_pass_kernel<kMetropolis>, a, grid, threads, st, pdl); break;
+        case kOverrelaxRotate: launch_pass(colour_pass_kernel<kOverrelaxRotate>, a, grid, threads, st, pdl); break;
+        case kOverrelaxReflect: launch_pass(colour_pass_kernel<kOverrelaxReflect>, a, grid, threads, st, pdl); break;
+        case kOverrelaxTheta: launch_pass(colour_pass_kernel<kOverrelaxTheta>, a, grid, threads, st, pdl); break;
+        case kFusedRotate: launch_pass(colour_pass_kernel<kFusedRotate>, a, grid, threads, st, pdl); break;
+        case kFusedReflect: launch_pass(colour_pass_kernel<kFusedReflect>, a, grid, threads, st, pdl); break;
     }
 }
 
@@ -483,10 +508,8 @@ __global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constan
 }
 
 void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = a.n_tiles < sms * 4 ? a.n_tiles : sms * 4;
+    // one CTA per tile: many resident CTAs per SM hide the neighbour-gather latency
+    const int grid = a.n_tiles;
     if (a.structured && threads <= 256)
         energy_struct_kernel<<<grid, threads, 0, st>>>(a);
     else
@@ -496,15 +519,22 @@ void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st) {
 // One block per replica: each thread sums a fixed strided subset of the
 // replica's tile partials, then a fixed-shape tree combines them, so the
 // result does not depend on scheduling (deterministic).
-__global__ void __launch_bounds__(256) energy_finalize_kernel(const double* partial, const int32_t* tb,
+__global__ void __launch_bounds__(1024) energy_finalize_kernel(const double* partial, const int32_t* tb,
                                                               const int32_t* te, const ReplicaDev* reps, int R,
                                                               double* e, double* mag) {
     __shared__ double red[4 * 32];
     const int r = blockIdx.x;
     if (r >= R) return;
     double v[4] = {0, 0, 0, 0};
-    for (int t = tb[r] + int(threadIdx.x); t < te[r]; t += blockDim.x)
-        for (int j = 0; j < 4; ++j) v[j] += partial[size_t(t) * 4 + j];
+    const double4* p4 = reinterpret_cast<const double4*>(partial);
+#pragma unroll 8
+    for (int t = tb[r] + int(threadIdx.x); t < te[r]; t += blockDim.x) {
+        const double4 q = p4[t];
+        v[0] += q.x;
+        v[1] += q.y;
+        v[2] += q.z;
+        v[3] += q.w;
+    }
     block_sum<4>(v, red);
     if (threadIdx.x == 0) {
         e[r] = v[0] / double(reps[r].Nc);
@@ -515,7 +545,7 @@ __global__ void __launch_bounds__(256) energy_finalize_kernel(const double* part
 
 void launch_energy_finalize(const double* partial, const int32_t* tile_begin, const int32_t* tile_end,
                             const ReplicaDev* reps, int R, double* e, double* mag, cudaStream_t st) {
-    energy_finalize_kernel<<<R, 256, 0, st>>>(partial, tile_begin, tile_end, reps, R, e, mag);
+    energy_finalize_kernel<<<R, 1024, 0, st>>>(partial, tile_begin, tile_end, reps, R, e, mag);
 }
 
 __global__ void __launch_bounds__(512) local_field_kernel(const FieldArgs a) {
@@ -622,10 +652,7 @@ __global__ void __launch_bounds__(256) energy_grad_kernel(const GradArgs a) {
 }
 
 void launch_energy_grad_partials(const GradArgs& a, int threads, cudaStream_t st) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = a.n_tiles < sms * 4 ? a.n_tiles : sms * 4;
+    const int grid = a.n_tiles;  // one CTA per tile
     const size_t smem = sizeof(double) * size_t(4 + 9 * a.n_spec);
     energy_grad_kernel<<<grid, threads, smem, st>>>(a);
 }

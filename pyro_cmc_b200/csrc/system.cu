@@ -173,7 +173,8 @@ struct pc_system {
     uint64_t launches = 0;
 
     // sweep graph cache, keyed by n_overrelax
-    std::map<int, std::pair<cudaGraphExec_t, int>> sweep_graphs;
+    std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> sweep_graphs;  // (n_or, sweeps) -> (graph, nodes)
+    bool pdl = true;  // colour passes launched with programmatic dependent launch
 
     // kernel timing
     bool timing = false;
@@ -482,7 +483,11 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     return a;
 }
 
-int grid_for(pc_system* s, int n_tiles) { return std::max(1, std::min(n_tiles, s->sms * s->ctas_per_sm)); }
+// ctas_per_sm = 0: one CTA per tile (the hardware balances the waves)
+int grid_for(pc_system* s, int n_tiles) {
+    if (s->ctas_per_sm == 0) return std::max(1, n_tiles);
+    return std::max(1, std::min(n_tiles, s->sms * s->ctas_per_sm));
+}
 
 // Launches one sweep's passes (sweep offset `off` relative to *d_sweep).
 int enqueue_sweep(pc_system* s, uint64_t off, int n_or, bool record_events) {
@@ -511,7 +516,7 @@ int enqueue_sweep(pc_system* s, uint64_t off, int n_or, bool record_events) {
         const pc::PassArgs a = pass_args(s, c, off, 0);
         int rc = record(0, true);
         if (rc) return rc;
-        pc::launch_colour_pass(mm, a, grid_for(s, a.n_tiles), s->threads, s->stream);
+        pc::launch_colour_pass(mm, a, grid_for(s, a.n_tiles), s->threads, s->stream, s->pdl);
         PC_LAUNCH_CK();
         rc = record(0, false);
         if (rc) return rc;
@@ -523,7 +528,7 @@ int enqueue_sweep(pc_system* s, uint64_t off, int n_or, bool record_events) {
             const pc::PassArgs a = pass_args(s, c, off, k);
             int rc = record(1, true);
             if (rc) return rc;
-            pc::launch_colour_pass(om, a, grid_for(s, a.n_tiles), s->threads, s->stream);
+            pc::launch_colour_pass(om, a, grid_for(s, a.n_tiles), s->threads, s->stream, s->pdl);
             PC_LAUNCH_CK();
             rc = record(1, false);
             if (rc) return rc;
@@ -532,9 +537,12 @@ int enqueue_sweep(pc_system* s, uint64_t off, int n_or, bool record_events) {
     return PC_OK;
 }
 
-// A captured graph of one sweep plus the counter advance; nodes = kernels.
-int sweep_graph(pc_system* s, int n_or, cudaGraphExec_t* exec, int* nodes) {
-    auto it = s->sweep_graphs.find(n_or);
+// A captured graph of k sweeps (sweep offsets 0..k-1 from *d_sweep) plus one
+// counter advance by k; nodes = kernels.
+constexpr int kGraphSweeps = 16;
+int sweep_graph(pc_system* s, int n_or, int k, cudaGraphExec_t* exec, int* nodes) {
+    const auto key = std::make_pair(n_or, k);
+    auto it = s->sweep_graphs.find(key);
     if (it != s->sweep_graphs.end()) {
         *exec = it->second.first;
         *nodes = it->second.second;
@@ -542,18 +550,24 @@ int sweep_graph(pc_system* s, int n_or, cudaGraphExec_t* exec, int* nodes) {
     }
     const uint64_t before = s->launches;
     PC_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_sweep(s, 0, n_or, false);
-    pc::launch_advance_counter(s->d_sweep.p, 1, s->stream);
+    int rc = PC_OK;
+    for (int i = 0; i < k && rc == PC_OK; ++i) rc = enqueue_sweep(s, uint64_t(i), n_or, false);
+    pc::launch_advance_counter(s->d_sweep.p, uint64_t(k), s->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
-    if (rc) return rc;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        s->launches = before;
+        return rc;
+    }
     if (e != cudaSuccess) return fail(PC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     cudaGraphExec_t x = nullptr;
-    PC_CK(cudaGraphInstantiate(&x, g, 0));
+    e = cudaGraphInstantiate(&x, g, 0);
     cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(PC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     const int n = int(s->launches - before) + 1;
     s->launches = before;  // capture launched nothing
-    s->sweep_graphs[n_or] = {x, n};
+    s->sweep_graphs[key] = {x, n};
     *exec = x;
     *nodes = n;
     return PC_OK;
@@ -569,13 +583,16 @@ int run_sweeps(pc_system* s, int n_sweeps, int n_or) {
         PC_LAUNCH_CK();
         s->launches++;
     } else {
-        cudaGraphExec_t g;
-        int nodes;
-        int rc = sweep_graph(s, n_or, &g, &nodes);
-        if (rc) return rc;
-        for (int i = 0; i < n_sweeps; ++i) {
+        int done = 0;
+        while (done < n_sweeps) {
+            const int k = std::min(kGraphSweeps, n_sweeps - done);
+            cudaGraphExec_t g;
+            int nodes;
+            int rc = sweep_graph(s, n_or, k, &g, &nodes);
+            if (rc) return rc;
             PC_CK(cudaGraphLaunch(g, s->stream));
             s->launches += uint64_t(nodes);
+            done += k;
         }
     }
     s->host_sweep += uint64_t(n_sweeps);
@@ -656,7 +673,7 @@ int ensure_groups(pc_system* s) {
         PC_CK(g.d_rep_index.alloc(g.reps.size()));
         PC_CK(cudaMemcpy(g.d_rep_index.p, g.reps.data(), sizeof(int32_t) * g.reps.size(), cudaMemcpyHostToDevice));
         const size_t L3 = size_t(g.L) * g.L * g.L;
-        PC_CK(g.d_G.alloc(g.reps.size() * 12 * L3));
+        PC_CK(g.d_G.alloc(g.reps.size() * 24 * L3));  // 3 components x 8 half-groups
     }
     return PC_OK;
 }
@@ -818,6 +835,14 @@ int pc_set_sweep_schedule(pc_system* sys, int schedule) {
     if (rc) return rc;
     if (schedule != 0 && schedule != 1) return fail(PC_ERR_INVALID, "sweep schedule must be 0 (reference order) or 1 (fused)");
     sys->schedule = schedule;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_set_launch_overlap(pc_system* sys, int on) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    sys->pdl = on != 0;
     sys->drop_graphs();
     return PC_OK;
 }
@@ -1629,7 +1654,8 @@ int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm) {
     int rc = check_sys(sys, false);
     if (rc) return rc;
     if (threads < 32 || threads > 512 || threads % 32 != 0) return fail(PC_ERR_INVALID, "threads must be 32..512, a multiple of 32");
-    if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(PC_ERR_INVALID, "ctas_per_sm must be 1..32");
+    if (ctas_per_sm < 0 || ctas_per_sm > 32)
+        return fail(PC_ERR_INVALID, "ctas_per_sm must be 0 (one CTA per tile) or 1..32");
     sys->threads = threads;
     sys->ctas_per_sm = ctas_per_sm;
     if (sys->ready) return build_tiles(sys);
@@ -1665,8 +1691,9 @@ int pc_autotune(pc_system* sys) {
     PC_CK(cudaMemcpy(sys->d_T.p, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
     // candidates: neighbour-load variant x threads per CTA x resident CTAs per
     // SM (the structured kernels run at most 256 threads per CTA)
-    const int cand_threads[3] = {128, 256, 512};
-    const int cand_ctas[6] = {2, 3, 4, 5, 6, 8};
+    // (ctas 0: one CTA per tile, the hardware balancing the waves)
+    const int cand_threads[4] = {64, 128, 256, 512};
+    const int cand_ctas[11] = {0, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16};
     int best_t = sys->threads, best_c = sys->ctas_per_sm, best_v = sys->load_variant;
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;
@@ -1676,8 +1703,8 @@ int pc_autotune(pc_system* sys) {
     sys->timing = false;
     const int n_var = sys->structured ? 3 : 1;
     for (int vi = 0; vi < n_var; ++vi)
-        for (int ti = 0; ti < 3; ++ti)
-            for (int ci = 0; ci < 6; ++ci) {
+        for (int ti = 0; ti < 4; ++ti)
+            for (int ci = 0; ci < 11; ++ci) {
                 if (sys->structured && cand_threads[ti] > 256) continue;
                 sys->load_variant = vi;
                 sys->threads = cand_threads[ti];

@@ -163,6 +163,10 @@ class System:
         colour pass, sharing the local field)."""
         call("pc_set_sweep_schedule", self._h, int(schedule))
 
+    def set_launch_overlap(self, on: bool):
+        """Programmatic dependent launch between colour passes (default on)."""
+        call("pc_set_launch_overlap", self._h, int(bool(on)))
+
     def set_kernel_path(self, force_generic: bool):
         """Force the generic bond-table kernels (True) or allow the structured
         pyrochlore kernels (False, default)."""

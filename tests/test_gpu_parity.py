@@ -184,6 +184,30 @@ def test_sweep_reflection_mode_follows_oracle(schedule):
     assert np.mean(d <= 1e-4) >= 0.95 and d.max() <= 1e-3
 
 
+def _sweep_state(L, n, setup, c=COUPLINGS[1], schedule=1):
+    g = pc.pyrochlore_system(L, seed=4, schedule=schedule, **c)
+    g.random_spins(9)
+    setup(g)
+    acc = g.sweep(0.7, n, 1)
+    return g.spins_f4(), acc
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_launch_modes_give_identical_sweeps(schedule):
+    """Graphs of up to 16 sweeps (37 = 16 + 16 + 5), plain launches with
+    per-kernel events, launch overlap on and off, a strided grid and one CTA
+    per tile: the same moves, bit for bit."""
+    L, n = 6, 37
+    ref, acc_ref = _sweep_state(L, n, lambda g: g.set_kernel_timing(True), schedule=schedule)
+    for setup in (lambda g: None,
+                  lambda g: g.set_launch_overlap(False),
+                  lambda g: g.set_tile(64, 0),
+                  lambda g: g.set_tile(128, 3)):
+        S, acc = _sweep_state(L, n, setup, schedule=schedule)
+        assert np.array_equal(S, ref)
+        assert np.array_equal(acc, acc_ref)
+
+
 def test_batched_replicas_are_independent_streams():
     c = COUPLINGS[1]
     g = pc.pyrochlore_system(2, seed=5, n_replicas=3, **c)
@@ -236,6 +260,31 @@ def test_ssf_matches_oracle(L):
         # S(q) = 0 on the whole grid, where only an absolute bound means anything
         scale = max(np.abs(ref).max(), o.N)
         assert np.abs(got - ref).max() <= REL * scale, (name, np.abs(got - ref).max() / scale)
+
+
+@pytest.mark.parametrize("L", [11, 16, 32, 64])
+def test_ssf_large_L_matches_fft_restatement(L):
+    """S(q) of random spins at sizes beyond the direct-sum oracle: L = 11
+    (a prime line length, the runtime-radix path), 16 / 32 / 64 (the swizzled
+    shared-memory layout; 64 is the field-cool size), against the numpy-FFT
+    restatement of ssf_manager::sample."""
+    from oracle import ssf_fft
+    g = pc.pyrochlore_system(L, **COUPLINGS[0])
+    g.ssf_configure(CORR9, 1)
+    g.random_spins(L)
+    got = g.ssf_current()
+    ref = ssf_fft.ssf(g.spins(), L, CORR9)
+    scale = max(np.abs(ref).max(), g.N())
+    assert np.abs(got - ref).max() <= REL * scale, np.abs(got - ref).max() / scale
+    # structured state: a spiral along z concentrates S^yy + S^zz at one K
+    pos, _ = g.positions()
+    q = 2 * np.pi * 3 / (8 * L)
+    spiral = np.stack([np.zeros(len(pos)), np.cos(q * pos[:, 2]), np.sin(q * pos[:, 2])], axis=1)
+    g.set_spins(spiral)
+    got = g.ssf_current()
+    ref = ssf_fft.ssf(g.spins(), L, CORR9)
+    scale = max(np.abs(ref).max(), g.N())
+    assert np.abs(got - ref).max() <= REL * scale, np.abs(got - ref).max() / scale
 
 
 def test_ssf_accumulates_like_ssf_manager():

@@ -193,6 +193,19 @@ def test_ssf_direct_equals_reference_sublattice_contraction(L):
     np.testing.assert_allclose(a, b, atol=1e-10 * np.abs(a).max())
 
 
+@pytest.mark.parametrize("L", [1, 2, 3, 4])
+def test_ssf_fft_restatement_equals_direct_sum(L):
+    """The numpy-FFT S(q) used as the checker at large L against the oracle's
+    direct sum (9 correlators, random spins)."""
+    from oracle import ssf_fft
+    s = oracle.System(L, seed=5)
+    s.random_spins(L)
+    corr = ["xx", "yy", "zz", "xy", "xz", "yz", "zx", "yx", "zy"]
+    a = s.ssf(corr, mode=0)
+    b = ssf_fft.ssf(s.spins(), L, corr)
+    np.testing.assert_allclose(b, a, atol=1e-9 * max(np.abs(a).max(), 1.0))
+
+
 def test_ssf_ferromagnet_k0():
     s = oracle.System(2)
     n = np.array([0.0, 0.6, 0.8])
