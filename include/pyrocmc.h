@@ -105,6 +105,17 @@ int pc_set_colouring(pc_system* sys, int mode);
  * ensemble with one local-field evaluation per site instead of two. The
  * Philox draws per site are those of schedule 0. */
 int pc_set_sweep_schedule(pc_system* sys, int schedule);
+/* The single-site move of a sweep. 0 (default): local_Metropolis
+ * (src/MC.cpp:111-130), sweep_local_Metropolis. 1: lifted Metropolis, u-form
+ * (local_lifted_Metropolis, src/MC.cpp:249-281; sweep_lifted_Metropolis
+ * :284-291, the move of `anneal --lifted`). 2: lifted Metropolis, rotation
+ * form (local_lifted_Metropolis_rot, src/MC.cpp:194-244;
+ * sweep_lifted_Metropolis_rot :293-302). The per-spin lifting direction
+ * (include/MC.hpp:57) is the sign of the spin's fourth float4 component
+ * (>= 0: +1); pc_set_spins resets it to +1. Lifted sweeps visit the classes in
+ * the reference's order (a lifted pass, then the overrelaxation passes), for
+ * either sweep schedule. */
+int pc_set_update(pc_system* sys, int mode);
 /* Kernel path: 0 (default) uses the structured pyrochlore kernels whenever the
  * couplings fit the fixed J1/J2/J3a/J3b neighbour structure, 1 forces the
  * generic bond-table kernels. Reports the path in use via pc_kernel_path. */
@@ -271,7 +282,9 @@ int pc_energy_noalloc(const void* spins_dev, int L, const double* params, void* 
  * state and sweep counter are saved and restored). */
 int pc_autotune(pc_system* sys);
 /* How the structured kernels issue the 30 neighbour loads of a site:
- * 0 group by group (fewest registers), 1 all at once, 2 in two batches. */
+ * 0 group by group (fewest registers), 1 all at once, 2 in two batches, 3 staged:
+ * a CTA copies the 24 neighbour-row blocks of its tile of x-rows into shared
+ * memory with bulk asynchronous copies (L <= threads <= 256; else variant 0). */
 int pc_set_load_variant(pc_system* sys, int variant);
 int pc_get_load_variant(pc_system* sys, int* variant);
 /* Current tile shape (threads per CTA, CTAs per SM). CTAs per SM = 0 launches

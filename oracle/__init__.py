@@ -71,7 +71,13 @@ def lib():
         l.orc_sweep.restype = _U64
         l.orc_sweep.argtypes = [_P, _D, _I, _I]
         l.orc_sweep_philox.restype = _U64
-        l.orc_sweep_philox.argtypes = [_P, _D, _U64, _U32, _U64, _I, _I32P, _I, _I]
+        l.orc_sweep_philox.argtypes = [_P, _D, _U64, _U32, _U64, _I, _I32P, _I, _I, _I]
+        l.orc_sweep_lifted.restype = _U64
+        l.orc_sweep_lifted.argtypes = [_P, _D, _I, _I, _I]
+        l.orc_get_lifted.restype = None
+        l.orc_get_lifted.argtypes = [_P, C.POINTER(C.c_int8)]
+        l.orc_set_lifted.restype = None
+        l.orc_set_lifted.argtypes = [_P, C.POINTER(C.c_int8)]
         l.orc_overrelax.argtypes = [_P, _DP, _I32P]
         l.orc_ssf.argtypes = [_P, _I32P, _I, _I, _DP, _DP]
         l.orc_T_profile.argtypes = [_D, _D, _DP, _I, _I, _DP, _I32P, _I]
@@ -189,10 +195,26 @@ class System:
     def sweep(self, T, n_sweeps=1, n_overrelax=1):
         return lib().orc_sweep(self._h, T, n_sweeps, n_overrelax)
 
-    def sweep_philox(self, T, seed, replica, sweep, colour_of_sl, n_overrelax=1, or_mode=0, fused=False):
+    def sweep_philox(self, T, seed, replica, sweep, colour_of_sl, n_overrelax=1, or_mode=0, fused=False, update=0):
+        """One sweep in the GPU's schedule with its Philox draws; update 0
+        Metropolis, 1 lifted (u-form), 2 lifted (rotation form)."""
         col = _arr(colour_of_sl, np.int32)
         return lib().orc_sweep_philox(self._h, T, seed, replica, sweep, n_overrelax,
-                                      col.ctypes.data_as(_I32P), or_mode, int(bool(fused)))
+                                      col.ctypes.data_as(_I32P), or_mode, int(bool(fused)), int(update))
+
+    def sweep_lifted(self, T, n_sweeps=1, n_overrelax=1, rot=False):
+        """sweep_lifted_Metropolis(_rot) (src/MC.cpp:284-302) with the
+        reference's Xoroshiro draws."""
+        return lib().orc_sweep_lifted(self._h, T, n_sweeps, n_overrelax, int(bool(rot)))
+
+    def lifted_dirs(self):
+        d = np.empty(self.N, dtype=np.int8)
+        lib().orc_get_lifted(self._h, d.ctypes.data_as(C.POINTER(C.c_int8)))
+        return d
+
+    def set_lifted_dirs(self, d):
+        d = np.ascontiguousarray(np.asarray(d), dtype=np.int8)
+        lib().orc_set_lifted(self._h, d.ctypes.data_as(C.POINTER(C.c_int8)))
 
     def overrelax(self, theta=None, colour_of_sl=None):
         col = None if colour_of_sl is None else _arr(colour_of_sl, np.int32)

@@ -288,6 +288,7 @@ struct Runner {
     Xoroshiro128pp rng;
     std::normal_distribution<double> normal_dist;
     std::uniform_real_distribution<double> rand01{0.0, 1.0};
+    std::exponential_distribution<double> exp_dist;  // rate 1 (include/MC.hpp:97)
 
     Runner(Lattice& l, uint64_t seed) : lat(&l), rng(seed) {}
 
@@ -382,6 +383,97 @@ struct Runner {
         return acc;
     }
 
+    // --- lifted moves (the move formulas; the draws are passed in) -----
+    // src/MC.cpp:249-281, u-form: slide u = S.h_hat by du = dir*sqrt(T/T_ref)*E,
+    // E ~ Exp(1), keep the azimuth; out of [-1, 1] or at a pole: flip dir.
+    bool lifted_u_move(double T, Spin* spin, const vec3& h, double e1, double u01) const {
+        const double curr_E = dot(spin->S, h);
+        const vec3 hh = scale(1.0 / std::sqrt(dot(h, h)), h);
+        const double u = dot(hh, spin->S);
+        const double du = spin->lifted_dir * std::sqrt(T / T_ref) * e1;
+        const double nu = u + du;
+        if (nu > 1 || nu < -1 || std::abs(1 - u * u) < 1e-16) {
+            spin->lifted_dir = int8_t(-spin->lifted_dir);
+            return false;
+        }
+        vec3 nS = add(scale(nu, hh), scale(std::sqrt((1 - nu * nu) / (1 - u * u)), sub(spin->S, scale(u, hh))));
+        nS = scale(1.0 / std::sqrt(dot(nS, nS)), nS);
+        const double dE = dot(nS, h) - curr_E;
+        if (u01 < std::exp(-dE / T)) {
+            spin->S = nS;
+            return true;
+        }
+        spin->lifted_dir = int8_t(-spin->lifted_dir);
+        return false;
+    }
+    // src/MC.cpp:194-244, rotation form: rotate by dir*sqrt(T/T_ref) about
+    // S x h; poles and pole crossings bounce; acceptance carries the Jacobian
+    // |S' x h| / |S x h|.
+    bool lifted_rot_move(double T, Spin* spin, const vec3& h, double u01) const {
+        const double curr_E = dot(spin->S, h);
+        const double delta = std::sqrt(T / T_ref);
+        const vec3 axis = cross(spin->S, h);
+        const double n2_old = dot(axis, axis);
+        if (n2_old <= 1e-20) {
+            spin->lifted_dir = int8_t(-spin->lifted_dir);
+            return false;
+        }
+        vec3 nS = spin->S;
+        rotate_about_vector(nS, axis, spin->lifted_dir * delta);
+        nS = scale(1.0 / std::sqrt(dot(nS, nS)), nS);
+        const vec3 axis_new = cross(nS, h);
+        const double n2_new = dot(axis_new, axis_new);
+        if (dot(axis, axis_new) < 0) {
+            spin->lifted_dir = int8_t(-spin->lifted_dir);
+            return false;
+        }
+        const double dE = dot(nS, h) - curr_E;
+        if (u01 < std::sqrt(n2_new / n2_old) * std::exp(-dE / T)) {
+            spin->S = nS;
+            return true;
+        }
+        spin->lifted_dir = int8_t(-spin->lifted_dir);
+        return false;
+    }
+    // src/MC.cpp:249-281 with the reference's draws (exp_dist, then rand01
+    // only when the proposal stays on the sphere)
+    size_t local_lifted_Metropolis(double T, Spin* spin) {
+        const vec3 h = sub(local_field(spin), B);
+        const double e1 = exp_dist(rng);
+        const vec3 hh = scale(1.0 / std::sqrt(dot(h, h)), h);
+        const double u = dot(hh, spin->S);
+        const double nu = u + spin->lifted_dir * std::sqrt(T / T_ref) * e1;
+        if (nu > 1 || nu < -1 || std::abs(1 - u * u) < 1e-16) {
+            spin->lifted_dir = int8_t(-spin->lifted_dir);
+            return 0;
+        }
+        return lifted_u_move(T, spin, h, e1, rand01(rng)) ? 1 : 0;
+    }
+    // src/MC.cpp:194-244 (rand01 drawn only when the move reaches the test)
+    size_t local_lifted_Metropolis_rot(double T, Spin* spin) {
+        const vec3 h = sub(local_field(spin), B);
+        const vec3 axis = cross(spin->S, h);
+        if (dot(axis, axis) <= 1e-20) {
+            spin->lifted_dir = int8_t(-spin->lifted_dir);
+            return 0;
+        }
+        vec3 nS = spin->S;
+        rotate_about_vector(nS, axis, spin->lifted_dir * std::sqrt(T / T_ref));
+        nS = scale(1.0 / std::sqrt(dot(nS, nS)), nS);
+        if (dot(axis, cross(nS, h)) < 0) {
+            spin->lifted_dir = int8_t(-spin->lifted_dir);
+            return 0;
+        }
+        return lifted_rot_move(T, spin, h, rand01(rng)) ? 1 : 0;
+    }
+    // src/MC.cpp:284-302
+    size_t sweep_lifted_Metropolis(double T, size_t n_overrelax, bool rot) {
+        size_t acc = 0;
+        for (auto& s : lat->spins) acc += rot ? local_lifted_Metropolis_rot(T, &s) : local_lifted_Metropolis(T, &s);
+        for (size_t i = 0; i < n_overrelax; ++i) overrelax_all();
+        return acc;
+    }
+
     // src/MC.cpp:305-312
     double total_energy_per_unit_cell() const {
         double E = 0;
@@ -400,16 +492,30 @@ struct Runner {
     // formulas are those of local_Metropolis / overrelax_all above.
     // fused: the first overrelaxation move of each site follows its Metropolis
     // move inside the same colour class, with the same local field.
+    // update 1 / 2: the lifted move (u-form / rotation form) in place of the
+    // Metropolis move, draws from Philox draw 1 (Exp(1) = -ln of the open
+    // 24-bit uniform of word 0, the acceptance uniform from word 1); lifted
+    // sweeps are never fused.
     size_t sweep_philox(double T, uint64_t seed, uint32_t replica, uint64_t sweep, int n_or,
-                        const std::vector<std::vector<int>>& colour_sls, int or_mode, bool fused = false) {
+                        const std::vector<std::vector<int>>& colour_sls, int or_mode, bool fused = false,
+                        int update = 0) {
         size_t acc = 0;
         const double sigma = std::sqrt(T / T_ref);
-        const bool fuse = fused && n_or >= 1;
+        const bool fuse = fused && n_or >= 1 && update == 0;
         for (const auto& cls : colour_sls)
             for (int sl : cls)
                 for (int cell = 0; cell < lat->Nc; ++cell) {
                     const uint32_t site = uint32_t(sl * lat->Nc + cell);
                     Spin* spin = &lat->spins[site];
+                    if (update != 0) {
+                        uint32_t wl[4];
+                        philox_site(seed, replica, sweep, 1, site, wl);
+                        const vec3 h = sub(local_field(spin), B);
+                        const bool a = update == 1 ? lifted_u_move(T, spin, h, -std::log(u24_open0(wl[0])), u24(wl[1]))
+                                                   : lifted_rot_move(T, spin, h, u24(wl[1]));
+                        acc += a ? 1 : 0;
+                        continue;
+                    }
                     uint32_t w[4];
                     philox_site(seed, replica, sweep, 0, site, w);
                     const double r0 = std::sqrt(-2.0 * std::log(u24_open0(w[0])));
@@ -761,14 +867,31 @@ uint64_t orc_sweep(void* h, double T, int n_sweeps, int n_overrelax) {
 
 // colour_of_sl[16]: colour index per sublattice; colours visited 0..n_colours-1,
 // sublattices inside a colour in increasing order.
+uint64_t orc_sweep_lifted(void* h, double T, int n_sweeps, int n_overrelax, int rot) {
+    auto* s = static_cast<System*>(h);
+    uint64_t acc = 0;
+    for (int i = 0; i < n_sweeps; ++i) acc += s->mc.sweep_lifted_Metropolis(T, size_t(n_overrelax), rot != 0);
+    return acc;
+}
+
+// lifting directions (+1 / -1) per site in storage order
+void orc_get_lifted(void* h, int8_t* out) {
+    auto* s = static_cast<System*>(h);
+    for (size_t i = 0; i < s->lat.spins.size(); ++i) out[i] = s->lat.spins[i].lifted_dir;
+}
+void orc_set_lifted(void* h, const int8_t* in) {
+    auto* s = static_cast<System*>(h);
+    for (size_t i = 0; i < s->lat.spins.size(); ++i) s->lat.spins[i].lifted_dir = in[i] < 0 ? int8_t(-1) : int8_t(1);
+}
+
 uint64_t orc_sweep_philox(void* h, double T, uint64_t seed, uint32_t replica, uint64_t sweep, int n_overrelax,
-                          const int32_t* colour_of_sl, int or_mode, int fused) {
+                          const int32_t* colour_of_sl, int or_mode, int fused, int update) {
     auto* s = static_cast<System*>(h);
     int nc = 0;
     for (int i = 0; i < 16; ++i) nc = std::max(nc, colour_of_sl[i] + 1);
     std::vector<std::vector<int>> cls(static_cast<size_t>(nc));
     for (int i = 0; i < 16; ++i) cls[size_t(colour_of_sl[i])].push_back(i);
-    return s->mc.sweep_philox(T, seed, replica, sweep, n_overrelax, cls, or_mode, fused != 0);
+    return s->mc.sweep_philox(T, seed, replica, sweep, n_overrelax, cls, or_mode, fused != 0, update);
 }
 
 // One overrelaxation pass with caller-supplied angles (theta[i] per site) or

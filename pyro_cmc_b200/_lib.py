@@ -43,6 +43,7 @@ _SIGNATURES = {
     "pc_set_colouring": (_I, [_P, _I]),
     "pc_set_kernel_path": (_I, [_P, _I]),
     "pc_set_sweep_schedule": (_I, [_P, _I]),
+    "pc_set_update": (_I, [_P, _I]),
     "pc_kernel_path": (_I, [_P, _IP]),
     "pc_setup_lattice": (_I, [_P]),
     "pc_num_replicas": (_I, [_P, _IP]),

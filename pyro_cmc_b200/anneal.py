@@ -45,18 +45,19 @@ def anneal_batch(K: int, L: int, J1: float, J2: float = 0.0, J3: float = 0.0, B=
                  Delta: float = 1.0, T_hot: float = 10.0, T_cold: float | None = None, T_sample=(0.1,),
                  n_steps: int = 100, n_sweep: int = 16, n_burn_in: int = 16, n_sample: int = 64,
                  corr=("xx", "yy", "zz", "xy", "xz", "yz"), T_ref: float = 1.0, seed: int = 0,
-                 init_seed: int | None = None, schedule: int = 0):
+                 init_seed: int | None = None, schedule: int = 0, update: int = 0):
     """The anneal protocol for K seeds at once: burn-in at T_hot, then for each
     T of the profile n_sweep sweeps and one energy sample; at the sample
     temperatures, n_sample x (n_sweep sweeps + one S(q) sample).
     Returns dict(T, sample_idx, e[K, n_T], ssf_sum/ssf_sq[K, n_Ts, n_corr, n_k, 2],
-    n_ssf[n_Ts], accepted[K, n_T]); S(q) slots in visit (descending T) order."""
+    n_ssf[n_Ts], accepted[K, n_T]); S(q) slots in visit (descending T) order.
+    update 1: lifted Metropolis (src/anneal.cpp:184-188, --lifted)."""
     T_sample = list(T_sample)
     if T_cold is None:
         T_cold = min(T_sample)
     T_grid, S_idx = generate_T_profile(T_hot, T_cold, T_sample, n_steps)
     s = pyrochlore_system(L, J1=J1, J2=J2, J3=J3, Delta=Delta, B=B, T_ref=T_ref, seed=seed, n_replicas=K,
-                          schedule=schedule)
+                          schedule=schedule, update=update)
     s.random_spins(seed if init_seed is None else init_seed)
     nTs = len(S_idx)
     s.ssf_configure(list(corr), max(1, K * nTs), [L] * max(1, K * nTs))

@@ -75,6 +75,7 @@ __device__ __forceinline__ float u24_lowbytes(uint4 w) {
 }
 
 constexpr uint32_t kDrawMetropolis = 0;
+constexpr uint32_t kDrawLifted = 1;  // lifted Metropolis: Exp(1) from word 0, acceptance uniform from word 1
 constexpr uint32_t kDrawOverrelax0 = 2;
 constexpr uint32_t kDrawInit = 250;
 constexpr uint32_t kDrawExchange = 251;

@@ -19,7 +19,9 @@ enum PassMode {
     kOverrelaxReflect = 2,
     kOverrelaxTheta = 3,
     kFusedRotate = 4,
-    kFusedReflect = 5
+    kFusedReflect = 5,
+    kLifted = 6,     // lifted Metropolis, u-form (src/MC.cpp:249-281)
+    kLiftedRot = 7   // lifted Metropolis, rotation form (src/MC.cpp:194-244)
 };
 
 struct PassArgs {
@@ -41,13 +43,17 @@ struct PassArgs {
     const double* theta;      // kOverrelaxTheta: per-site angle of replica theta_replica (device)
     int theta_replica;
     int structured;    // 1: couplings fit the pyrochlore structure, use `mats`
-    int load_variant;  // structured path: how neighbour loads are batched (0, 1, 2)
+    int load_variant;  // structured path: how neighbour loads are batched (0, 1, 2), 3 = staged rows
     PyroMats mats;
+    int staged_rl;  // load variant 3: largest tile (rows x L sites); sizes the shared row blocks
+    int* err;       // device error flag (set by a kernel whose bounded wait ran out)
 };
 
 // pdl: launch with programmatic dependent launch (the kernel waits for the
 // previous kernel on the stream with griddepcontrol.wait before touching spins)
 void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl = false);
+// Load variant 3 (row tiles staged by bulk copies): sets the kernels' shared-memory limit.
+void staged_prepare();
 
 struct EnergyArgs {
     const float4* spins;

@@ -148,6 +148,55 @@ __host__ __device__ constexpr int group_of(int sl, int e) {
 }
 __host__ __device__ constexpr int grp_size(int sl, int g) { return kStruct.t[sl].gbegin[g + 1] - kStruct.t[sl].gbegin[g]; }
 
+// Neighbour rows: the distinct (sublattice, dy, dz) of the 30 neighbours of a
+// sublattice, in first-use order. A row of cells (fixed cy, cz) of sublattice
+// sl finds all its neighbours in these rows of the other sublattices, shifted
+// by dx in {-1, 0, +1} along x. 24 rows for every sublattice of the pyrochlore
+// structure; kMaxRows bounds the table.
+constexpr int kMaxRows = 32;
+struct SRows {
+    int n;
+    int s2[kMaxRows], dy[kMaxRows], dz[kMaxRows];
+    int row_of[kStructNb];
+};
+__host__ __device__ constexpr SRows make_rows(int sl) {
+    SRows r{};
+    r.n = 0;
+    for (int e = 0; e < kStructNb; ++e) {
+        const SNb& b = kStruct.t[sl].nb[e];
+        int u = 0;
+        while (u < r.n && !(r.s2[u] == b.sl && r.dy[u] == b.dy && r.dz[u] == b.dz)) ++u;
+        if (u == r.n) {
+            r.s2[u] = b.sl;
+            r.dy[u] = b.dy;
+            r.dz[u] = b.dz;
+            ++r.n;
+        }
+        r.row_of[e] = u;
+    }
+    return r;
+}
+struct SRowsAll {
+    SRows t[16];
+};
+__host__ __device__ constexpr SRowsAll make_all_rows() {
+    SRowsAll a{};
+    for (int sl = 0; sl < 16; ++sl) a.t[sl] = make_rows(sl);
+    return a;
+}
+constexpr SRowsAll kRows = make_all_rows();
+__host__ __device__ constexpr int rows_n(int sl) { return kRows.t[sl].n; }
+__host__ __device__ constexpr int row_s2(int sl, int u) { return kRows.t[sl].s2[u]; }
+__host__ __device__ constexpr int row_dy(int sl, int u) { return kRows.t[sl].dy[u]; }
+__host__ __device__ constexpr int row_dz(int sl, int u) { return kRows.t[sl].dz[u]; }
+__host__ __device__ constexpr int row_of(int sl, int e) { return kRows.t[sl].row_of[e]; }
+__host__ __device__ constexpr int max_rows() {
+    int m = 0;
+    for (int sl = 0; sl < 16; ++sl) m = kRows.t[sl].n > m ? kRows.t[sl].n : m;
+    return m;
+}
+static_assert(max_rows() <= kMaxRows, "neighbour row table too small");
+
 // Group matrices per sublattice (row-major 3x3) and the groups with a nonzero
 // matrix; passed to the kernels by value (constant bank).
 struct PyroMats {

@@ -152,11 +152,28 @@ __device__ __forceinline__ int plane_pos(int x, int y, int L) {
 
 __host__ __device__ __forceinline__ bool ssf_fast_path(int P, int Q) { return P <= kMaxRadix && Q <= kMaxRadix; }
 
-template <bool SWZ>
+// The split L = P*Q of the host's split_PQ (largest divisor P <= sqrt L), at
+// compile time for the instantiated sizes. LT = 0: sizes from the geometry at
+// run time.
+__host__ __device__ constexpr int ct_split_P(int L) {
+    int best = 1;
+    for (int p = 1; p * p <= L; ++p)
+        if (L % p == 0) best = p;
+    return best;
+}
+template <int LT>
+struct SsfDims {
+    int L, P, Q;
+    __device__ __forceinline__ explicit SsfDims(const SsfGeom& g)
+        : L(LT ? LT : g.L), P(LT ? ct_split_P(LT) : g.P), Q(LT ? LT / ct_split_P(LT) : g.Q) {}
+};
+
+template <int LT, bool SWZ>
 __global__ void __launch_bounds__(512) ssf_plane_kernel(const SsfGeom g, const float4* __restrict__ spins,
                                                         const ReplicaDev* __restrict__ reps, float2* __restrict__ G) {
     extern __shared__ float2 sm[];
-    const int L = g.L, LL = L * L, P = g.P, Q = g.Q;
+    const SsfDims<LT> dm(g);
+    const int L = dm.L, LL = L * L, P = dm.P, Q = dm.Q;
     float2* tw = sm;
     float2* ph = tw + L;
     float2* buf = ph + 8 * L;  // planes A0, A1, Az
@@ -225,9 +242,11 @@ __host__ __device__ __forceinline__ int ssf_chunk(int L) { return L < 16 ? L : 1
 // groups -> B^a(K), then the correlators and the FP64 accumulators. Shared
 // layout T[(a*4 + gz)][z][CP], CP = C + 1 (odd row stride: the per-K reads
 // with consecutive Kz hit distinct banks).
+template <int LT>
 __global__ void __launch_bounds__(512) ssf_line_kernel(const SsfGeom g, const float2* __restrict__ G, const SsfOut o) {
     extern __shared__ float2 sm[];
-    const int L = g.L, LL = L * L, P = g.P, Q = g.Q;
+    const SsfDims<LT> dm(g);
+    const int L = dm.L, LL = L * L, P = dm.P, Q = dm.Q;
     const int C = ssf_chunk(L), CP = C + 1;
     const int n_chunk = (L + C - 1) / C;
     float2* tw = sm;
@@ -279,34 +298,48 @@ __global__ void __launch_bounds__(512) ssf_line_kernel(const SsfGeom g, const fl
         const size_t k = (size_t(Kx0 + c) * L + Ky) * L + Kz;
         if (o.amp)
             for (int a = 0; a < 3; ++a) o.amp[(size_t(rp) * 3 + a) * n_k + k] = B[a];
-        if (o.val || slot >= 0)
+        if (o.val || slot >= 0) {
+            double* __restrict__ acc_s = slot >= 0 ? o.acc_sum + size_t(slot) * o.slot_stride : nullptr;
+            double* __restrict__ acc_q = slot >= 0 ? o.acc_sq + size_t(slot) * o.slot_stride : nullptr;
+            // correlators in groups of three: the group's accumulator loads are
+            // issued together, then the updates, then the stores
 #pragma unroll
-            for (int cc = 0; cc < 9; ++cc) {  // unrolled: constant indices into the parameter arrays
-                if (cc >= o.n_corr) break;
-                const int ca = o.corr_a[cc], cb = o.corr_b[cc];  // selects keep B[] in registers
-                const float2 ba = ca == 0 ? B[0] : (ca == 1 ? B[1] : B[2]);
-                const float2 bb = cb == 0 ? B[0] : (cb == 1 ? B[1] : B[2]);
-                // conj(B^a) B^b
-                const double re = double(ba.x) * bb.x + double(ba.y) * bb.y;
-                const double im = double(ba.x) * bb.y - double(ba.y) * bb.x;
-                if (o.val) {
-                    double2* v = reinterpret_cast<double2*>(o.val + ((size_t(rp) * o.n_corr + cc) * n_k + k) * 2);
-                    *v = make_double2(re, im);
+            for (int c0 = 0; c0 < 9; c0 += 3) {
+                double re[3], im[3];
+                double2 sv[3], qv[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const int cc = c0 + j;
+                    if (cc < o.n_corr) {
+                        const int ca = o.corr_a[cc], cb = o.corr_b[cc];
+                        const float2 ba = ca == 0 ? B[0] : (ca == 1 ? B[1] : B[2]);
+                        const float2 bb = cb == 0 ? B[0] : (cb == 1 ? B[1] : B[2]);
+                        // conj(B^a) B^b
+                        re[j] = double(ba.x) * bb.x + double(ba.y) * bb.y;
+                        im[j] = double(ba.x) * bb.y - double(ba.y) * bb.x;
+                        if (acc_s) {
+                            sv[j] = *reinterpret_cast<const double2*>(acc_s + (size_t(cc) * n_k + k) * 2);
+                            qv[j] = *reinterpret_cast<const double2*>(acc_q + (size_t(cc) * n_k + k) * 2);
+                        }
+                    }
                 }
-                if (slot >= 0) {
-                    double2* s = reinterpret_cast<double2*>(o.acc_sum + size_t(slot) * o.slot_stride +
-                                                            (size_t(cc) * n_k + k) * 2);
-                    double2* q = reinterpret_cast<double2*>(o.acc_sq + size_t(slot) * o.slot_stride +
-                                                            (size_t(cc) * n_k + k) * 2);
-                    double2 sv = *s, qv = *q;
-                    sv.x += re;
-                    sv.y += im;
-                    qv.x += re * re;
-                    qv.y += im * im;
-                    *s = sv;
-                    *q = qv;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const int cc = c0 + j;
+                    if (cc < o.n_corr) {
+                        if (o.val)
+                            *reinterpret_cast<double2*>(o.val + ((size_t(rp) * o.n_corr + cc) * n_k + k) * 2) =
+                                make_double2(re[j], im[j]);
+                        if (acc_s) {
+                            *reinterpret_cast<double2*>(acc_s + (size_t(cc) * n_k + k) * 2) =
+                                make_double2(sv[j].x + re[j], sv[j].y + im[j]);
+                            *reinterpret_cast<double2*>(acc_q + (size_t(cc) * n_k + k) * 2) =
+                                make_double2(qv[j].x + re[j] * re[j], qv[j].y + im[j] * im[j]);
+                        }
+                    }
                 }
             }
+        }
     }
 }
 
@@ -367,10 +400,18 @@ void launch_ssf_xy(const SsfGeom& g, const float4* spins, const ReplicaDev* reps
     const size_t smem = sizeof(float2) * (size_t(9) * L + 3 * size_t(L) * L);
     if (ssf_fast_path(g.P, g.Q)) {
         const int threads = ssf_plane_threads(L);
-        if (L % 16 == 0)
-            ssf_plane_kernel<true><<<g.n_rep * L * 8, threads, smem, st>>>(g, spins, reps, G);
-        else
-            ssf_plane_kernel<false><<<g.n_rep * L * 8, threads, smem, st>>>(g, spins, reps, G);
+        const int grid = g.n_rep * L * 8;
+        switch (L) {
+            case 64: ssf_plane_kernel<64, true><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+            case 32: ssf_plane_kernel<32, true><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+            case 16: ssf_plane_kernel<16, true><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+            case 8: ssf_plane_kernel<8, false><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+            default:
+                if (L % 16 == 0)
+                    ssf_plane_kernel<0, true><<<grid, threads, smem, st>>>(g, spins, reps, G);
+                else
+                    ssf_plane_kernel<0, false><<<grid, threads, smem, st>>>(g, spins, reps, G);
+        }
         return;
     }
     ssf_xy_kernel<<<g.n_rep * L * 4, 256, smem, st>>>(g, spins, reps, G);
@@ -460,7 +501,14 @@ void launch_ssf_z(const SsfGeom& g, const float2* G, const SsfOut& o, cudaStream
     const int n_chunk = (L + C - 1) / C;
     if (ssf_fast_path(g.P, g.Q)) {
         const size_t smem = sizeof(float2) * (size_t(9) * L + 12 * size_t(L) * (C + 1));
-        ssf_line_kernel<<<g.n_rep * L * n_chunk, ssf_line_threads(L, g.P, g.Q), smem, st>>>(g, G, o);
+        const int grid = g.n_rep * L * n_chunk, threads = ssf_line_threads(L, g.P, g.Q);
+        switch (L) {
+            case 64: ssf_line_kernel<64><<<grid, threads, smem, st>>>(g, G, o); break;
+            case 32: ssf_line_kernel<32><<<grid, threads, smem, st>>>(g, G, o); break;
+            case 16: ssf_line_kernel<16><<<grid, threads, smem, st>>>(g, G, o); break;
+            case 8: ssf_line_kernel<8><<<grid, threads, smem, st>>>(g, G, o); break;
+            default: ssf_line_kernel<0><<<grid, threads, smem, st>>>(g, G, o);
+        }
         return;
     }
     const size_t smem = sizeof(float2) * (size_t(9) * L + 5 * size_t(L) * C);
@@ -569,9 +617,18 @@ __global__ void __launch_bounds__(256) ssf_adj_xy_kernel(const SsfGeom g, const 
 }
 
 void ssf_prepare() {
-    cudaFuncSetAttribute(ssf_plane_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(ssf_plane_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(ssf_line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    const int smem_max = 200 * 1024;
+    cudaFuncSetAttribute(ssf_plane_kernel<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_xy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(ssf_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(ssf_adj_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -156,6 +156,8 @@ struct pc_system {
     DevBuf<double> d_T;
     DevBuf<uint64_t> d_sweep;
     DevBuf<unsigned long long> d_acc;
+    DevBuf<int> d_err;  // set by a kernel whose bounded wait ran out
+    int staged_rl = 0;  // load variant 3: largest row tile (R*L sites)
     DevBuf<SlTable> d_tab_active, d_tab_full;
     std::vector<DevBuf<Tile>> d_colour_tiles;
     std::vector<int> n_colour_tiles;
@@ -175,6 +177,7 @@ struct pc_system {
     // sweep graph cache, keyed by n_overrelax
     std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> sweep_graphs;  // (n_or, sweeps) -> (graph, nodes)
     bool pdl = true;  // colour passes launched with programmatic dependent launch
+    int update = 0;   // 0 Metropolis, 1 lifted (u-form), 2 lifted (rotation form)
 
     // kernel timing
     bool timing = false;
@@ -219,6 +222,7 @@ struct pc_system {
         d_T.release();
         d_sweep.release();
         d_acc.release();
+        d_err.release();
         d_tab_active.release();
         d_tab_full.release();
         for (auto& t : d_colour_tiles) t.release();
@@ -417,19 +421,44 @@ int build_colours(pc_system* s) {
     return PC_OK;
 }
 
+// Load variant 3 (row tiles staged into shared memory by bulk copies): the
+// structured kernels, a whole x-row per tile (L <= threads <= 256).
+bool use_staged(const pc_system* s) {
+    if (!s->structured || s->load_variant != 3 || s->threads > 256) return false;
+    for (int L : s->L)
+        if (L > s->threads) return false;
+    return true;
+}
+
 int build_tiles(pc_system* s) {
     const int T = s->threads;
     for (auto& t : s->d_colour_tiles) t.release();
     s->d_colour_tiles.clear();
     s->n_colour_tiles.clear();
     s->d_colour_tiles.resize(size_t(s->n_colours));
+    const bool staged = use_staged(s);
+    s->staged_rl = 0;
     for (int c = 0; c < s->n_colours; ++c) {
         std::vector<Tile> tiles;
         const auto& sls = s->colour_sls[size_t(c)];
         for (int r = 0; r < s->R; ++r)
-            for (size_t k = 0; k < sls.size(); ++k)
+            for (size_t k = 0; k < sls.size(); ++k) {
+                const int L = s->L[size_t(r)];
+                if (staged) {
+                    // row tiles (x = replica, y = class slot << 8 | sublattice,
+                    // z = first row cy0 + L cz, w = rows R): R*L <= T sites
+                    const int R = std::max(1, std::min(L, T / L));
+                    for (int cz = 0; cz < L; ++cz)
+                        for (int cy0 = 0; cy0 < L; cy0 += R) {
+                            const int n = std::min(R, L - cy0);
+                            tiles.push_back(make_int4(r, int(k << 8) | sls[k], cy0 + L * cz, n));
+                            s->staged_rl = std::max(s->staged_rl, n * L);
+                        }
+                    continue;
+                }
                 for (int64_t c0 = 0; c0 < s->Nc(r); c0 += T)
                     tiles.push_back(make_int4(r, int(k << 8) | sls[k], int(c0), int(std::min<int64_t>(T, s->Nc(r) - c0))));
+            }
         PC_CK(s->d_colour_tiles[size_t(c)].alloc(tiles.size()));
         PC_CK(cudaMemcpy(s->d_colour_tiles[size_t(c)].p, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
         s->n_colour_tiles.push_back(int(tiles.size()));
@@ -478,8 +507,10 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.acc = s->d_acc.p;
     a.or_pass = or_pass;
     a.structured = s->structured ? 1 : 0;
-    a.load_variant = s->load_variant;
+    a.load_variant = use_staged(s) ? 3 : (s->load_variant == 3 ? 0 : s->load_variant);
     a.mats = s->mats;
+    a.staged_rl = s->staged_rl;
+    a.err = s->d_err.p;
     return a;
 }
 
@@ -509,9 +540,11 @@ int enqueue_sweep(pc_system* s, uint64_t off, int n_or, bool record_events) {
         }
         return PC_OK;
     };
-    const bool fused = s->schedule == 1 && n_or >= 1;
-    const pc::PassMode mm =
-        fused ? (s->or_mode == 1 ? pc::kFusedReflect : pc::kFusedRotate) : pc::kMetropolis;
+    const bool fused = s->schedule == 1 && n_or >= 1 && s->update == 0;  // lifted sweeps: reference order
+    const pc::PassMode mm = s->update == 1   ? pc::kLifted
+                            : s->update == 2 ? pc::kLiftedRot
+                            : fused ? (s->or_mode == 1 ? pc::kFusedReflect : pc::kFusedRotate)
+                                    : pc::kMetropolis;
     for (int c = 0; c < s->n_colours; ++c) {
         const pc::PassArgs a = pass_args(s, c, off, 0);
         int rc = record(0, true);
@@ -716,6 +749,8 @@ int pc_create(int n_replicas, const int32_t* L, uint64_t seed, pc_system** out) 
     if (e == cudaSuccess) e = s->d_sweep.alloc(1);
     if (e == cudaSuccess) e = cudaMemset(s->d_sweep.p, 0, sizeof(uint64_t));
     if (e == cudaSuccess) e = s->d_acc.alloc(size_t(n_replicas));
+    if (e == cudaSuccess) e = s->d_err.alloc(1);
+    if (e == cudaSuccess) e = cudaMemset(s->d_err.p, 0, sizeof(int));
     if (e == cudaSuccess) e = s->d_e.alloc(size_t(n_replicas));
     if (e == cudaSuccess) e = s->d_mag.alloc(size_t(3 * n_replicas));
     if (e != cudaSuccess) {
@@ -839,6 +874,16 @@ int pc_set_sweep_schedule(pc_system* sys, int schedule) {
     return PC_OK;
 }
 
+int pc_set_update(pc_system* sys, int mode) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (mode < 0 || mode > 2)
+        return fail(PC_ERR_INVALID, "update must be 0 (Metropolis), 1 (lifted) or 2 (lifted, rotation form)");
+    sys->update = mode;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
 int pc_set_launch_overlap(pc_system* sys, int on) {
     int rc = check_sys(sys, false);
     if (rc) return rc;
@@ -888,6 +933,7 @@ int pc_setup_lattice(pc_system* sys) {
     PC_CK(sys->d_tab_full.alloc(16));
     PC_CK(cudaMemcpy(sys->d_tab_active.p, sys->tab_active, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
     PC_CK(cudaMemcpy(sys->d_tab_full.p, sys->tab_full, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
+    pc::staged_prepare();
     rc = build_tiles(sys);
     if (rc) return rc;
     sys->ready = true;
@@ -1094,6 +1140,18 @@ int pc_set_sweep_counter(pc_system* sys, int replica, uint64_t sweep) {
     return PC_OK;
 }
 
+// Reads (and clears) the device error flag that a kernel sets when one of its
+// bounded waits runs out. Synchronises the system's stream.
+int device_error(pc_system* s) {
+    int flag = 0;
+    PC_CK(cudaMemcpyAsync(&flag, s->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    PC_CK(cudaStreamSynchronize(s->stream));
+    if (!flag) return PC_OK;
+    PC_CK(cudaMemsetAsync(s->d_err.p, 0, sizeof(int), s->stream));
+    return fail(PC_ERR_CUDA, "a colour pass stopped waiting for its staged neighbour rows (bounded wait ran out); "
+                             "the updates of that pass were skipped");
+}
+
 int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uint64_t* accepted) {
     int rc = check_sys(sys);
     if (rc) return rc;
@@ -1108,7 +1166,7 @@ int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uin
     if (accepted) {
         PC_CK(cudaMemcpyAsync(accepted, sys->d_acc.p, sizeof(uint64_t) * size_t(sys->R), cudaMemcpyDeviceToHost,
                               sys->stream));
-        PC_CK(cudaStreamSynchronize(sys->stream));
+        return device_error(sys);
     }
     return PC_OK;
 }
@@ -1176,8 +1234,7 @@ int pc_energy(pc_system* sys, double* e_per_cell, double* mag) {
     if (mag)
         PC_CK(cudaMemcpyAsync(mag, sys->d_mag.p, sizeof(double) * 3 * size_t(sys->R), cudaMemcpyDeviceToHost,
                               sys->stream));
-    PC_CK(cudaStreamSynchronize(sys->stream));
-    return PC_OK;
+    return device_error(sys);
 }
 
 int pc_local_field(pc_system* sys, int replica, double* h) {
@@ -1665,9 +1722,10 @@ int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm) {
 int pc_set_load_variant(pc_system* sys, int variant) {
     int rc = check_sys(sys, false);
     if (rc) return rc;
-    if (variant < 0 || variant > 2) return fail(PC_ERR_INVALID, "load variant must be 0, 1 or 2");
+    if (variant < 0 || variant > 3) return fail(PC_ERR_INVALID, "load variant must be 0, 1, 2 or 3");
     sys->load_variant = variant;
     sys->drop_graphs();
+    if (sys->ready) return build_tiles(sys);  // variant 3 uses row tiles
     return PC_OK;
 }
 int pc_get_load_variant(pc_system* sys, int* variant) {
@@ -1701,7 +1759,7 @@ int pc_autotune(pc_system* sys) {
     PC_CK(cudaEventCreate(&e1));
     const bool timing = sys->timing;
     sys->timing = false;
-    const int n_var = sys->structured ? 3 : 1;
+    const int n_var = sys->structured ? 4 : 1;
     for (int vi = 0; vi < n_var; ++vi)
         for (int ti = 0; ti < 4; ++ti)
             for (int ci = 0; ci < 11; ++ci) {
@@ -1709,6 +1767,7 @@ int pc_autotune(pc_system* sys) {
                 sys->load_variant = vi;
                 sys->threads = cand_threads[ti];
                 sys->ctas_per_sm = cand_ctas[ci];
+                if (vi == 3 && (!use_staged(sys) || ci > 0)) continue;  // row tiles: one CTA per tile
                 rc = build_tiles(sys);
                 if (rc) return rc;
                 rc = run_sweeps(sys, 2, 1);  // warm-up + graph instantiation
@@ -1793,8 +1852,7 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     if (e_out) PC_CK(cudaMemcpyAsync(e_out, sys->d_e.p, sizeof(double), cudaMemcpyDeviceToHost, sys->stream));
     if (accepted)
         PC_CK(cudaMemcpyAsync(accepted, sys->d_acc.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, sys->stream));
-    PC_CK(cudaStreamSynchronize(sys->stream));
-    return PC_OK;
+    return device_error(sys);
 }
 
 int pc_set_kernel_timing(pc_system* sys, int on) {

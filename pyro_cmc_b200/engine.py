@@ -163,6 +163,13 @@ class System:
         colour pass, sharing the local field)."""
         call("pc_set_sweep_schedule", self._h, int(schedule))
 
+    def set_update(self, mode: int):
+        """0: Metropolis (sweep_local_Metropolis); 1: lifted Metropolis
+        (sweep_lifted_Metropolis); 2: lifted, rotation form
+        (sweep_lifted_Metropolis_rot). The lifting direction of each spin is
+        the sign of its float4 w component."""
+        call("pc_set_update", self._h, int(mode))
+
     def set_launch_overlap(self, on: bool):
         """Programmatic dependent launch between colour passes (default on)."""
         call("pc_set_launch_overlap", self._h, int(bool(on)))
@@ -400,12 +407,13 @@ class System:
 
 def pyrochlore_system(L, J1=1.0, J2=0.0, J3=0.0, Delta=1.0, B=(0.0, 0.0, 0.0), T_ref=1.0, seed=0,
                       n_replicas=None, split_J1=True, overrelax_mode=0, colouring=0, generic=False,
-                      schedule=0) -> System:
+                      schedule=0, update=0) -> System:
     """build_J1J2J3_h (include/cli_bits.hpp:144-207) on the GPU engine."""
     s = System(L, seed=seed, n_replicas=n_replicas)
     s.set_colouring(colouring)
     s.set_kernel_path(generic)
     s.set_sweep_schedule(schedule)
+    s.set_update(update)
     s.define_pyrochlore(J1, J2, J3, Delta, split_J1=split_J1)
     s.set_global_field(B)
     s.set_T_ref(T_ref)

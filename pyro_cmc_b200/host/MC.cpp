@@ -75,21 +75,27 @@ HeisenbergSpin* Lattice::get_object_at(const ipos_t& x) {
     throw std::out_of_range("get_object_at: no site at this position");
 }
 
+// The device keeps each spin as a float4 whose fourth component carries the
+// lifting direction (include/MC.hpp:57): its sign, >= 0 meaning +1.
 void Lattice::to_device() {
     if (!host_newer_) return;
-    std::vector<double> S(3 * spins_.size());
-    for (size_t i = 0; i < spins_.size(); ++i)
-        for (int a = 0; a < 3; ++a) S[3 * i + size_t(a)] = spins_[i].S[a];
-    check(pc_set_spins(sys_, 0, S.data()));
+    std::vector<float> S(4 * spins_.size());
+    for (size_t i = 0; i < spins_.size(); ++i) {
+        for (int a = 0; a < 3; ++a) S[4 * i + size_t(a)] = float(spins_[i].S[a]);
+        S[4 * i + 3] = spins_[i].lifted_dir < 0 ? -1.f : 1.f;
+    }
+    check(pc_set_spins_f4(sys_, 0, S.data()));
     host_newer_ = false;
 }
 
 void Lattice::to_host() {
     if (device_newer_) {
-        std::vector<double> S(3 * spins_.size());
-        check(pc_get_spins(sys_, 0, S.data()));
-        for (size_t i = 0; i < spins_.size(); ++i)
-            for (int a = 0; a < 3; ++a) spins_[i].S[a] = S[3 * i + size_t(a)];
+        std::vector<float> S(4 * spins_.size());
+        check(pc_get_spins_f4(sys_, 0, S.data()));
+        for (size_t i = 0; i < spins_.size(); ++i) {
+            for (int a = 0; a < 3; ++a) spins_[i].S[a] = double(S[4 * i + size_t(a)]);
+            spins_[i].lifted_dir = S[4 * i + 3] < 0.f ? int8_t(-1) : int8_t(1);
+        }
         device_newer_ = false;
     }
     host_newer_ = true;  // the caller holds a mutable reference from here on
@@ -149,15 +155,26 @@ void MC_runner::rebind(Lattice& new_lat) {
     if (ready_ && pc_colours(lat->device(), &n_col, nullptr) != PC_OK) push_to(*lat);
 }
 
-size_t MC_runner::sweep_local_Metropolis_n(double T, size_t n_sweeps, size_t n_overrelax) {
+size_t MC_runner::sweep_n(int update, double T, size_t n_sweeps, size_t n_overrelax) {
     if (!ready_) throw std::logic_error("setup_lattice() has not been called");
     check(pc_set_T_ref(lat->device(), settings.T_ref));
+    check(pc_set_update(lat->device(), update));
     lat->to_device();
     uint64_t acc = 0;
     check(pc_sweep(lat->device(), &T, int(n_sweeps), int(n_overrelax), &acc));
     lat->mark_device_newer();
     return size_t(acc);
 }
+
+size_t MC_runner::sweep_local_Metropolis_n(double T, size_t n_sweeps, size_t n_overrelax) {
+    return sweep_n(0, T, n_sweeps, n_overrelax);
+}
+
+// src/MC.cpp:284-291
+size_t MC_runner::sweep_lifted_Metropolis(double T, size_t n_overrelax) { return sweep_n(1, T, 1, n_overrelax); }
+
+// src/MC.cpp:293-302
+size_t MC_runner::sweep_lifted_Metropolis_rot(double T, size_t n_overrelax) { return sweep_n(2, T, 1, n_overrelax); }
 
 // src/MC.cpp:155-163
 size_t MC_runner::sweep_local_Metropolis(double T, size_t n_overrelax) {

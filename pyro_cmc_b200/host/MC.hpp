@@ -129,6 +129,11 @@ public:
     size_t sweep_local_Metropolis(double T, size_t n_overrelax = 1);
     // n sweeps in one call (one host round trip)
     size_t sweep_local_Metropolis_n(double T, size_t n_sweeps, size_t n_overrelax = 1);
+    // src/MC.cpp:284-302: lifted Metropolis sweeps (u-form / rotation form)
+    size_t sweep_lifted_Metropolis(double T, size_t n_overrelax = 1);
+    size_t sweep_lifted_Metropolis_rot(double T, size_t n_overrelax = 1);
+    // n sweeps of the given single-site move (0 Metropolis, 1 lifted, 2 lifted rotation form)
+    size_t sweep_n(int update, double T, size_t n_sweeps, size_t n_overrelax = 1);
 
     const std::vector<CouplingSpec>& couplings() const { return coupling_specs; }
 

@@ -72,7 +72,6 @@ int main(int argc, char* argv[]) {
                 std::printf("%zu %.17g %d\n", i, T_grid[i], S_idx.count(i) ? 1 : 0);
             return 0;
         }
-        if (prog.boolean("--lifted")) throw std::runtime_error("--lifted is not available in this build");
         if (prog.boolean("--save_state_ft")) throw std::runtime_error("--save_state_ft is not available in this build");
 
         auto lat = build_pyro_lat(prog);
@@ -94,19 +93,21 @@ int main(int argc, char* argv[]) {
         ssf_manager ssfm(lat, prog.strs("--correlators"), file, "/ssf", T_sample, true);
         const double N = double(lat.num_spins());
 
-        std::printf("Done. Begin anneal...\n");
+        // src/anneal.cpp:184-188: --lifted swaps the single-site move
+        const int update = prog.boolean("--lifted") ? 1 : 0;
+        std::printf("Done. Begin anneal%s...\n", update ? " (lifted Metropolis)" : "");
         std::printf("Burning in (%zu sweeps)...\n", n_burn_in);
-        mc.sweep_local_Metropolis_n(T_hot, n_burn_in);
+        mc.sweep_n(update, T_hot, n_burn_in);
         for (size_t i = 0; i < T_grid.size(); ++i) {
             const double T = T_grid[i];
             e_manager.new_T(T);
-            const size_t accepted = mc.sweep_local_Metropolis_n(T, n_sweep);
+            const size_t accepted = mc.sweep_n(update, T, n_sweep);
             e_manager.sample(mc.total_energy_per_unit_cell());
             if (S_idx.count(i)) {
                 std::printf("Sampling at T=%lf (%zu sweeps)...\n", T, n_sample);
                 ssfm.new_T(T);
                 for (size_t k = 0; k < n_sample; k++) {
-                    const size_t accepted_ssf = mc.sweep_local_Metropolis_n(T, n_sweep);
+                    const size_t accepted_ssf = mc.sweep_n(update, T, n_sweep);
                     std::printf("[ssf] Iter %4zu T=%.3e Acceptance rate: %.2f%%\n", k, T,
                                 accepted_ssf * 100.0 / N / double(n_sweep));
                     ssfm.sample();

@@ -142,7 +142,7 @@ def test_colour_classes():
 
 
 @pytest.mark.parametrize("schedule", [0, 1])
-@pytest.mark.parametrize("path", ["generic", "v0", "v1", "v2"])
+@pytest.mark.parametrize("path", ["generic", "v0", "v1", "v2", "v3"])
 @pytest.mark.parametrize("colouring", [0, 1])
 @pytest.mark.parametrize("T", [0.3, 2.0])
 def test_sweeps_follow_oracle_mirror(colouring, T, path, schedule):
@@ -184,6 +184,15 @@ def test_sweep_reflection_mode_follows_oracle(schedule):
     assert np.mean(d <= 1e-4) >= 0.95 and d.max() <= 1e-3
 
 
+def _close_rounding(a, b):
+    """Two FP32 chains that differ only in rounding, a few sweeps apart:
+    99.5 % of the components within 1e-5, all within 1e-3 (an overrelaxation
+    about a nearly cancelling field amplifies a last-bit difference)."""
+    d = np.abs(np.asarray(a, float) - np.asarray(b, float))
+    assert (d <= 1e-5).mean() >= 0.995, (d <= 1e-5).mean()
+    assert d.max() <= 1e-3, d.max()
+
+
 def _sweep_state(L, n, setup, c=COUPLINGS[1], schedule=1):
     g = pc.pyrochlore_system(L, seed=4, schedule=schedule, **c)
     g.random_spins(9)
@@ -206,6 +215,37 @@ def test_launch_modes_give_identical_sweeps(schedule):
         S, acc = _sweep_state(L, n, setup, schedule=schedule)
         assert np.array_equal(S, ref)
         assert np.array_equal(acc, acc_ref)
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("threads", [64, 256])
+def test_staged_rows_match_per_site_kernel(schedule, threads):
+    """Load variant 3 (neighbour rows staged by bulk copies) against the
+    per-site kernel over two sweeps: the same moves up to FP32 rounding (the
+    two kernels may contract the arithmetic differently, and a chaotic chain
+    amplifies a last-bit difference over many sweeps)."""
+    L, n = 6, 2
+    ref, acc_ref = _sweep_state(L, n, lambda g: g.set_tile(threads, 0), schedule=schedule)
+    S, acc = _sweep_state(L, n, lambda g: (g.set_tile(threads, 0), g.set_load_variant(3)), schedule=schedule)
+    _close_rounding(S, ref)
+    assert np.array_equal(acc, acc_ref)
+
+
+def test_mixed_sizes_staged_rows():
+    """Replicas of different L in one launch (row tiles of different shapes,
+    a ragged last tile for L = 12): the staged kernel makes the same moves as
+    the per-site kernel, up to FP32 rounding."""
+    Ls = [3, 8, 5, 12]
+    out = []
+    for variant in (0, 3):
+        g = pc.pyrochlore_system(Ls, seed=6, schedule=1, **COUPLINGS[1])
+        g.set_load_variant(variant)
+        g.random_spins(4)
+        acc = g.sweep(0.9, 2, 1)
+        out.append((acc, [g.spins_f4(r) for r in range(len(Ls))]))
+    assert np.array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        _close_rounding(a, b)
 
 
 def test_batched_replicas_are_independent_streams():
