@@ -44,3 +44,27 @@ def ssf(S: np.ndarray, L: int, corr) -> np.ndarray:
         out[c, :, 0] = v.real
         out[c, :, 1] = v.imag
     return out
+
+
+def adjoint(S: np.ndarray, L: int, corr, dval: np.ndarray) -> np.ndarray:
+    """dLoss/dS_i^c for dLoss/dS^{ab}(k) = dval[n_corr, L^3, 2] (real, imag
+    parts): Re sum_k exp(+i q.x_i) Y^c(k), Y^c = sum over correlators of
+    [c == a] conj(D) B^b + [c == b] D B^a, D = dval[..., 0] + i dval[..., 1].
+    Returns [16*L^3, 3] in storage order."""
+    B = amplitudes(S, L)
+    Y = np.zeros_like(B)
+    for c, name in enumerate(corr):
+        a, b = AXIS[name[0]], AXIS[name[1]]
+        D = dval[c, :, 0] + 1j * dval[c, :, 1]
+        Y[a] += np.conj(D) * B[b]
+        Y[b] += D * B[a]
+    Y = Y.reshape(3, L, L, L)  # [a][Kx][Ky][Kz]
+    K = np.arange(L)
+    out = np.empty((16, L, L, L, 3))  # [sl][cz][cy][cx][a]
+    for sl in range(16):
+        r = R_SL[sl]
+        ph = [np.exp(+2j * np.pi * K * r[d] / (8 * L)) for d in range(3)]
+        Z = Y * ph[0][None, :, None, None] * ph[1][None, None, :, None] * ph[2][None, None, None, :]
+        G = np.fft.ifftn(Z, axes=(1, 2, 3)) * L ** 3  # [a][cx][cy][cz], exp(+)
+        out[sl] = np.transpose(G.real, (3, 2, 1, 0))
+    return out.reshape(16 * L ** 3, 3)

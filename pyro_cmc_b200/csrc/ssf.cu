@@ -343,6 +343,153 @@ __global__ void __launch_bounds__(512) ssf_line_kernel(const SsfGeom g, const fl
     }
 }
 
+// ------------------------------------------------ fast-path backward (P, Q <= 8)
+// dLoss/dS_i^c = Re sum_K exp(+i q.x_i) Y^c(K), with
+// Y^c(K) = sum_corr [c == a] conj(D) B^b + [c == b] D B^a, D = dL/dReS + i dL/dImS.
+// Adjoint stage z, one CTA per (replica, Ky, chunk of C Kx values): Y^a times
+// the conjugate z phase of each z group, inverse z-DFT of the 12 line sets ->
+// H[replica][a][gz][nz][Ky][Kx].
+template <int LT>
+__global__ void __launch_bounds__(512) ssf_line_adj_kernel(const SsfGeom g, const SsfOut o, const double* __restrict__ dval,
+                                                           const float2* __restrict__ amp, float2* __restrict__ H) {
+    extern __shared__ float2 sm[];
+    const SsfDims<LT> dm(g);
+    const int L = dm.L, LL = L * L, P = dm.P, Q = dm.Q;
+    const int C = ssf_chunk(L), CP = C + 1;
+    const int n_chunk = (L + C - 1) / C;
+    float2* tw = sm;
+    float2* ph = tw + L;
+    float2* T = ph + 8 * L;
+    const int chunk = blockIdx.x % n_chunk;
+    const int Ky = (blockIdx.x / n_chunk) % L;
+    const int rp = (blockIdx.x / n_chunk) / L;
+    const int Kx0 = chunk * C;
+    const int nc = min(C, L - Kx0);
+    const int n_k = L * LL;
+    fill_tables(tw, ph, L);
+    __syncthreads();
+    for (int i = threadIdx.x; i < L * C; i += blockDim.x) {
+        const int c = i / L, Kz = i - c * L;
+        float2 y[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        if (c < nc) {
+            const size_t k = (size_t(Kx0 + c) * L + Ky) * L + Kz;
+            float2 b[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) b[a] = amp[(size_t(rp) * 3 + a) * n_k + k];
+#pragma unroll
+            for (int cc = 0; cc < 9; ++cc) {
+                if (cc >= o.n_corr) break;
+                const double2 d2 = *reinterpret_cast<const double2*>(dval + ((size_t(rp) * o.n_corr + cc) * n_k + k) * 2);
+                const float2 D = make_float2(float(d2.x), float(d2.y));
+                const int ca = o.corr_a[cc], cb = o.corr_b[cc];
+                const float2 ba = ca == 0 ? b[0] : (ca == 1 ? b[1] : b[2]);
+                const float2 bb = cb == 0 ? b[0] : (cb == 1 ? b[1] : b[2]);
+                const float2 t1 = cmulc(bb, D);  // conj(D) B^b -> Y^a
+                const float2 t2 = cmul(D, ba);   // D B^a      -> Y^b
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    if (q == ca) {
+                        y[q].x += t1.x;
+                        y[q].y += t1.y;
+                    }
+                    if (q == cb) {
+                        y[q].x += t2.x;
+                        y[q].y += t2.y;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int gz = 0; gz < 4; ++gz)  // times exp(+i qz rz)
+                T[((a * 4 + gz) * L + Kz) * CP + c] = cmulc(y[a], phase(ph, L, Kz * (2 * gz - 1)));
+    }
+    __syncthreads();
+    const int lpr = max(1, int(kPassBItems * blockDim.x) / P);
+    auto zl = [=](int l, int e) {
+        const int ag = l / C;
+        return (ag * L + e) * CP + (l - ag * C);
+    };
+    dft_lines<true, true>(T, P, Q, 12 * C, lpr, zl, tw);
+    const size_t L3 = size_t(L) * LL;
+    for (int i = threadIdx.x; i < 12 * L * C; i += blockDim.x) {
+        const int c = i % C, zr = i / C;  // zr = (a*4 + gz) * L + nz
+        if (c >= nc) continue;
+        const int ag = zr / L, nz = zr - ag * L;
+        H[(size_t(rp) * 12 + ag) * L3 + size_t(nz) * LL + size_t(Ky) * L + Kx0 + c] = T[zr * CP + c];
+    }
+}
+
+// Adjoint stage xy, one CTA per (replica, z plane, z group, sublattice pair):
+// X_a(K) = H_a(K) exp(+i q.r_s0) (x, y parts), Y_a likewise for s1; the real
+// part of the inverse 2-D DFT of X_a is the inverse DFT of its Hermitian part
+// (X_a(K) + conj X_a(-K)) / 2, so Z_a = herm(X_a) + i herm(Y_a) gives both
+// sublattices' gradients in one transform: Re -> s0, Im -> s1.
+template <int LT, bool SWZ>
+__global__ void __launch_bounds__(512) ssf_plane_adj_kernel(const SsfGeom g, const float2* __restrict__ H,
+                                                            const ReplicaDev* __restrict__ reps,
+                                                            float4* __restrict__ grad) {
+    extern __shared__ float2 sm[];
+    const SsfDims<LT> dm(g);
+    const int L = dm.L, LL = L * L, P = dm.P, Q = dm.Q;
+    float2* tw = sm;
+    float2* ph = tw + L;
+    float2* buf = ph + 8 * L;  // planes Z_0, Z_1, Z_2
+    const int h = blockIdx.x & 7, gz = h >> 1, pr = h & 1;
+    const int nz = (blockIdx.x >> 3) % L;
+    const int rp = (blockIdx.x >> 3) / L;
+    const ReplicaDev rep = reps[g.rep_index[rp]];
+    const int s0 = c_zgroup[gz][2 * pr], s1 = c_zgroup[gz][2 * pr + 1];
+    const int rx0 = c_rsl[s0][0], ry0 = c_rsl[s0][1], rx1 = c_rsl[s1][0], ry1 = c_rsl[s1][1];
+    const size_t L3 = size_t(L) * LL;
+    fill_tables(tw, ph, L);
+    __syncthreads();
+    for (int i = threadIdx.x; i < LL; i += blockDim.x) {
+        const int Ky = i / L, Kx = i - Ky * L;
+        const int mx = Kx ? L - Kx : 0, my = Ky ? L - Ky : 0;
+        const int im = my * L + mx;
+        // conj of the forward phases at K and at -K
+        const float2 e0 = cmul(phase(ph, L, Kx * rx0), phase(ph, L, Ky * ry0));
+        const float2 e1 = cmul(phase(ph, L, Kx * rx1), phase(ph, L, Ky * ry1));
+        const float2 f0 = cmul(phase(ph, L, mx * rx0), phase(ph, L, my * ry0));
+        const float2 f1 = cmul(phase(ph, L, mx * rx1), phase(ph, L, my * ry1));
+        const int q = plane_pos<SWZ>(Kx, Ky, L);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float2* Ha = H + ((size_t(rp) * 3 + a) * 4 + gz) * L3 + size_t(nz) * LL;
+            const float2 hk = Ha[i], hm = Ha[im];
+            const float2 X = cmulc(hk, e0), Xm = cmulc(hm, f0);  // X(K), X(-K)
+            const float2 Y = cmulc(hk, e1), Ym = cmulc(hm, f1);
+            // herm(X) = (X + conj Xm)/2, herm(Y) likewise; Z = herm(X) + i herm(Y)
+            const float2 hx = make_float2(0.5f * (X.x + Xm.x), 0.5f * (X.y - Xm.y));
+            const float2 hy = make_float2(0.5f * (Y.x + Ym.x), 0.5f * (Y.y - Ym.y));
+            buf[a * LL + q] = make_float2(hx.x - hy.y, hx.y + hy.x);
+        }
+    }
+    __syncthreads();
+    const int lpr = max(1, int(kPassBItems * blockDim.x) / P);
+    auto col = [=](int l, int e) {
+        const int b = l / L;
+        return b * LL + plane_pos<SWZ>(l - b * L, e, L);
+    };
+    dft_lines<true, true>(buf, P, Q, 3 * L, lpr, col, tw);
+    auto row = [=](int l, int e) {
+        const int b = l / L;
+        return b * LL + plane_pos<SWZ>(e, l - b * L, L);
+    };
+    dft_lines<true, false>(buf, P, Q, 3 * L, lpr, row, tw);
+    float4* g0 = grad + rep.off + size_t(s0) * rep.Nc + size_t(nz) * LL;
+    float4* g1 = grad + rep.off + size_t(s1) * rep.Nc + size_t(nz) * LL;
+    for (int i = threadIdx.x; i < LL; i += blockDim.x) {
+        const int y = i / L, x = i - y * L;
+        const int q = plane_pos<SWZ>(x, y, L);
+        const float2 z0 = buf[q], z1 = buf[LL + q], z2 = buf[2 * LL + q];
+        g0[i] = make_float4(z0.x, z1.x, z2.x, 0.f);
+        g1[i] = make_float4(z0.y, z1.y, z2.y, 0.f);
+    }
+}
+
 // ------------------------------------------------ generic path, P or Q > 8
 // stage 1: per (replica, z plane, z group), runtime-length DFT loops
 __global__ void __launch_bounds__(256) ssf_xy_kernel(const SsfGeom g, const float4* __restrict__ spins,
@@ -629,6 +776,17 @@ void ssf_prepare() {
     cudaFuncSetAttribute(ssf_line_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_adj_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_adj_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_adj_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_adj_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_adj_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_adj_kernel<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_adj_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_adj_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_adj_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_adj_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_adj_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_xy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(ssf_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(ssf_adj_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -639,6 +797,37 @@ void launch_ssf_adjoint(const SsfGeom& g, const SsfOut& o, const double* dval, c
                         float4* grad_S, const ReplicaDev* reps, cudaStream_t st) {
     const int L = g.L, C = ssf_chunk(L);
     const int n_chunk = (L + C - 1) / C;
+    if (ssf_fast_path(g.P, g.Q)) {
+        const size_t smem_z = sizeof(float2) * (size_t(9) * L + 12 * size_t(L) * (C + 1));
+        const int grid_z = g.n_rep * L * n_chunk, thr_z = ssf_line_threads(L, g.P, g.Q);
+        const size_t smem_xy = sizeof(float2) * (size_t(9) * L + 3 * size_t(L) * L);
+        const int grid_xy = g.n_rep * L * 8, thr_xy = ssf_plane_threads(L);
+        switch (L) {
+            case 64:
+                ssf_line_adj_kernel<64><<<grid_z, thr_z, smem_z, st>>>(g, o, dval, amp, H);
+                ssf_plane_adj_kernel<64, true><<<grid_xy, thr_xy, smem_xy, st>>>(g, H, reps, grad_S);
+                break;
+            case 32:
+                ssf_line_adj_kernel<32><<<grid_z, thr_z, smem_z, st>>>(g, o, dval, amp, H);
+                ssf_plane_adj_kernel<32, true><<<grid_xy, thr_xy, smem_xy, st>>>(g, H, reps, grad_S);
+                break;
+            case 16:
+                ssf_line_adj_kernel<16><<<grid_z, thr_z, smem_z, st>>>(g, o, dval, amp, H);
+                ssf_plane_adj_kernel<16, true><<<grid_xy, thr_xy, smem_xy, st>>>(g, H, reps, grad_S);
+                break;
+            case 8:
+                ssf_line_adj_kernel<8><<<grid_z, thr_z, smem_z, st>>>(g, o, dval, amp, H);
+                ssf_plane_adj_kernel<8, false><<<grid_xy, thr_xy, smem_xy, st>>>(g, H, reps, grad_S);
+                break;
+            default:
+                ssf_line_adj_kernel<0><<<grid_z, thr_z, smem_z, st>>>(g, o, dval, amp, H);
+                if (L % 16 == 0)
+                    ssf_plane_adj_kernel<0, true><<<grid_xy, thr_xy, smem_xy, st>>>(g, H, reps, grad_S);
+                else
+                    ssf_plane_adj_kernel<0, false><<<grid_xy, thr_xy, smem_xy, st>>>(g, H, reps, grad_S);
+        }
+        return;
+    }
     const size_t smem_z = sizeof(float2) * (size_t(9) * L + 5 * size_t(L) * C);
     ssf_adj_z_kernel<<<g.n_rep * L * n_chunk, 256, smem_z, st>>>(g, o, dval, amp, H);
     const size_t smem_xy = sizeof(float2) * (size_t(9) * L + 3 * size_t(L) * L);

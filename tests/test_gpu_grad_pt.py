@@ -261,3 +261,26 @@ def test_anneal_config1_statistical_parity(schedule):
     # order (descending), as does the oracle
     _stats_compare(s_gpu.mean(0).ravel(), (s_gpu.std(0, ddof=1) / np.sqrt(K)).ravel(),
                    s_cpu.mean(0).ravel(), (s_cpu.std(0, ddof=1) / np.sqrt(K)).ravel(), "S(q)")
+
+
+@pytest.mark.parametrize("L", [8, 11, 16, 64])
+def test_ssf_backward_large_L_matches_fft_adjoint(L):
+    """The S(q) backward at sizes beyond finite differences: L = 11 (runtime
+    line length), 8, 16 and 64 (the instantiated sizes; 16 and 64 with the
+    swizzled shared layout), against the numpy-FFT adjoint of
+    ssf_manager::sample."""
+    from oracle import ssf_fft
+    corr = ["xx", "yy", "zz", "xy", "xz", "yz", "zx"]
+    g = pc.pyrochlore_system(L, J1=1.0)
+    g.ssf_configure(corr, 0, [])
+    g.random_spins(L)
+    spins = ag.spins_tensor(g).clone().requires_grad_(True)
+    rng = np.random.default_rng(L)
+    nk = L ** 3
+    D = rng.normal(size=(1, len(corr), nk, 2))
+    S = ag.ssf(g, spins)
+    (S * torch.as_tensor(D, device="cuda")).sum().backward()
+    got = spins.grad[:, :3].cpu().numpy()
+    ref = ssf_fft.adjoint(g.spins(), L, corr, D[0])
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 1e-5 * scale * max(1.0, np.log2(nk)), np.abs(got - ref).max() / scale

@@ -236,3 +236,57 @@ def test_anneal_runs_and_cools():
     assert e[-1] < e[0]
     assert ssum.shape == (1, 1, 8, 2)
     assert (ssq[..., 0] >= 0).all()
+
+
+def _bench_lifted_estimates(update, seed, L=2, T=0.5, n_burn=400, n_sample=2500):
+    """test/bench_lifted.cpp:100-133 on the pyrochlore lattice: <E>, <E^2> per
+    spin and batch-means errors for one sampler."""
+    s = oracle.System(L, J1=-1.0, J2=0.3, seed=seed)
+    s.random_spins(seed + 1)
+    sweep = (lambda: s.sweep(T, 1, 1)) if update == "standard" else \
+        (lambda: s.sweep_lifted(T, 1, 1, rot=(update == "rot")))
+    for _ in range(n_burn):
+        sweep()
+    e = np.empty(n_sample)
+    for i in range(n_sample):
+        sweep()
+        e[i] = s.energy() / 16.0  # per spin
+    nb = 25
+    bm = lambda x: x[: len(x) // nb * nb].reshape(nb, -1).mean(axis=1)
+    err = lambda x: bm(x).std(ddof=1) / np.sqrt(nb)
+    return e.mean(), (e ** 2).mean(), err(e), err(e ** 2)
+
+
+@pytest.mark.parametrize("update", ["lifted", "rot"])
+def test_lifted_restatement_samples_the_boltzmann_distribution(update):
+    """The reference's own acceptance test for lifted Metropolis
+    (test/bench_lifted.cpp:240-272: |<E>_std - <E>_lifted| and the same for
+    <E^2> below 0.1 min(|J1|, |J2|)), run on the oracle's restatement with the
+    reference's J1 = -1, J2 = 0.3, T = 0.5 on the pyrochlore lattice."""
+    a = _bench_lifted_estimates("standard", 11)
+    b = _bench_lifted_estimates(update, 29)
+    tol = 0.1 * min(1.0, 0.3)
+    assert abs(a[0] - b[0]) < tol, (a, b)
+    assert abs(a[1] - b[1]) < tol, (a, b)
+    # and statistically: within 5 sigma of the batch-means errors
+    assert abs(a[0] - b[0]) < 5 * np.hypot(a[2], b[2]) + 1e-3, (a, b)
+
+
+def test_ssf_fft_adjoint_matches_finite_differences():
+    """The numpy S(q) adjoint (the checker of the GPU backward at large L)
+    against FP64 central differences of the numpy forward."""
+    from oracle import ssf_fft
+    L = 2
+    corr = ["xx", "yy", "zz", "xy", "xz", "yz", "zx"]
+    rng = np.random.default_rng(3)
+    S = rng.normal(size=(16 * L ** 3, 3))
+    dval = rng.normal(size=(len(corr), L ** 3, 2))
+    loss = lambda X: float((ssf_fft.ssf(X, L, corr) * dval).sum())
+    g = ssf_fft.adjoint(S, L, corr, dval)
+    h = 1e-5
+    for i, a in [(0, 0), (5, 1), (37, 2), (100, 0), (127, 2)]:
+        Sp, Sm = S.copy(), S.copy()
+        Sp[i, a] += h
+        Sm[i, a] -= h
+        fd = (loss(Sp) - loss(Sm)) / (2 * h)
+        assert abs(fd - g[i, a]) <= 1e-6 * max(1.0, abs(fd)), (i, a, fd, g[i, a])
