@@ -198,6 +198,16 @@ int pc_local_field(pc_system* sys, int replica, double* h);
  * (temperatures), each for replicas of size L_of_slot[slot]. Bad labels fail
  * with PC_ERR_INVALID and the reference's message. Clears all slots. */
 int pc_ssf_configure(pc_system* sys, const char* const* names, int n_corr, int n_slots, const int32_t* L_of_slot);
+/* Sublattice-resolved accumulators (resolved != 0): the correlator of
+ * ssf_manager::sample before its phase contraction, C^{ab}_{mu nu}(k) =
+ * conj(A^a_mu(k)) A^b_nu(k) with A^a_mu the DFT over cells of S^a on sublattice
+ * mu (include/ssf_manager.hpp:260-293, correlate()), accumulated as sums and
+ * (Re)^2, (Im)^2 sums in the layout [n_corr][n_k][16][16][2] per slot that
+ * src/temper.cpp:121-159 writes to /ssf. 256x the memory of the contracted
+ * form. Call before pc_ssf_configure (it invalidates a configured SSF); the
+ * reads (pc_ssf_read, pc_ssf_current) then return the resolved layout.
+ * Needs every L to factor into two parts <= 8 (L <= 64). */
+int pc_ssf_set_resolved(pc_system* sys, int resolved);
 /* ssf_manager::sample (include/ssf_manager.hpp:260-293) for every replica r
  * with slot_of_replica[r] >= 0 (host array): accumulates S(q) and
  * (Re S)^2, (Im S)^2 into that slot in FP64 and counts the sample. */
@@ -304,6 +314,18 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
 /* CUDA events around the last pc_sweep call's kernels: average duration in
  * milliseconds of the Metropolis and overrelaxation colour-pass kernels. */
 int pc_last_kernel_times(pc_system* sys, double* metropolis_ms, double* overrelax_ms);
+/* Luttinger-Tisza bound (src/luttinger_tisza.cpp, the ltgs program): for
+ * every k = 2 pi K / (8L) of the L^3 grid the smallest eigenvalue of the
+ * 48 x 48 Hermitian M(k) = sum over directed bonds J_bond exp(i k.d)
+ * (build_bonds :31-81: J1 XXZ, J2, J3a, J3b; zero couplings skipped;
+ * :153-178), on the GPU in FP64. Outputs (each may be null):
+ * lambda_map[L^3] (flat C order over K, the reference's eigenvalue_map),
+ * *e_per_spin = lambda_min / 2 (:181, the reference's E_min), k_star[3] = the
+ * first K in flat order attaining the minimum, eigvec[48][2] = a unit
+ * eigenvector there (rows spin-x,y,z of sublattice 0, 1, ...). Uses the
+ * current device; needs no pc_system. */
+int pc_lt_minimum(int L, double J1, double J2, double J3, double Delta, double* lambda_map, double* e_per_spin,
+                  int64_t* k_star, double* eigvec);
 /* Enables per-kernel CUDA-event timing (off by default). */
 int pc_set_kernel_timing(pc_system* sys, int on);
 /* Launch overlap of consecutive colour passes (on by default): each pass is

@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpyrocmc.so")
-SOURCES = ["system.cu", "sweep.cu", "ssf.cu", "pt.cu", "noalloc.cu"]
+SOURCES = ["system.cu", "sweep.cu", "ssf.cu", "pt.cu", "noalloc.cu", "lt.cu"]
 HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh", "struct_field.cuh"]
 
 NVCC_FLAGS = [

@@ -107,6 +107,7 @@ struct SsfGeom {
     int P, Q;  // L = P*Q, two-level Cooley-Tukey split
     int n_rep;
     const int32_t* rep_index;  // replicas of this size (device)
+    int resolved = 0;          // 1: sublattice-resolved correlators [n_corr][n_k][16][16][2]
 };
 
 // Raises the dynamic shared-memory limits of the SSF kernels (once, host side).
@@ -118,7 +119,8 @@ void launch_ssf_xy(const SsfGeom& g, const float4* spins, const ReplicaDev* reps
 struct SsfOut {
     int n_corr;
     int corr_a[9], corr_b[9];
-    // accumulate mode: sum/sq [slot][n_corr][n_k][2] doubles, slot per replica
+    // accumulate mode: sum/sq [slot][n_corr][n_k][2] doubles ([slot][n_corr][n_k][16][16][2]
+    // when resolved), slot per replica
     double* acc_sum;
     double* acc_sq;
     const int32_t* slot_of_rep;  // indexed by replica index

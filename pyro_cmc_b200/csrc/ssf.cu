@@ -168,7 +168,7 @@ struct SsfDims {
         : L(LT ? LT : g.L), P(LT ? ct_split_P(LT) : g.P), Q(LT ? LT / ct_split_P(LT) : g.Q) {}
 };
 
-template <int LT, bool SWZ>
+template <int LT, bool SWZ, bool RES>
 __global__ void __launch_bounds__(512) ssf_plane_kernel(const SsfGeom g, const float4* __restrict__ spins,
                                                         const ReplicaDev* __restrict__ reps, float2* __restrict__ G) {
     extern __shared__ float2 sm[];
@@ -207,6 +207,25 @@ __global__ void __launch_bounds__(512) ssf_plane_kernel(const SsfGeom g, const f
     dft_lines<false, true>(buf, P, Q, 3 * L, lpr, col, tw);
     const int rx0 = c_rsl[s0][0], ry0 = c_rsl[s0][1], rx1 = c_rsl[s1][0], ry1 = c_rsl[s1][1];
     const size_t L3 = size_t(L) * LL;
+    if constexpr (RES) {
+        // per-sublattice planes, no phases: G[replica][a][sl][nz][Ky][Kx]
+        float2* Gr = G + size_t(rp) * 48 * L3 + size_t(nz) * LL;
+        for (int i = threadIdx.x; i < LL; i += blockDim.x) {
+            const int Ky = i / L, Kx = i - Ky * L;
+            const int q = plane_pos<SWZ>(Kx, Ky, L);
+            const int qm = plane_pos<SWZ>(Kx ? L - Kx : 0, Ky ? L - Ky : 0, L);
+            const float2 a = buf[q], am = buf[qm];
+            const float2 b = buf[LL + q], bm = buf[LL + qm];
+            const float2 z = buf[2 * LL + q], zm = buf[2 * LL + qm];
+            Gr[size_t(0 * 16 + s0) * L3 + i] = make_float2(0.5f * (a.x + am.x), 0.5f * (a.y - am.y));
+            Gr[size_t(1 * 16 + s0) * L3 + i] = make_float2(0.5f * (a.y + am.y), -0.5f * (a.x - am.x));
+            Gr[size_t(2 * 16 + s0) * L3 + i] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            Gr[size_t(0 * 16 + s1) * L3 + i] = make_float2(0.5f * (b.x + bm.x), 0.5f * (b.y - bm.y));
+            Gr[size_t(1 * 16 + s1) * L3 + i] = make_float2(0.5f * (b.y + bm.y), -0.5f * (b.x - bm.x));
+            Gr[size_t(2 * 16 + s1) * L3 + i] = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+        }
+        return;
+    }
     float2* Gx = G + ((size_t(rp) * 3) * 8 + h) * L3 + size_t(nz) * LL;
     float2* Gy = Gx + 8 * L3;
     float2* Gz = Gy + 8 * L3;
@@ -339,6 +358,84 @@ __global__ void __launch_bounds__(512) ssf_line_kernel(const SsfGeom g, const fl
                     }
                 }
             }
+        }
+    }
+}
+
+// ------------------------------------------------ sublattice-resolved S(q)
+// The reference's correlate() output before contract(): for each correlator
+// (a, b), C_{mu nu}(K) = conj(A^a_mu(K)) A^b_nu(K) with A^a_mu the 3-D DFT over
+// cells of S^a on sublattice mu (include/ssf_manager.hpp:260-293; the layout
+// [n_corr, n_k, n_sl, n_sl, 2] that src/temper.cpp:121-159 writes). Stage 1 is
+// ssf_plane_kernel<.., RES = true> (per-sublattice planes, no phases);
+// then the z-DFT in place, then one CTA per (replica, K) for the 256 (mu, nu).
+__host__ __device__ __forceinline__ int ssf_chunk_res(int L) { return L <= 16 ? L : (L <= 32 ? 8 : 4); }
+
+template <int LT>
+__global__ void __launch_bounds__(256) ssf_zdft_res_kernel(const SsfGeom g, float2* __restrict__ G) {
+    extern __shared__ float2 sm[];
+    const SsfDims<LT> dm(g);
+    const int L = dm.L, LL = L * L, P = dm.P, Q = dm.Q;
+    const int C = ssf_chunk_res(L), CP = C + 1, PS = L * CP + 1;  // odd plane stride
+    const int n_chunk = (L + C - 1) / C;
+    float2* tw = sm;
+    float2* ph = tw + L;
+    float2* T = ph + 8 * L;  // [48][L][CP], planes PS apart
+    const int chunk = blockIdx.x % n_chunk;
+    const int Ky = (blockIdx.x / n_chunk) % L;
+    const int rp = (blockIdx.x / n_chunk) / L;
+    const int Kx0 = chunk * C;
+    const int nc = min(C, L - Kx0);
+    const size_t L3 = size_t(L) * LL;
+    float2* base = G + size_t(rp) * 48 * L3 + size_t(Ky) * L + Kx0;
+    fill_tables(tw, ph, L);
+    for (int i = threadIdx.x; i < 48 * L * C; i += blockDim.x) {
+        const int c = i % C, zr = i / C;  // zr = plane * L + z
+        const int pl = zr / L, z = zr - pl * L;
+        T[pl * PS + z * CP + c] = c < nc ? base[size_t(pl) * L3 + size_t(z) * LL + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int lpr = max(1, int(kPassBItems * blockDim.x) / P);
+    auto zl = [=](int l, int e) {
+        const int pl = l / C;
+        return pl * PS + e * CP + (l - pl * C);
+    };
+    dft_lines<false, true>(T, P, Q, 48 * C, lpr, zl, tw);
+    for (int i = threadIdx.x; i < 48 * L * C; i += blockDim.x) {
+        const int c = i % C, zr = i / C;
+        const int pl = zr / L, z = zr - pl * L;
+        if (c < nc) base[size_t(pl) * L3 + size_t(z) * LL + c] = T[pl * PS + z * CP + c];
+    }
+}
+
+// One CTA of 256 threads per (replica, K); thread t = 16 mu + nu.
+__global__ void __launch_bounds__(256) ssf_accum_res_kernel(const SsfGeom g, const float2* __restrict__ A, const SsfOut o) {
+    __shared__ float2 amp[48];
+    const int L = g.L, LL = L * L;
+    const int n_k = L * LL;
+    const int k = blockIdx.x % n_k, rp = blockIdx.x / n_k;
+    const int Kx = k / LL, Ky = (k / L) % L, Kz = k % L;
+    const size_t L3 = size_t(L) * LL;
+    const int t = threadIdx.x;
+    if (t < 48) amp[t] = A[(size_t(rp) * 48 + t) * L3 + size_t(Kz) * LL + size_t(Ky) * L + Kx];
+    __syncthreads();
+    const int mu = t >> 4, nu = t & 15;
+    const int rep_glob = g.rep_index[rp];
+    const int slot = o.acc_sum ? o.slot_of_rep[rep_glob] : -1;
+#pragma unroll
+    for (int cc = 0; cc < 9; ++cc) {
+        if (cc >= o.n_corr) break;
+        const float2 a = amp[o.corr_a[cc] * 16 + mu], b = amp[o.corr_b[cc] * 16 + nu];
+        const double re = double(a.x) * b.x + double(a.y) * b.y;  // conj(A^a_mu) A^b_nu
+        const double im = double(a.x) * b.y - double(a.y) * b.x;
+        const size_t off = (size_t(cc) * n_k + k) * 256 + t;
+        if (o.val) reinterpret_cast<double2*>(o.val + (size_t(rp) * o.n_corr * n_k * 256) * 2)[off] = make_double2(re, im);
+        if (slot >= 0) {
+            double2* s = reinterpret_cast<double2*>(o.acc_sum + size_t(slot) * o.slot_stride) + off;
+            double2* q = reinterpret_cast<double2*>(o.acc_sq + size_t(slot) * o.slot_stride) + off;
+            const double2 sv = *s, qv = *q;
+            *s = make_double2(sv.x + re, sv.y + im);
+            *q = make_double2(qv.x + re * re, qv.y + im * im);
         }
     }
 }
@@ -536,6 +633,22 @@ __global__ void __launch_bounds__(256) ssf_xy_kernel(const SsfGeom g, const floa
     }
 }
 
+template <bool RES>
+void launch_plane(const SsfGeom& g, const float4* spins, const ReplicaDev* reps, float2* G, int grid, int threads,
+                  size_t smem, cudaStream_t st) {
+    switch (g.L) {
+        case 64: ssf_plane_kernel<64, true, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+        case 32: ssf_plane_kernel<32, true, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+        case 16: ssf_plane_kernel<16, true, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+        case 8: ssf_plane_kernel<8, false, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+        default:
+            if (g.L % 16 == 0)
+                ssf_plane_kernel<0, true, RES><<<grid, threads, smem, st>>>(g, spins, reps, G);
+            else
+                ssf_plane_kernel<0, false, RES><<<grid, threads, smem, st>>>(g, spins, reps, G);
+    }
+}
+
 int ssf_plane_threads(int L) { return std::min(512, std::max(64, (L * L / 8 + 31) / 32 * 32)); }
 int ssf_line_threads(int L, int P, int Q) {
     const int items = 12 * ssf_chunk(L) * std::max(P, Q) / 4;
@@ -548,17 +661,10 @@ void launch_ssf_xy(const SsfGeom& g, const float4* spins, const ReplicaDev* reps
     if (ssf_fast_path(g.P, g.Q)) {
         const int threads = ssf_plane_threads(L);
         const int grid = g.n_rep * L * 8;
-        switch (L) {
-            case 64: ssf_plane_kernel<64, true><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
-            case 32: ssf_plane_kernel<32, true><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
-            case 16: ssf_plane_kernel<16, true><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
-            case 8: ssf_plane_kernel<8, false><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
-            default:
-                if (L % 16 == 0)
-                    ssf_plane_kernel<0, true><<<grid, threads, smem, st>>>(g, spins, reps, G);
-                else
-                    ssf_plane_kernel<0, false><<<grid, threads, smem, st>>>(g, spins, reps, G);
-        }
+        if (g.resolved)
+            launch_plane<true>(g, spins, reps, G, grid, threads, smem, st);
+        else
+            launch_plane<false>(g, spins, reps, G, grid, threads, smem, st);
         return;
     }
     ssf_xy_kernel<<<g.n_rep * L * 4, 256, smem, st>>>(g, spins, reps, G);
@@ -646,6 +752,21 @@ __global__ void __launch_bounds__(256) ssf_z_kernel(const SsfGeom g, const float
 void launch_ssf_z(const SsfGeom& g, const float2* G, const SsfOut& o, cudaStream_t st) {
     const int L = g.L, C = ssf_chunk(L);
     const int n_chunk = (L + C - 1) / C;
+    if (ssf_fast_path(g.P, g.Q) && g.resolved) {
+        const int Cr = ssf_chunk_res(L);
+        const size_t smem = sizeof(float2) * (size_t(9) * L + 48 * (size_t(L) * (Cr + 1) + 1));
+        const int grid = g.n_rep * L * ((L + Cr - 1) / Cr);
+        float2* A = const_cast<float2*>(G);
+        switch (L) {
+            case 64: ssf_zdft_res_kernel<64><<<grid, 256, smem, st>>>(g, A); break;
+            case 32: ssf_zdft_res_kernel<32><<<grid, 256, smem, st>>>(g, A); break;
+            case 16: ssf_zdft_res_kernel<16><<<grid, 256, smem, st>>>(g, A); break;
+            case 8: ssf_zdft_res_kernel<8><<<grid, 256, smem, st>>>(g, A); break;
+            default: ssf_zdft_res_kernel<0><<<grid, 256, smem, st>>>(g, A);
+        }
+        ssf_accum_res_kernel<<<g.n_rep * L * L * L, 256, 0, st>>>(g, A, o);
+        return;
+    }
     if (ssf_fast_path(g.P, g.Q)) {
         const size_t smem = sizeof(float2) * (size_t(9) * L + 12 * size_t(L) * (C + 1));
         const int grid = g.n_rep * L * n_chunk, threads = ssf_line_threads(L, g.P, g.Q);
@@ -763,14 +884,25 @@ __global__ void __launch_bounds__(256) ssf_adj_xy_kernel(const SsfGeom g, const 
     }
 }
 
+template <bool RES>
+void prepare_plane(int smem_max) {
+    cudaFuncSetAttribute(ssf_plane_kernel<64, true, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<32, true, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<16, true, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<8, false, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<0, true, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<0, false, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+}
+
 void ssf_prepare() {
     const int smem_max = 200 * 1024;
-    cudaFuncSetAttribute(ssf_plane_kernel<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(ssf_plane_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(ssf_plane_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(ssf_plane_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(ssf_plane_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(ssf_plane_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    prepare_plane<false>(smem_max);
+    prepare_plane<true>(smem_max);
+    cudaFuncSetAttribute(ssf_zdft_res_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_zdft_res_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_zdft_res_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_zdft_res_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_zdft_res_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);

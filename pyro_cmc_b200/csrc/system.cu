@@ -192,6 +192,7 @@ struct pc_system {
     int n_slots = 0;
     std::vector<int> L_of_slot;
     int64_t slot_stride = 0;
+    bool ssf_resolved = false;  // sublattice-resolved accumulators [n_corr][n_k][16][16][2]
     DevBuf<double> d_ssf_sum, d_ssf_sq;
     std::vector<uint64_t> ssf_n;
     std::vector<SsfGroup> groups;
@@ -658,6 +659,7 @@ int enqueue_ssf(pc_system* s, const pc::SsfOut& o, bool selected_only) {
         geom.L = g.L;
         geom.P = g.P;
         geom.Q = g.Q;
+        geom.resolved = s->ssf_resolved ? 1 : 0;
         if (selected_only) {
             if (g.n_sel == 0) continue;
             geom.n_rep = g.n_sel;
@@ -706,7 +708,7 @@ int ensure_groups(pc_system* s) {
         PC_CK(g.d_rep_index.alloc(g.reps.size()));
         PC_CK(cudaMemcpy(g.d_rep_index.p, g.reps.data(), sizeof(int32_t) * g.reps.size(), cudaMemcpyHostToDevice));
         const size_t L3 = size_t(g.L) * g.L * g.L;
-        PC_CK(g.d_G.alloc(g.reps.size() * 24 * L3));  // 3 components x 8 half-groups
+        PC_CK(g.d_G.alloc(g.reps.size() * 48 * L3));  // 3 components x 8 half-groups, or x 16 sublattices
     }
     return PC_OK;
 }
@@ -1148,8 +1150,8 @@ int device_error(pc_system* s) {
     PC_CK(cudaStreamSynchronize(s->stream));
     if (!flag) return PC_OK;
     PC_CK(cudaMemsetAsync(s->d_err.p, 0, sizeof(int), s->stream));
-    return fail(PC_ERR_CUDA, "a colour pass stopped waiting for its staged neighbour rows (bounded wait ran out); "
-                             "the updates of that pass were skipped");
+    return fail(PC_ERR_TIMEOUT, "a colour pass stopped waiting for its staged neighbour rows (bounded wait ran out); "
+                                "the updates of that pass were skipped");
 }
 
 int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uint64_t* accepted) {
@@ -1295,7 +1297,11 @@ int pc_ssf_configure(pc_system* sys, const char* const* names, int n_corr, int n
         if (!found) return fail(PC_ERR_INVALID, "slot size matches no replica");
         max_nk = std::max<int64_t>(max_nk, int64_t(L_of_slot[sl]) * L_of_slot[sl] * L_of_slot[sl]);
     }
-    sys->slot_stride = int64_t(n_corr) * max_nk * 2;
+    if (sys->ssf_resolved)
+        for (auto& g : sys->groups)
+            if (g.P > 8 || g.Q > 8)
+                return fail(PC_ERR_UNSUPPORTED, "sublattice-resolved S(q) needs every L to factor into two parts <= 8");
+    sys->slot_stride = int64_t(n_corr) * max_nk * 2 * (sys->ssf_resolved ? 256 : 1);
     PC_CK(sys->d_ssf_sum.alloc(size_t(std::max(1, n_slots)) * size_t(sys->slot_stride)));
     PC_CK(sys->d_ssf_sq.alloc(size_t(std::max(1, n_slots)) * size_t(sys->slot_stride)));
     PC_CK(cudaMemset(sys->d_ssf_sum.p, 0, sizeof(double) * sys->d_ssf_sum.n));
@@ -1303,6 +1309,15 @@ int pc_ssf_configure(pc_system* sys, const char* const* names, int n_corr, int n
     PC_CK(sys->d_slot_of_rep.alloc(size_t(sys->R)));
     sys->ssf_n.assign(size_t(n_slots), 0);
     sys->ssf_ready = true;
+    sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_ssf_set_resolved(pc_system* sys, int resolved) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    sys->ssf_resolved = resolved != 0;
+    sys->ssf_ready = false;  // accumulators change shape: configure again
     sys->drop_graphs();
     return PC_OK;
 }
@@ -1345,7 +1360,7 @@ int pc_ssf_read(pc_system* sys, int slot, double* sum, double* sq, uint64_t* n_s
     if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
     if (slot < 0 || slot >= sys->n_slots) return fail(PC_ERR_INVALID, "slot index out of range");
     const int L = sys->L_of_slot[size_t(slot)];
-    const size_t n = size_t(sys->n_corr) * size_t(L) * L * L * 2;
+    const size_t n = size_t(sys->n_corr) * size_t(L) * L * L * 2 * (sys->ssf_resolved ? 256 : 1);
     PC_CK(cudaStreamSynchronize(sys->stream));
     if (sum)
         PC_CK(cudaMemcpy(sum, sys->d_ssf_sum.p + size_t(slot) * sys->slot_stride, sizeof(double) * n,
@@ -1375,6 +1390,7 @@ int pc_ssf_forward(pc_system* sys, void* out_dev) {
     int rc = check_sys(sys);
     if (rc) return rc;
     if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    if (sys->ssf_resolved) return fail(PC_ERR_UNSUPPORTED, "the differentiable S(q) is the contracted one");
     // out_dev is [R][n_corr][n_k][2] with replicas in index order; the kernel
     // indexes by position inside each size group, so offset per group.
     size_t base = 0;
@@ -1403,6 +1419,7 @@ int pc_ssf_backward(pc_system* sys, const void* grad_out_dev, void* grad_S_dev) 
     int rc = check_sys(sys);
     if (rc) return rc;
     if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    if (sys->ssf_resolved) return fail(PC_ERR_UNSUPPORTED, "the differentiable S(q) is the contracted one");
     PC_CK(cudaMemsetAsync(grad_S_dev, 0, sizeof(float4) * size_t(sys->N_tot), sys->stream));
     for (auto& g : sys->groups) {
         for (size_t i = 0; i < g.reps.size(); ++i)
@@ -1436,7 +1453,7 @@ int pc_ssf_current(pc_system* sys, int replica, double* out) {
     rc = check_rep(sys, replica);
     if (rc) return rc;
     if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
-    const size_t n = size_t(sys->n_corr) * size_t(sys->Nc(replica)) * 2;
+    const size_t n = size_t(sys->n_corr) * size_t(sys->Nc(replica)) * 2 * (sys->ssf_resolved ? 256 : 1);
     DevBuf<double> val;
     PC_CK(val.alloc(n));
     for (auto& g : sys->groups) {
@@ -1444,7 +1461,7 @@ int pc_ssf_current(pc_system* sys, int replica, double* out) {
         DevBuf<int32_t> idx;
         PC_CK(idx.alloc(1));
         PC_CK(cudaMemcpy(idx.p, &replica, sizeof(int32_t), cudaMemcpyHostToDevice));
-        pc::SsfGeom geom{g.L, g.P, g.Q, 1, idx.p};
+        pc::SsfGeom geom{g.L, g.P, g.Q, 1, idx.p, sys->ssf_resolved ? 1 : 0};
         pc::SsfOut o = ssf_out_base(sys);
         o.val = val.p;
         pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, g.d_G.p, sys->stream);
@@ -1751,7 +1768,7 @@ int pc_autotune(pc_system* sys) {
     // SM (the structured kernels run at most 256 threads per CTA)
     // (ctas 0: one CTA per tile, the hardware balancing the waves)
     const int cand_threads[4] = {64, 128, 256, 512};
-    const int cand_ctas[11] = {0, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16};
+    const int cand_ctas[8] = {0, 2, 3, 4, 5, 6, 7, 8};
     int best_t = sys->threads, best_c = sys->ctas_per_sm, best_v = sys->load_variant;
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;
@@ -1762,7 +1779,7 @@ int pc_autotune(pc_system* sys) {
     const int n_var = sys->structured ? 4 : 1;
     for (int vi = 0; vi < n_var; ++vi)
         for (int ti = 0; ti < 4; ++ti)
-            for (int ci = 0; ci < 11; ++ci) {
+            for (int ci = 0; ci < 8; ++ci) {
                 if (sys->structured && cand_threads[ti] > 256) continue;
                 sys->load_variant = vi;
                 sys->threads = cand_threads[ti];
@@ -1772,13 +1789,17 @@ int pc_autotune(pc_system* sys) {
                 if (rc) return rc;
                 rc = run_sweeps(sys, 2, 1);  // warm-up + graph instantiation
                 if (rc) return rc;
-                PC_CK(cudaEventRecord(e0, sys->stream));
-                rc = run_sweeps(sys, 5, 1);
-                if (rc) return rc;
-                PC_CK(cudaEventRecord(e1, sys->stream));
-                PC_CK(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                PC_CK(cudaEventElapsedTime(&ms, e0, e1));
+                float ms = 1e30f;  // best of three repeats: robust against a noisy neighbour
+                for (int rep = 0; rep < 3; ++rep) {
+                    PC_CK(cudaEventRecord(e0, sys->stream));
+                    rc = run_sweeps(sys, 4, 1);
+                    if (rc) return rc;
+                    PC_CK(cudaEventRecord(e1, sys->stream));
+                    PC_CK(cudaEventSynchronize(e1));
+                    float t = 0.f;
+                    PC_CK(cudaEventElapsedTime(&t, e0, e1));
+                    ms = std::min(ms, t);
+                }
                 if (ms < best_ms) {
                     best_ms = ms;
                     best_t = cand_threads[ti];
@@ -1837,7 +1858,7 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
             o.acc_sum = sys->d_ssf_sum.p;
             o.acc_sq = sys->d_ssf_sq.p;
             o.slot_of_rep = sys->d_slot_of_rep.p;
-            pc::SsfGeom geom{grp->L, grp->P, grp->Q, 1, grp->d_rep_index.p};
+            pc::SsfGeom geom{grp->L, grp->P, grp->Q, 1, grp->d_rep_index.p, sys->ssf_resolved ? 1 : 0};
             pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, grp->d_G.p, sys->stream);
             PC_LAUNCH_CK();
             pc::launch_ssf_z(geom, grp->d_G.p, o, sys->stream);

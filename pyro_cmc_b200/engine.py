@@ -282,6 +282,17 @@ class System:
         return h
 
     # ------------------------------------------------------------------ SSF
+    ssf_resolved = False
+
+    def ssf_set_resolved(self, on: bool):
+        """Sublattice-resolved S(q) accumulators [n_corr][n_k][16][16][2]
+        (call before ssf_configure)."""
+        call("pc_ssf_set_resolved", self._h, int(bool(on)))
+        self.ssf_resolved = bool(on)
+
+    def _ssf_shape(self, nk: int):
+        return (self.n_corr, nk, 16, 16, 2) if self.ssf_resolved else (self.n_corr, nk, 2)
+
     def ssf_configure(self, names: Sequence[str], n_slots: int, L_of_slot: Sequence[int] | None = None):
         arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
         if L_of_slot is None:
@@ -297,7 +308,7 @@ class System:
 
     def ssf_read(self, slot: int, L: int | None = None):
         L = L or self.L[0]
-        shape = (self.n_corr, L ** 3, 2)
+        shape = self._ssf_shape(L ** 3)
         s = np.empty(shape)
         q = np.empty(shape)
         n = C.c_uint64(0)
@@ -308,7 +319,7 @@ class System:
         call("pc_ssf_clear", self._h, slot)
 
     def ssf_current(self, replica: int = 0):
-        out = np.empty((self.n_corr, self.Nc(replica), 2))
+        out = np.empty(self._ssf_shape(self.Nc(replica)))
         call("pc_ssf_current", self._h, replica, _dp(out))
         return out
 

@@ -41,6 +41,7 @@ int main(int argc, char* argv[]) {
     prog.flag({"--lifted"}, "Use lifted Metropolis (flip direction on rejection) instead of standard Metropolis");
     prog.option({"--correlators"}, "S(q) correlators", "xx yy zz xy xz yz", false, "+");
     prog.flag({"--dry_run"}, "Print the run name and temperature grid and exit");
+    prog.flag({"--ssf_resolved"}, "Write /ssf sublattice-resolved, [n_corr, n_T, n_k, n_sl, n_sl, 2]");
     provide_physical_args(prog);
     try {
         prog.parse(argc, argv);
@@ -91,6 +92,7 @@ int main(int argc, char* argv[]) {
         const auto file_path = outdir / (name.str() + ".out.npz");
         OutFile file(file_path.string());
         ssf_manager ssfm(lat, prog.strs("--correlators"), file, "/ssf", T_sample, true);
+        if (prog.boolean("--ssf_resolved")) ssfm.set_sublattice_resolved(true);
         const double N = double(lat.num_spins());
 
         // src/anneal.cpp:184-188: --lifted swaps the single-site move

@@ -45,6 +45,13 @@ ssf_manager::ssf_manager(CMC::Lattice& sc, const std::vector<std::string>& corre
     std::sort(T_sorted_.begin(), T_sorted_.end());
 }
 
+void ssf_manager::set_sublattice_resolved(bool on) {
+    if (!T_list.empty()) throw std::logic_error("set_sublattice_resolved: call before the first new_T()");
+    CMC::check(pc_ssf_set_resolved(sc_->device(), on ? 1 : 0));
+    ew_ = on ? 512 : 2;
+    configure(get_corr_labels());
+}
+
 std::vector<std::string> ssf_manager::get_corr_labels() const {
     std::vector<std::string> l;
     for (const auto& c : corr_specs_) l.push_back(c.label);
@@ -64,11 +71,12 @@ void ssf_manager::point_at(CMC::Lattice& sc2) {
     uint64_t n = 0;
     const bool carry = have_current_;
     if (carry) {
-        s.resize(get_n_corr() * size_t(n_kpoints_) * 2);
+        s.resize(get_n_corr() * size_t(n_kpoints_) * ew_);
         q.resize(s.size());
         CMC::check(pc_ssf_read(sc_->device(), 0, s.data(), q.data(), &n));
     }
     sc_ = &sc2;
+    CMC::check(pc_ssf_set_resolved(sc_->device(), ew_ == 512 ? 1 : 0));
     configure(get_corr_labels());
     if (carry) {
         // the accumulators restart on the new device; keep the old sums on the host
@@ -96,7 +104,7 @@ void ssf_manager::sample() {
 
 void ssf_manager::get_flat_buffer(size_t t_idx, std::vector<double>& corr_buf, std::vector<double>& corr_sq_buf) const {
     if (t_idx != curr_idx) throw std::logic_error("get_flat_buffer: t_idx must be the current temperature");
-    const size_t n = get_n_corr() * size_t(n_kpoints_) * 2;
+    const size_t n = get_n_corr() * size_t(n_kpoints_) * ew_;
     corr_buf.assign(n, 0.0);
     corr_sq_buf.assign(n, 0.0);
     uint64_t ns = 0;
@@ -135,12 +143,13 @@ void ssf_manager::write_group(CMC::OutFile& f, const char* group_name) {
     std::iota(ord.begin(), ord.end(), 0);
     std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return T_list[a] < T_list[b]; });
     const size_t n_T_out = streaming_ ? T_sorted_.size() : n_T;
-    std::vector<double> sum(nc * n_T_out * nk * 2, 0.0), sq(sum.size(), 0.0);
+    const size_t ew = ew_;
+    std::vector<double> sum(nc * n_T_out * nk * ew, 0.0), sq(sum.size(), 0.0);
     auto place = [&](size_t slot, const std::vector<double>& s, const std::vector<double>& q) {
         for (size_t c = 0; c < nc; ++c)
-            for (size_t j = 0; j < nk * 2; ++j) {
-                sum[(c * n_T_out + slot) * nk * 2 + j] = s[c * nk * 2 + j];
-                if (!q.empty()) sq[(c * n_T_out + slot) * nk * 2 + j] = q[c * nk * 2 + j];
+            for (size_t j = 0; j < nk * ew; ++j) {
+                sum[(c * n_T_out + slot) * nk * ew + j] = s[c * nk * ew + j];
+                if (!q.empty()) sq[(c * n_T_out + slot) * nk * ew + j] = q[c * nk * ew + j];
             }
     };
     if (streaming_) {
@@ -151,8 +160,10 @@ void ssf_manager::write_group(CMC::OutFile& f, const char* group_name) {
         get_flat_buffer(curr_idx, s, q);
         place(curr_idx, s, q);
     }
-    f.dataset_f64(g + "/static_corr", {nc, n_T_out, nk, 2}, sum.data());
-    if (store_error_term_) f.dataset_f64(g + "/static_corr_2", {nc, n_T_out, nk, 2}, sq.data());
+    const std::vector<uint64_t> shape = ew == 512 ? std::vector<uint64_t>{nc, n_T_out, nk, 16, 16, 2}
+                                                  : std::vector<uint64_t>{nc, n_T_out, nk, 2};
+    f.dataset_f64(g + "/static_corr", shape, sum.data());
+    if (store_error_term_) f.dataset_f64(g + "/static_corr_2", shape, sq.data());
     std::vector<double> sT;
     std::vector<uint64_t> sN;
     for (size_t i : ord) {

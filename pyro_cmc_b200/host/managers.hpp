@@ -114,6 +114,12 @@ public:
     void flush();
     void write_group(CMC::OutFile& f, const char* group_name = "/ssf") override;
 
+    // Keep the sublattice-resolved correlator C_{mu nu}(k) (the layout
+    // [n_corr, n_T, n_k, 16, 16, 2] of the reference's temper output) instead
+    // of the contracted S(q). Call before the first new_T().
+    void set_sublattice_resolved(bool on);
+    bool sublattice_resolved() const { return ew_ == 512; }
+
 private:
     CMC::Lattice* sc_;
     std::vector<CorrSpec> corr_specs_;
@@ -127,6 +133,7 @@ private:
     // flushed temperatures (streaming) : slot -> (sum, sq)
     std::map<size_t, std::pair<std::vector<double>, std::vector<double>>> flushed_;
     bool have_current_ = false;
+    size_t ew_ = 2;  // doubles per (correlator, k): 2, or 16*16*2 resolved
 
     void configure(const std::vector<std::string>& names);
     void on_new_temp() override;

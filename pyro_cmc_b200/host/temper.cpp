@@ -9,8 +9,9 @@
 //    (temper.cpp:418-474); the reference's extra sweep on non-sampled ranks
 //    (:426-429), a load-balancing device, is not reproduced;
 //  * /ssf holds the rungs of --T_sample in the contracted layout
-//    [n_corr, n_T, n_k, 2] that ssf_manager produces (the reference's
-//    temper writes a stale 6-D layout sized for sublattice-resolved data);
+//    [n_corr, n_T, n_k, 2] that ssf_manager produces, or with --ssf_resolved
+//    the sublattice-resolved layout [n_corr, n_T, n_k, 16, 16, 2] that the
+//    reference's write_ssf_group (temper.cpp:121-159) is written for;
 //  * output is <name>.out.npz; --seed is the Philox key.
 #include <algorithm>
 #include <cstdio>
@@ -31,6 +32,7 @@ int main(int argc, char* argv[]) {
     prog.option({"--n_replicas"}, "Number of replicas (rungs), one per temperature", "", true);
     prog.flag({"--save_state"}, "Save the spin state of the coldest replica");
     prog.flag({"--init_uniform"}, "Start from spins uniform on the sphere (device Philox) instead of zero");
+    prog.flag({"--ssf_resolved"}, "Write /ssf sublattice-resolved, [n_corr, n_T, n_k, n_sl, n_sl, 2]");
     prog.option({"--T_hot"}, "Temperature of the hottest replica");
     prog.option({"--T_cold"}, "Temperature of the coldest replica (defaults to min(T_sample))");
     prog.option({"--T_ref"}, "Reference temperature for proposal distribution", "1.0");
@@ -89,6 +91,9 @@ int main(int argc, char* argv[]) {
         if (prog.boolean("--init_uniform")) check(pc_random_spins(sys, seed ^ 0x5eedULL));
         const char* corr[3] = {"xx", "yy", "zz"};
         std::vector<int32_t> L_of_slot(size_t(R), L);
+        const bool resolved = prog.boolean("--ssf_resolved");
+        const size_t ew = resolved ? 512 : 2;  // doubles per (correlator, k)
+        check(pc_ssf_set_resolved(sys, resolved ? 1 : 0));
         check(pc_ssf_configure(sys, corr, 3, R, L_of_slot.data()));
 
         std::printf("[temper] Burning in %d replicas (%d sweeps each)...\n", R, n_burn_in);
@@ -129,22 +134,24 @@ int main(int argc, char* argv[]) {
         std::vector<size_t> rungs(S_idx.begin(), S_idx.end());
         std::sort(rungs.begin(), rungs.end(), [&](size_t a, size_t b) { return T_grid[a] < T_grid[b]; });
         const size_t nk = size_t(L) * L * L, nT = rungs.size();
-        std::vector<double> sum(3 * nT * nk * 2), sq(sum.size()), st;
+        std::vector<double> sum(3 * nT * nk * ew), sq(sum.size()), st;
         std::vector<uint64_t> sn;
         for (size_t t = 0; t < nT; ++t) {
-            std::vector<double> s(3 * nk * 2), q(3 * nk * 2);
+            std::vector<double> s(3 * nk * ew), q(3 * nk * ew);
             uint64_t n = 0;
             check(pc_ssf_read(sys, int(rungs[t]), s.data(), q.data(), &n));
             for (size_t c = 0; c < 3; ++c)
-                for (size_t j = 0; j < nk * 2; ++j) {
-                    sum[(c * nT + t) * nk * 2 + j] = s[c * nk * 2 + j];
-                    sq[(c * nT + t) * nk * 2 + j] = q[c * nk * 2 + j];
+                for (size_t j = 0; j < nk * ew; ++j) {
+                    sum[(c * nT + t) * nk * ew + j] = s[c * nk * ew + j];
+                    sq[(c * nT + t) * nk * ew + j] = q[c * nk * ew + j];
                 }
             st.push_back(T_grid[rungs[t]]);
             sn.push_back(n);
         }
-        file.dataset_f64("/ssf/static_corr", {3, nT, nk, 2}, sum.data());
-        file.dataset_f64("/ssf/static_corr_2", {3, nT, nk, 2}, sq.data());
+        const std::vector<uint64_t> shape =
+            resolved ? std::vector<uint64_t>{3, nT, nk, 16, 16, 2} : std::vector<uint64_t>{3, nT, nk, 2};
+        file.dataset_f64("/ssf/static_corr", shape, sum.data());
+        file.dataset_f64("/ssf/static_corr_2", shape, sq.data());
         file.dataset_f64("/ssf/T_list", {nT}, st.data());
         file.dataset_u64("/ssf/n_samples", {nT}, sn.data());
         file.dataset_strings("/ssf/corr_lookup", {"xx", "yy", "zz"});

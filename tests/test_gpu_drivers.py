@@ -95,3 +95,35 @@ def test_fieldcool_driver(tmp_path):
         assert len(f["/energy/T_list"]) == 8
         assert list(f["/ssf/n_samples"]) == [3]
         assert f["/ssf/static_corr"].shape == (3, 1, 8, 2)
+
+
+def test_resolved_ssf_from_the_drivers(tmp_path):
+    """anneal and temper with --ssf_resolved: /ssf/static_corr in the
+    sublattice-resolved layout [n_corr, n_T, n_k, 16, 16, 2] (src/temper.cpp:121-159),
+    whose phase contraction is the contracted S(q) of the same run."""
+    from oracle import ssf_fft
+    base = ["-s", 5, 2, "--J1", 1, "--T_sample", 0.5, "--n_steps", 4, "--n_sweep", 2, "--n_burn_in", 2,
+            "--n_sample", 2, "--init_uniform", "--correlators", "xx", "xy"]
+    outs = {}
+    for tag, extra in (("c", []), ("r", ["--ssf_resolved"])):
+        d = tmp_path / tag
+        d.mkdir()
+        run("anneal", "-o", d, *base, *extra)
+        with File(only(d, ".out.npz")) as f:
+            outs[tag] = f["/ssf/static_corr"][:]
+    c, r = outs["c"], outs["r"]
+    assert c.shape == (2, 1, 8, 2) and r.shape == (2, 1, 8, 16, 16, 2)
+    L = 2
+    K = np.stack(np.meshgrid(np.arange(L), np.arange(L), np.arange(L), indexing="ij"), -1).reshape(-1, 3)
+    dr = ssf_fft.R_SL[:, None, :] - ssf_fft.R_SL[None, :, :]
+    ph = np.exp(1j * 2 * np.pi * np.einsum("kd,mnd->kmn", K, dr) / (8 * L))
+    Sq = np.einsum("ctkmn,kmn->ctk", r[..., 0] + 1j * r[..., 1], ph)
+    np.testing.assert_allclose(Sq.real, c[..., 0], atol=1e-6 * np.abs(c).max())
+    np.testing.assert_allclose(Sq.imag, c[..., 1], atol=1e-6 * np.abs(c).max())
+    d = tmp_path / "t"
+    d.mkdir()
+    run("temper", "-o", d, "-s", 3, "--n_replicas", 4, 2, "--J1", 1, "--T_sample", 0.3, "--n_sweep", 2,
+        "--n_burn_in", 2, "--n_sample", 3, "--init_uniform", "--ssf_resolved")
+    with File(only(d, ".out.npz")) as f:
+        assert f["/ssf/static_corr"].shape == (3, 1, 8, 16, 16, 2)
+        assert (f["/ssf/static_corr_2"][..., 0] >= 0).all()

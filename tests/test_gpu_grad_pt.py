@@ -284,3 +284,48 @@ def test_ssf_backward_large_L_matches_fft_adjoint(L):
     ref = ssf_fft.adjoint(g.spins(), L, corr, D[0])
     scale = np.abs(ref).max()
     assert np.abs(got - ref).max() <= 1e-5 * scale * max(1.0, np.log2(nk)), np.abs(got - ref).max() / scale
+
+
+def _lt_matrix(L, K, J1, J2, J3, Delta):
+    """The oracle's LT matrix M(k) (oracle/lt.py bonds) at one K, numpy."""
+    import oracle.lt as olt
+    sysd = oracle.System(1, J1=1.0, J2=1.0, J3=1.0, j1_mode=1)
+    tables = {k: [sysd.spec_displacements(spec, p) for p in range(4)] for k, spec in
+              (("J1", 0), ("J2", 1), ("J3a", 2), ("J3b", 3))}
+    r = np.array([olt.LINK[s % 4] + olt.FCC[s // 4] for s in range(16)])
+    rmod = {tuple(x % 8): s for s, x in enumerate(r)}
+    z = olt.LINK / np.sqrt(3.0)
+    k = 2 * np.pi * np.asarray(K) / (8.0 * L)
+    Mk = np.zeros((48, 48), complex)
+    for name, j in (("J1", J1), ("J2", J2), ("J3a", J3), ("J3b", J3)):
+        if j == 0.0:
+            continue
+        for a in range(16):
+            for d in tables[name][a % 4]:
+                b = rmod[tuple((r[a] + d) % 8)]
+                M = j * (np.eye(3) + (Delta - 1.0) * np.outer(z[a % 4], z[b % 4])) if name == "J1" else j * np.eye(3)
+                Mk[3 * a:3 * a + 3, 3 * b:3 * b + 3] += M * np.exp(1j * (k @ np.asarray(d, float)))
+    return Mk
+
+
+@pytest.mark.parametrize("L,J", [(2, (1.0, 0.0, 0.0, 1.0)), (3, (1.0, 0.1, -0.05, 0.5)),
+                                 (4, (-0.7, 0.3, 0.02, 1.3)), (4, (1.0, -0.1, 0.05, 1.0))])
+def test_lt_on_gpu_matches_oracle(L, J):
+    """pc_lt_minimum against the numpy restatement of src/luttinger_tisza.cpp:
+    the eigenvalue map at every k (FP64 eigvalsh), E_min and k*, and the
+    eigenvector (M v = lambda v, unit norm)."""
+    import oracle.lt as olt
+    from pyro_cmc_b200.lt import lt_minimum
+    J1, J2, J3, D = J
+    res = lt_minimum(L, J1, J2, J3, D)
+    e_ref, k_ref = olt.lt_minimum(L, J1, J2, J3, D)
+    assert abs(res["E_min"] - e_ref) <= 1e-9 * max(1.0, abs(e_ref))
+    lam = res["eigenvalue_map"]
+    for K in [(0, 0, 0), tuple(res["k_star_idx"]), (1, 0, L - 1), (L - 1, L // 2, 1)]:
+        Mk = _lt_matrix(L, K, J1, J2, J3, D)
+        assert abs(lam[K] - np.linalg.eigvalsh(Mk)[0]) <= 1e-9 * max(1.0, np.abs(Mk).max())
+    assert abs(lam[tuple(k_ref)] - 2 * e_ref) <= 1e-9 * max(1.0, abs(e_ref))
+    v = res["eigenvector"]
+    Mk = _lt_matrix(L, tuple(res["k_star_idx"]), J1, J2, J3, D)
+    assert abs(np.linalg.norm(v) - 1.0) < 1e-9
+    assert np.linalg.norm(Mk @ v - 2 * res["E_min"] * v) <= 1e-6 * max(1.0, np.abs(Mk).max())

@@ -405,3 +405,51 @@ def test_nonstructural_coupling_uses_generic_path():
     assert g.structured()
     g.set_coupling_matrix(6, [[0.1, 0.05, 0.0], [0.0, 0.1, 0.0], [0.0, 0.0, 0.1]])
     assert not g.structured()
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 4])
+def test_ssf_resolved_matches_oracle_correlate(L):
+    """The sublattice-resolved correlator (ssf_manager's correlate() output)
+    against the oracle's per-sublattice DFT, 9 correlators, random spins."""
+    g, o = pair(L, COUPLINGS[0])
+    g.ssf_set_resolved(True)
+    g.ssf_configure(CORR9, 1)
+    rng = np.random.default_rng(L + 40)
+    g.set_spins(unit(rng, o.N))
+    o.set_spins(g.spins())
+    got = g.ssf_current()
+    _, ref = o.ssf(CORR9, mode=1, resolved=True)
+    scale = max(np.abs(ref).max(), 1.0)
+    assert got.shape == ref.shape
+    assert np.abs(got - ref).max() <= REL * scale * 10, np.abs(got - ref).max() / scale
+
+
+@pytest.mark.parametrize("L", [6, 8, 16])
+def test_ssf_resolved_contracts_to_ssf(L):
+    """Contracting the resolved correlator with exp(+i q.(r_mu - r_nu)) gives
+    S(q) (include/ssf_manager.hpp:275-280); accumulation in slots as
+    ssf_manager does (two samples)."""
+    from oracle import ssf_fft
+    corr = ["xx", "zz", "xy", "yz"]
+    g = pc.pyrochlore_system(L, **COUPLINGS[0])
+    g.ssf_set_resolved(True)
+    g.ssf_configure(corr, 2)
+    refs = []
+    for k in range(2):
+        g.random_spins(100 + k)
+        refs.append(ssf_fft.ssf(g.spins(), L, corr))
+        g.ssf_sample([1])
+    s, q, n = g.ssf_read(1)
+    assert n == 2 and s.shape == (len(corr), L ** 3, 16, 16, 2)
+    K = np.stack(np.meshgrid(np.arange(L), np.arange(L), np.arange(L), indexing="ij"), -1).reshape(-1, 3)
+    dr = ssf_fft.R_SL[:, None, :] - ssf_fft.R_SL[None, :, :]  # [mu][nu][3]
+    ph = np.exp(1j * 2 * np.pi * np.einsum("kd,mnd->kmn", K, dr) / (8 * L))
+    C = s[..., 0] + 1j * s[..., 1]
+    Sq = np.einsum("ckmn,kmn->ck", C, ph)
+    ref = refs[0] + refs[1]
+    scale = np.abs(ref).max()
+    assert np.abs(Sq.real - ref[..., 0]).max() <= 1e-5 * scale
+    assert np.abs(Sq.imag - ref[..., 1]).max() <= 1e-5 * scale
+    assert (q[..., 0] >= 0).all() and (q[..., 1] >= 0).all()
+    with pytest.raises(pc.PyroCMCError):
+        g.ssf_forward_device(0)  # the differentiable S(q) is the contracted one
