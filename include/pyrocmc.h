@@ -112,7 +112,8 @@ int pc_set_sweep_schedule(pc_system* sys, int schedule);
  * form (local_lifted_Metropolis_rot, src/MC.cpp:194-244;
  * sweep_lifted_Metropolis_rot :293-302). The per-spin lifting direction
  * (include/MC.hpp:57) is the sign of the spin's fourth float4 component
- * (>= 0: +1); pc_set_spins resets it to +1. Lifted sweeps visit the classes in
+ * (>= 0: +1); lifted passes and overrelaxation passes keep it, while
+ * pc_set_spins and a Metropolis (non-lifted) pass reset it to +1. Lifted sweeps visit the classes in
  * the reference's order (a lifted pass, then the overrelaxation passes), for
  * either sweep schedule. */
 int pc_set_update(pc_system* sys, int mode);
@@ -208,6 +209,16 @@ int pc_ssf_configure(pc_system* sys, const char* const* names, int n_corr, int n
  * reads (pc_ssf_read, pc_ssf_current) then return the resolved layout.
  * Needs every L to factor into two parts <= 8 (L <= 64). */
 int pc_ssf_set_resolved(pc_system* sys, int resolved);
+/* Seed merge (scripts/acc_runs.py:228-370, merge_group) of K slots that hold
+ * the same temperature for K seeds with the same sample count n, computed on
+ * the device: static_corr = sum of the slots' S(q) sums, static_corr_2 = sum
+ * of their squares, var_inter = static_corr_2/(K n^2) - (static_corr/(K n))^2,
+ * var_intra = sum of the slots' square sums / n - static_corr_2 / n^2, each
+ * [n_corr][n_k][2]; and per seed the spiral-plane invariants of
+ * plane_invariants (:103-167) w, chi_frac and tr, each [K][n_k] (need the
+ * correlators xx, yy, zz, xy, xz, yz). Every output may be null. */
+int pc_ssf_merge(pc_system* sys, const int32_t* slots, int K, double* static_corr, double* static_corr_2,
+                 double* var_inter, double* var_intra, double* w, double* chi_frac, double* tr);
 /* ssf_manager::sample (include/ssf_manager.hpp:260-293) for every replica r
  * with slot_of_replica[r] >= 0 (host array): accumulates S(q) and
  * (Re S)^2, (Im S)^2 into that slot in FP64 and counts the sample. */

@@ -46,6 +46,7 @@ _SIGNATURES = {
     "pc_set_update": (_I, [_P, _I]),
     "pc_ssf_set_resolved": (_I, [_P, _I]),
     "pc_lt_minimum": (_I, [_I, _D, _D, _D, _D, _DP, _DP, _I64P, _DP]),
+    "pc_ssf_merge": (_I, [_P, _I32P, _I, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "pc_kernel_path": (_I, [_P, _IP]),
     "pc_setup_lattice": (_I, [_P]),
     "pc_num_replicas": (_I, [_P, _IP]),

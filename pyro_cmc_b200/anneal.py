@@ -45,13 +45,18 @@ def anneal_batch(K: int, L: int, J1: float, J2: float = 0.0, J3: float = 0.0, B=
                  Delta: float = 1.0, T_hot: float = 10.0, T_cold: float | None = None, T_sample=(0.1,),
                  n_steps: int = 100, n_sweep: int = 16, n_burn_in: int = 16, n_sample: int = 64,
                  corr=("xx", "yy", "zz", "xy", "xz", "yz"), T_ref: float = 1.0, seed: int = 0,
-                 init_seed: int | None = None, schedule: int = 0, update: int = 0):
+                 init_seed: int | None = None, schedule: int = 0, update: int = 0, merge: bool = False):
     """The anneal protocol for K seeds at once: burn-in at T_hot, then for each
     T of the profile n_sweep sweeps and one energy sample; at the sample
     temperatures, n_sample x (n_sweep sweeps + one S(q) sample).
     Returns dict(T, sample_idx, e[K, n_T], ssf_sum/ssf_sq[K, n_Ts, n_corr, n_k, 2],
     n_ssf[n_Ts], accepted[K, n_T]); S(q) slots in visit (descending T) order.
-    update 1: lifted Metropolis (src/anneal.cpp:184-188, --lifted)."""
+    update 1: lifted Metropolis (src/anneal.cpp:184-188, --lifted).
+    merge: also the seed merge of scripts/acc_runs.py over the K seeds,
+    result["merged"] = dict(energy=..., ssf=[per T_sample dict]) with the S(q)
+    part (sums, second moments, inter/intra-seed variances, spiral-plane
+    invariants when the six correlators xx..yz are sampled) computed on the
+    device (pc_ssf_merge)."""
     T_sample = list(T_sample)
     if T_cold is None:
         T_cold = min(T_sample)
@@ -75,6 +80,14 @@ def anneal_batch(K: int, L: int, J1: float, J2: float = 0.0, J3: float = 0.0, B=
                 s.ssf_sample(slots)
             slot += 1
     nk = L ** 3
+    merged = None
+    if merge:
+        six = {"xx", "yy", "zz", "xy", "xz", "yz"}.issubset(set(corr))
+        e_cnt = np.ones_like(e)
+        merged = dict(energy=dict(T_list=np.array(T_grid), E=e.sum(axis=0), E2=(e ** 2).sum(axis=0),
+                                  n_samples=e_cnt.sum(axis=0), e_mean=e.mean(axis=0),
+                                  e2_mean=(e ** 2).mean(axis=0), var=(e ** 2).mean(axis=0) - e.mean(axis=0) ** 2),
+                      ssf=[s.ssf_merge(np.arange(K) + t * K, planes=six) for t in range(nTs)])
     ssum = np.zeros((K, nTs, len(corr), nk, 2))
     ssq = np.zeros_like(ssum)
     n_ssf = np.zeros(nTs, dtype=np.uint64)
@@ -85,7 +98,10 @@ def anneal_batch(K: int, L: int, J1: float, J2: float = 0.0, J3: float = 0.0, B=
             ssq[r, t] = b
             n_ssf[t] = n
     s.close()
-    return dict(T=np.array(T_grid), sample_idx=S_idx, e=e, ssf_sum=ssum, ssf_sq=ssq, n_ssf=n_ssf, accepted=acc)
+    out = dict(T=np.array(T_grid), sample_idx=S_idx, e=e, ssf_sum=ssum, ssf_sq=ssq, n_ssf=n_ssf, accepted=acc)
+    if merged is not None:
+        out["merged"] = merged
+    return out
 
 
 def temper(L_list, T, J1: float, J2: float = 0.0, J3: float = 0.0, B=(0.0, 0.0, 0.0), Delta: float = 1.0,

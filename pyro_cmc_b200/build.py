@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpyrocmc.so")
-SOURCES = ["system.cu", "sweep.cu", "ssf.cu", "pt.cu", "noalloc.cu", "lt.cu"]
+SOURCES = ["system.cu", "sweep.cu", "ssf.cu", "pt.cu", "noalloc.cu", "lt.cu", "merge.cu"]
 HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh", "struct_field.cuh"]
 
 NVCC_FLAGS = [
@@ -50,7 +50,7 @@ HOST = os.path.join(HERE, "host")
 BIN = os.path.join(HERE, "bin")
 HOST_LIB_SOURCES = ["MC.cpp", "managers.cpp", "h5out.cpp"]
 HOST_HEADERS = ["MC.hpp", "managers.hpp", "h5out.hpp", "cli_bits.hpp", "vec3.hpp"]
-DRIVERS = ["anneal", "fieldcool", "temper", "spiral_byhand"]
+DRIVERS = ["anneal", "fieldcool", "temper", "spiral_byhand", "ltgs"]
 
 
 def build_host(force: bool = False, verbose: bool = False) -> None:

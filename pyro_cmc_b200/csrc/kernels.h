@@ -157,4 +157,25 @@ struct PtArgs {
 };
 void launch_pt_exchange(const PtArgs& a, cudaStream_t st);
 
+// Seed merge of S(q) accumulators and spiral-plane invariants (merge.cu).
+struct MergeArgs {
+    const double* sum;   // [slot][n_corr][n_k][2]
+    const double* sq;
+    int64_t slot_stride;
+    const int32_t* slots;  // K slot indices (device)
+    int K, n_corr, n_k;
+    double n;              // samples per seed
+    int ix[6];             // correlator index of xx, yy, zz, xy, xz, yz, or -1
+    double* out_corr;      // [n_corr][n_k][2]
+    double* out_corr2;
+    double* out_var_inter;
+    double* out_var_intra;
+    double* w;             // [K][n_k] (plane invariants; null: skipped)
+    double* chi;
+    double* tr;
+    unsigned long long* max_bits;  // [K][2]: bits of max_k I2^{3/2}, max_k tr (non-negative doubles)
+};
+
+void launch_ssf_merge(const MergeArgs& a, cudaStream_t st);
+
 }  // namespace pc

@@ -186,6 +186,14 @@ __device__ __forceinline__ bool lifted_spin(const PassArgs& a, float4 s0, float3
     return false;
 }
 
+// The w component a pass writes: the lifting direction survives overrelaxation
+// and lifted passes (the passes of a lifted sweep); a standard Metropolis or
+// fused pass writes 0, resetting it to +1.
+template <int MODE>
+__device__ __forceinline__ float w_after(float w) {
+    return (MODE == kMetropolis || MODE == kFusedRotate || MODE == kFusedReflect) ? 0.f : w;
+}
+
 // The move at site i with local field h (global field not yet subtracted).
 // Returns whether a Metropolis proposal was accepted.
 template <int MODE>
@@ -202,8 +210,9 @@ __device__ __forceinline__ bool apply_move(const PassArgs& a, float4* S, size_t 
     }
     bool acc = false;
     float4 s1 = s0;
+    s1.w = w_after<MODE>(s0.w);
     if (MODE == kMetropolis || MODE == kFusedRotate || MODE == kFusedReflect)
-        acc = metropolis_spin(a, s0, h, r, sweep, i, s1);
+        acc = metropolis_spin(a, s1, h, r, sweep, i, s1);
     if (MODE == kMetropolis) {
         if (acc) S[i] = s1;
         return acc;
@@ -349,6 +358,7 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
         sincosf(float(a.theta[i]), &sn, &cs);
     }
     float4 s1 = s0;
+    s1.w = w_after<MODE>(s0.w);
     float nx = 0.f, ny = 0.f, nz = 0.f, u = 0.f;
     if (kMet) {
         const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
@@ -379,7 +389,7 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
     if (kMet) {
         const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
         if (dE < 0.f || u < __expf(-dE * invT)) {
-            s1 = make_float4(nx, ny, nz, s0.w);
+            s1 = make_float4(nx, ny, nz, w_after<MODE>(s0.w));
             acc = true;
         }
         if (MODE == kMetropolis) {
@@ -637,10 +647,11 @@ __device__ __forceinline__ unsigned staged_tile(const PassArgs& a, const Tile ti
     }
     bool acc = false;
     float4 s1 = s0;
+    s1.w = w_after<MODE>(s0.w);
     if (kMet) {
         const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
         if (dE < 0.f || u < __expf(-dE * invT)) {
-            s1 = make_float4(nx, ny, nz, s0.w);
+            s1 = make_float4(nx, ny, nz, w_after<MODE>(s0.w));
             acc = true;
         }
         if (MODE == kMetropolis) {

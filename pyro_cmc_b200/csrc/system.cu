@@ -1313,6 +1313,76 @@ int pc_ssf_configure(pc_system* sys, const char* const* names, int n_corr, int n
     return PC_OK;
 }
 
+int pc_ssf_merge(pc_system* sys, const int32_t* slots, int K, double* static_corr, double* static_corr_2,
+                 double* var_inter, double* var_intra, double* w, double* chi_frac, double* tr) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    if (sys->ssf_resolved) return fail(PC_ERR_UNSUPPORTED, "seed merge works on the contracted S(q)");
+    if (K < 1 || !slots) return fail(PC_ERR_INVALID, "need at least one slot");
+    const int L = sys->L_of_slot[size_t(slots[0])];
+    uint64_t n = 0;
+    for (int s = 0; s < K; ++s) {
+        if (slots[s] < 0 || slots[s] >= sys->n_slots) return fail(PC_ERR_INVALID, "slot index out of range");
+        if (sys->L_of_slot[size_t(slots[s])] != L) return fail(PC_ERR_INVALID, "slots differ in lattice size");
+        const uint64_t ns = sys->ssf_n[size_t(slots[s])];
+        if (s == 0) n = ns;
+        if (ns != n) return fail(PC_ERR_INVALID, "seeds differ in their sample counts (the merge assumes one count)");
+    }
+    if (n == 0) return fail(PC_ERR_STATE, "no samples in the slots");
+    pc::MergeArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.sum = sys->d_ssf_sum.p;
+    a.sq = sys->d_ssf_sq.p;
+    a.slot_stride = sys->slot_stride;
+    a.K = K;
+    a.n_corr = sys->n_corr;
+    a.n_k = L * L * L;
+    a.n = double(n);
+    const int want[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    bool have_all = true;
+    for (int q = 0; q < 6; ++q) {
+        a.ix[q] = -1;
+        for (int c = 0; c < sys->n_corr; ++c)
+            if (sys->corr_a[c] == want[q][0] && sys->corr_b[c] == want[q][1]) a.ix[q] = c;
+        have_all = have_all && a.ix[q] >= 0;
+    }
+    const bool planes = w || chi_frac || tr;
+    if (planes && !have_all)
+        return fail(PC_ERR_INVALID, "plane invariants need the correlators xx, yy, zz, xy, xz, yz");
+    const size_t nv = size_t(a.n_corr) * size_t(a.n_k) * 2, np = size_t(K) * size_t(a.n_k);
+    DevBuf<int32_t> d_slots;
+    DevBuf<double> d_out;
+    DevBuf<unsigned long long> d_max;
+    PC_CK(d_slots.alloc(size_t(K)));
+    PC_CK(d_out.alloc(4 * nv + (planes ? 3 * np : 0)));
+    PC_CK(d_max.alloc(size_t(2 * K)));
+    PC_CK(cudaMemcpyAsync(d_slots.p, slots, sizeof(int32_t) * size_t(K), cudaMemcpyHostToDevice, sys->stream));
+    PC_CK(cudaMemsetAsync(d_max.p, 0, sizeof(unsigned long long) * size_t(2 * K), sys->stream));
+    a.slots = d_slots.p;
+    a.out_corr = d_out.p;
+    a.out_corr2 = d_out.p + nv;
+    a.out_var_inter = d_out.p + 2 * nv;
+    a.out_var_intra = d_out.p + 3 * nv;
+    if (planes) {
+        a.w = d_out.p + 4 * nv;
+        a.chi = a.w + np;
+        a.tr = a.chi + np;
+        a.max_bits = d_max.p;
+    }
+    pc::launch_ssf_merge(a, sys->stream);
+    PC_LAUNCH_CK();
+    sys->launches += planes ? 3 : 1;
+    double* outs[7] = {static_corr, static_corr_2, var_inter, var_intra, w, chi_frac, tr};
+    const double* src[7] = {a.out_corr, a.out_corr2, a.out_var_inter, a.out_var_intra, a.w, a.chi, a.tr};
+    const size_t cnt[7] = {nv, nv, nv, nv, np, np, np};
+    for (int i = 0; i < 7; ++i)
+        if (outs[i] && src[i])
+            PC_CK(cudaMemcpyAsync(outs[i], src[i], sizeof(double) * cnt[i], cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    return PC_OK;
+}
+
 int pc_ssf_set_resolved(pc_system* sys, int resolved) {
     int rc = check_sys(sys, false);
     if (rc) return rc;

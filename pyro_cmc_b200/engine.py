@@ -299,6 +299,7 @@ class System:
             L_of_slot = [self.L[0]] * n_slots
         Ls = _c(L_of_slot, np.int32)
         call("pc_ssf_configure", self._h, arr, len(names), int(n_slots), Ls.ctypes.data_as(_I32P))
+        self._L_of_slot = [int(x) for x in L_of_slot]
         self.n_corr = len(names)
         self.corr_names = list(names)
 
@@ -314,6 +315,25 @@ class System:
         n = C.c_uint64(0)
         call("pc_ssf_read", self._h, slot, _dp(s), _dp(q), C.byref(n))
         return s, q, n.value
+
+    def ssf_merge(self, slots, planes: bool = True):
+        """Seed merge of the given slots on the device (scripts/acc_runs.py
+        merge_group and plane_invariants): dict of static_corr,
+        static_corr_2, var_inter, var_intra [n_corr, n_k, 2] and, with
+        planes, w, chi_frac, tr [K, n_k]."""
+        sl = _c(slots, np.int32)
+        K = len(sl)
+        nk = self.L_of_slot_hint(int(sl[0])) ** 3
+        out = {k: np.empty((self.n_corr, nk, 2)) for k in ("static_corr", "static_corr_2", "var_inter", "var_intra")}
+        if planes:
+            out.update({k: np.empty((K, nk)) for k in ("w", "chi_frac", "tr")})
+        P = lambda k: _dp(out[k]) if k in out else None
+        call("pc_ssf_merge", self._h, sl.ctypes.data_as(_I32P), K, P("static_corr"), P("static_corr_2"),
+             P("var_inter"), P("var_intra"), P("w"), P("chi_frac"), P("tr"))
+        return out
+
+    def L_of_slot_hint(self, slot: int) -> int:
+        return self._L_of_slot[slot] if getattr(self, "_L_of_slot", None) else self.L[0]
 
     def ssf_clear(self, slot: int):
         call("pc_ssf_clear", self._h, slot)

@@ -127,3 +127,21 @@ def test_resolved_ssf_from_the_drivers(tmp_path):
     with File(only(d, ".out.npz")) as f:
         assert f["/ssf/static_corr"].shape == (3, 1, 8, 16, 16, 2)
         assert (f["/ssf/static_corr_2"][..., 0] >= 0).all()
+
+
+def test_ltgs_driver(tmp_path):
+    """ltgs (src/luttinger_tisza.cpp) with the k sweep on the GPU: printed lines,
+    output tree, and E_min / k* against the oracle's numpy restatement."""
+    import oracle.lt as olt
+    out = run("ltgs", "-o", tmp_path, 3, "--J1", 1, "--J2", 0.1, "--J3", -0.05, "--Delta", 0.5)
+    assert "LT minimum:" in out and "k*  idx" in out and "Saved to" in out
+    e_ref, k_ref = olt.lt_minimum(3, 1.0, 0.1, -0.05, 0.5)
+    with File(only(tmp_path, "ltgs.out.npz")) as f:
+        assert abs(float(f["/E_min"]) - e_ref) <= 1e-9
+        lam = f["/eigenvalue_map"][:]
+        assert lam.shape == (27,) and abs(lam.min() - 2 * e_ref) <= 1e-9
+        assert tuple(f["/k_star_idx"][:]) == tuple(k_ref)
+        assert f["/eigenvector"].shape == (48, 2)
+        np.testing.assert_allclose(f["/k_star_vec"][:], 2 * np.pi * np.array(k_ref) / 24.0)
+        assert (f["/geometry/index_cell"] == 24 * np.eye(3)).all()
+        assert list(f.attrs["k_dims"]) == [3, 3, 3]

@@ -329,3 +329,31 @@ def test_lt_on_gpu_matches_oracle(L, J):
     Mk = _lt_matrix(L, tuple(res["k_star_idx"]), J1, J2, J3, D)
     assert abs(np.linalg.norm(v) - 1.0) < 1e-9
     assert np.linalg.norm(Mk @ v - 2 * res["E_min"] * v) <= 1e-6 * max(1.0, np.abs(Mk).max())
+
+
+def test_seed_merge_on_device_matches_acc_runs():
+    """anneal_batch(merge=True): the device merge of K seeds (pc_ssf_merge)
+    against the restatement of scripts/acc_runs.py (pinned on the reference's
+    own outputs) applied to the per-seed accumulators."""
+    from oracle import merge as om
+    from pyro_cmc_b200.anneal import anneal_batch
+    corr = ["xx", "yy", "zz", "xy", "xz", "yz"]
+    K = 4
+    r = anneal_batch(K=K, L=3, J1=1.0, J2=-0.1, J3=0.05, T_hot=5.0, T_sample=[0.3, 0.1], n_steps=6, n_sweep=3,
+                     n_burn_in=3, n_sample=5, corr=corr, seed=8, merge=True)
+    # per-seed arrays in acc_runs layout: [K, n_corr, n_T, n_k, 2]
+    sc = np.transpose(r["ssf_sum"], (0, 2, 1, 3, 4))
+    sc2 = np.transpose(r["ssf_sq"], (0, 2, 1, 3, 4))
+    n = np.tile(r["n_ssf"].astype(float), (K, 1))
+    ref = om.merge_ssf(sc, sc2, n)
+    for t, m in enumerate(r["merged"]["ssf"]):
+        for k in ("static_corr", "static_corr_2", "var_inter", "var_intra"):
+            a, b = m[k], ref[k][:, t]
+            assert np.abs(a - b).max() <= 1e-12 * max(1.0, np.abs(b).max()), k
+        for s in range(K):
+            p = om.plane_invariants(sc[s][:, t:t + 1], n[s][t:t + 1], corr)
+            np.testing.assert_allclose(m["w"][s], p["w"][0], atol=1e-9)
+            np.testing.assert_allclose(m["chi_frac"][s], p["chi_frac"][0], atol=1e-9)
+            np.testing.assert_allclose(m["tr"][s], p["tr"][0], rtol=1e-12, atol=1e-9)
+    e = om.merge_energy(r["e"], r["e"] ** 2, np.ones_like(r["e"]))
+    np.testing.assert_allclose(r["merged"]["energy"]["var"], e["var"], rtol=1e-12, atol=1e-12)

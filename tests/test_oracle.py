@@ -290,3 +290,23 @@ def test_ssf_fft_adjoint_matches_finite_differences():
         Sm[i, a] -= h
         fd = (loss(Sp) - loss(Sm)) / (2 * h)
         assert abs(fd - g[i, a]) <= 1e-6 * max(1.0, abs(fd)), (i, a, fd, g[i, a])
+
+
+def test_merge_restatement_matches_reference_acc_runs():
+    """oracle/merge.py against the outputs of the reference's own
+    scripts/acc_runs.py merge_group and plane_invariants
+    (tests/golden/acc_runs_merge.npz)."""
+    from oracle import merge as om
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "acc_runs_merge.npz"))
+    e = om.merge_energy(d["in_E"], d["in_E2"], d["in_n"].astype(float))
+    for k, ref in (("E", "out_E"), ("E2", "out_E2"), ("e_mean", "out_e_mean"), ("e2_mean", "out_e2_mean"),
+                   ("var", "out_var")):
+        np.testing.assert_allclose(e[k], d[ref], rtol=1e-13, atol=1e-12)
+    m = om.merge_ssf(d["in_sc"], d["in_sc2"], d["in_ssf_n"].astype(float))
+    for k, ref in (("static_corr", "out_sc"), ("static_corr_2", "out_sc2"), ("var_inter", "out_var_inter"),
+                   ("var_intra", "out_var_intra")):
+        np.testing.assert_allclose(m[k], d[ref], rtol=1e-12, atol=1e-9)
+    p = om.plane_invariants(d["in_sc"][0], d["in_ssf_n"][0], d["corr"])
+    np.testing.assert_allclose(p["w"], d["pl_w"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(p["chi_frac"], d["pl_chi"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(p["tr"], d["pl_tr"], rtol=1e-12, atol=1e-12)
