@@ -54,6 +54,9 @@ struct PassArgs {
 void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl = false);
 // Load variant 3 (row tiles staged by bulk copies): sets the kernels' shared-memory limit.
 void staged_prepare();
+// The colour pass of load variant 3 (sweep_staged.cu) and of the lifted moves (sweep_lifted.cu).
+void launch_staged(PassMode mode, const PassArgs& a, int threads, cudaStream_t st, bool pdl);
+void launch_lifted_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl);
 
 struct EnergyArgs {
     const float4* spins;

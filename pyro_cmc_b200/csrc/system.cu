@@ -935,7 +935,6 @@ int pc_setup_lattice(pc_system* sys) {
     PC_CK(sys->d_tab_full.alloc(16));
     PC_CK(cudaMemcpy(sys->d_tab_active.p, sys->tab_active, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
     PC_CK(cudaMemcpy(sys->d_tab_full.p, sys->tab_full, sizeof(SlTable) * 16, cudaMemcpyHostToDevice));
-    pc::staged_prepare();
     rc = build_tiles(sys);
     if (rc) return rc;
     sys->ready = true;
