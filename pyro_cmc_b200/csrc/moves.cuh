@@ -2,9 +2,7 @@
 // (generic bond-table pass, structured pyrochlore pass), shared by the
 // translation units that instantiate them: sweep.cu (Metropolis,
 // overrelaxation and fused passes), sweep_lifted.cu (lifted Metropolis) and
-// sweep_staged.cu (row-staged passes). Instantiating each family in its own
-// module keeps the hot fused kernel's module small: with all families in one
-// module the fused pass measured 12 % slower.
+// sweep_staged.cu (row-staged passes), each family in its own module.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -253,13 +251,15 @@ __device__ __forceinline__ void flush_accepted(const PassArgs& a, unsigned int& 
     mine = 0;
 }
 
-// Programmatic dependent launch: let the next kernel on the stream start its
-// launch now, then wait until the previous kernel has finished and its writes
-// are visible (both are no-ops for a kernel launched without the attribute).
-__device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-}
+// Programmatic dependent launch. pdl_wait at entry: wait until the previous
+// kernel on the stream has finished and its writes are visible. pdl_trigger
+// once a CTA's updates are done: the next pass may start launching when every
+// CTA has triggered, overlapping its launch with this pass's last CTAs.
+// Triggering at entry instead made the next pass's CTAs resident early, where
+// they held warp slots the running pass needed (measured 6 % slower at L=64).
+// Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // Generic colour pass: bond tables (any coupling set) staged in shared memory.
 template <int MODE>
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
     __shared__ SlTable tab[4];
     __shared__ unsigned int warp_acc[16];
     stage_tables(tab, a.tables, a.n_tab, a.tab_sl);  // tables are never written by kernels
-    pdl_enter();
+    pdl_wait();
     __syncthreads();
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
     unsigned int mine = 0;
@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
             mine += apply_move<MODE>(a, S, size_t(sl) * Nc + cell, h, r, sweep) ? 1u : 0u;
         }
     }
+    pdl_trigger();
     if ((MODE == kMetropolis || MODE >= kFusedRotate) && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
 }
 
@@ -432,7 +433,7 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
 template <int MODE, int VAR>
 __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant__ PassArgs a) {
     __shared__ unsigned int warp_acc[8];
-    pdl_enter();
+    pdl_wait();
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
     unsigned int mine = 0;
     int r_cur = -1;
@@ -454,14 +455,14 @@ __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant_
             mine += accepted ? 1u : 0u;
         }
     }
+    pdl_trigger();
     if ((MODE == kMetropolis || MODE >= kFusedRotate) && r_cur >= 0) flush_accepted(a, mine, r_cur, warp_acc);
 }
 
 // The colour passes gather 30 neighbours per site through L1 and use almost no
 // shared memory: ask for the largest L1 (smallest shared-memory carveout), once
-// per kernel and device. Without it, after kernels with large dynamic shared
-// memory (the S(q) stages) had been loaded or run, the driver kept a
-// shared-heavy split and the fused L=64 pass measured 12 % slower.
+// per kernel and device, whatever kernels with large shared memory (the S(q)
+// stages) ran before.
 inline void prefer_l1(const void* fn) {
     static std::mutex mu;
     static std::set<std::pair<int, const void*>> done;

@@ -232,12 +232,13 @@ __global__ void __launch_bounds__(256) staged_pass_kernel(const __grid_constant_
     const ReplicaDev rep = a.reps[r];
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
-    pdl_enter();  // spins are read only after the previous kernel finished
+    pdl_wait();  // spins are read only after the previous kernel finished
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
     unsigned mine = 0;
 #define PC_CALL(K) mine = staged_tile<MODE, K>(a, tile, rep, r, rows, &bar, sweep)
     PC_SL_SWITCH(sl, PC_CALL)
 #undef PC_CALL
+    pdl_trigger();
     if (MODE == kMetropolis || MODE >= kFusedRotate) flush_accepted(a, mine, r, warp_acc);
 }
 
@@ -260,8 +261,8 @@ void staged_prepare() {
 }
 
 // The shared-memory limit of the staged kernels is raised on their first use on
-// a device, not at setup: raising it early (which loads this module first)
-// measured a 12 % slower fused pass of sweep.cu in the same process.
+// a device, not at setup: systems that never use load variant 3 never load
+// this module.
 void launch_staged(PassMode mode, const PassArgs& a, int threads, cudaStream_t st, bool pdl) {
     {
         static std::mutex mu;

@@ -176,7 +176,7 @@ struct pc_system {
 
     // sweep graph cache, keyed by n_overrelax
     std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> sweep_graphs;  // (n_or, sweeps) -> (graph, nodes)
-    bool pdl = true;  // colour passes launched with programmatic dependent launch
+    bool pdl = false;  // colour passes launched with programmatic dependent launch (measured: no gain)
     int update = 0;   // 0 Metropolis, 1 lifted (u-form), 2 lifted (rotation form)
 
     // kernel timing

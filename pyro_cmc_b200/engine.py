@@ -171,7 +171,7 @@ class System:
         call("pc_set_update", self._h, int(mode))
 
     def set_launch_overlap(self, on: bool):
-        """Programmatic dependent launch between colour passes (default on)."""
+        """Programmatic dependent launch between colour passes (default off)."""
         call("pc_set_launch_overlap", self._h, int(bool(on)))
 
     def set_kernel_path(self, force_generic: bool):
