@@ -15,8 +15,8 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
-    "-shared",
 ]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 
 def _nvcc():
@@ -34,10 +34,33 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _compile(src: str, force: bool, verbose: bool) -> str:
+    """One translation unit to an object; skipped when the object is newer
+    than the source and every header (no device symbol crosses units, so
+    whole-program device compilation is not needed)."""
+    obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS] + \
+        [os.path.join(REPO, "include", "pyrocmc.h")]
+    if not force and os.path.exists(obj) and all(os.path.getmtime(d) <= os.path.getmtime(obj) for d in deps):
+        return obj
+    cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(REPO, "include"), "-c", os.path.join(CSRC, src),
+           "-o", obj + ".tmp"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(obj + ".tmp", obj)
+    return obj
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or needs_build():
-        cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp",
-               *[os.path.join(CSRC, f) for f in SOURCES], "-lcudart"]
+        from concurrent.futures import ThreadPoolExecutor
+
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+            objs = list(ex.map(lambda f: _compile(f, force, verbose), SOURCES))
+        cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp", *objs,
+               "-lcudart"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
