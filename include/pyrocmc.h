@@ -265,7 +265,8 @@ int pc_pt_slots(pc_system* sys, int32_t* slot_of_replica);
  *   grad_J[r][spec][9] = g[r]/Nc * dE/dJ_spec      (host, may be NULL)
  *   grad_B[r][3] = -g[r]/Nc * sum_i S_i            (host, may be NULL)
  * and e_per_cell[r] (host). dE/dJ_spec[a][b] = sum over the spec's bonds of
- * S_src[a] S_tgt[b]. */
+ * S_src[a] S_tgt[b]. With grad_J NULL the coupling products are not formed at
+ * all (the spin gradient alone costs about one energy evaluation). */
 int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* grad_S_dev, double* grad_J,
                    double* grad_B);
 /* S(q) for every replica into a device buffer out_dev[R][n_corr][n_k][2]

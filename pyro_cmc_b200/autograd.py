@@ -111,8 +111,8 @@ class EnergyFunction(torch.autograd.Function):
         (spins,) = ctx.saved_tensors
         _load(system, spins)
         g = grad_e.detach().to("cpu", torch.float64).numpy()
-        grad_spins = torch.zeros_like(spins)
-        _, gJ, gB = system.energy_grad(g, grad_spins.data_ptr())
+        grad_spins = torch.empty_like(spins)  # every site is written
+        _, gJ, gB = system.energy_grad(g, grad_spins.data_ptr(), couplings=ctx.has_params)
         gp = None
         if ctx.has_params:
             gp = torch.as_tensor(_param_grads(system, gJ.reshape(system.R, -1, 3, 3), gB).sum(axis=0),
@@ -170,8 +170,8 @@ def gradient_quench(system: System, steps: int = 500, lr: float = 0.05) -> np.nd
     spins = spins_tensor(system)
     hist = []
     for _ in range(steps):
-        g = torch.zeros_like(spins)
-        e, _, _ = system.energy_grad(None, g.data_ptr())
+        g = torch.empty_like(spins)  # every site is written
+        e, _, _ = system.energy_grad(None, g.data_ptr(), couplings=False)
         hist.append(e)
         t = project_tangent(g, spins)
         new = spins[:, :3] - lr * t[:, :3]

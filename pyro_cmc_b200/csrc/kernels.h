@@ -63,9 +63,10 @@ struct EnergyArgs {
     const ReplicaDev* reps;
     const SlTable* tables;  // 16 tables
     const Tile* tiles;      // all sublattices of all replicas, replica-contiguous
+    const int32_t* order;   // tiles in execution order, sublattice by sublattice
     int n_tiles;
     float B[3];
-    double* partial;  // [n_tiles][4]: sum (0.5 S.h - S.B), sum S
+    double* partial;  // [n_tiles][4] by tile index: sum (0.5 S.h - S.B), sum S
     int structured;
     PyroMats mats;
 };
@@ -99,6 +100,25 @@ struct GradArgs {
 void launch_energy_grad_partials(const GradArgs& a, int threads, cudaStream_t st);
 void launch_grad_finalize(const double* partial, int width, const int32_t* tile_begin, const int32_t* tile_end,
                           int R, double* out /*[R][width]*/, cudaStream_t st);
+
+// Structured energy gradient (grad.cu): work items of up to kGradK
+// consecutive tiles of one (replica, sublattice), one site per tile and thread.
+constexpr int kGradK = 2;
+struct GradStructArgs {
+    const float4* spins;
+    const ReplicaDev* reps;
+    const Tile* tiles;
+    const int4* items;  // x = first tile, y = number of tiles (1..kGradK), z = partial-sum slot
+    int n_items;
+    int width;          // 4 (energy, sum S) or 4 + 9*n_spec (with dE/dJ per spec)
+    float B[3];
+    const double* g;    // per-replica upstream scalar (device)
+    float4* grad_S;     // may be null
+    double* partial;    // [n_items][width], by slot
+    PyroMats mats;
+    uint32_t spec_mask[16][kGroups][2];  // specs owning group g's side-k displacements
+};
+void launch_energy_grad_struct(const GradStructArgs& a, bool want_J, int threads, cudaStream_t st);
 
 void launch_random_spins(float4* spins, const ReplicaDev* reps, const Tile* tiles, int n_tiles, uint64_t seed,
                          int threads, cudaStream_t st);

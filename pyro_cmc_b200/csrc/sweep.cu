@@ -97,7 +97,8 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
 __global__ void __launch_bounds__(512) energy_partials_kernel(const __grid_constant__ EnergyArgs a) {
     __shared__ SlTable tab;
     __shared__ double red[4 * 32];
-    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+    for (int u = blockIdx.x; u < a.n_tiles; u += gridDim.x) {
+        const int t = a.order[u];
         const Tile tile = a.tiles[t];
         const int r = tile.x, sl = tile.y & 0xff;
         __syncthreads();
@@ -131,7 +132,8 @@ __device__ __forceinline__ float3 struct_field_e(const EnergyArgs& a, const floa
 
 __global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constant__ EnergyArgs a) {
     __shared__ double red[4 * 32];
-    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+    for (int u = blockIdx.x; u < a.n_tiles; u += gridDim.x) {
+        const int t = a.order[u];  // sublattice by sublattice: CTAs resident together run the same code
         const Tile tile = a.tiles[t];
         const int r = tile.x, sl = tile.y & 0xff;
         const ReplicaDev rep = a.reps[r];

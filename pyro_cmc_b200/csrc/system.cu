@@ -162,6 +162,7 @@ struct pc_system {
     std::vector<DevBuf<Tile>> d_colour_tiles;
     std::vector<int> n_colour_tiles;
     DevBuf<Tile> d_all_tiles;
+    DevBuf<int32_t> d_all_order;  // all tiles sublattice by sublattice (execution order of the energy)
     int n_all_tiles = 0;
     std::vector<int32_t> tile_begin, tile_end;
     DevBuf<int32_t> d_tile_begin, d_tile_end;
@@ -170,6 +171,15 @@ struct pc_system {
     DevBuf<double> d_theta;
     DevBuf<float4> d_field;
     DevBuf<double> d_grad_g, d_grad_out;  // energy-gradient upstream scalars and results
+    // structured energy gradient: specs per (sublattice, group, bond side) and
+    // work items of up to kGradK tiles of one (replica, sublattice)
+    bool grad_struct = false;
+    uint32_t spec_mask[16][pc::kGroups][2] = {};
+    DevBuf<int4> d_grad_items;
+    int n_grad_items = 0;
+    std::vector<int32_t> item_begin, item_end;
+    DevBuf<int32_t> d_item_begin, d_item_end;
+    DevBuf<double> d_grad_partial;
 
     uint64_t host_sweep = 0;
     uint64_t launches = 0;
@@ -228,6 +238,7 @@ struct pc_system {
         d_tab_full.release();
         for (auto& t : d_colour_tiles) t.release();
         d_all_tiles.release();
+        d_all_order.release();
         d_tile_begin.release();
         d_tile_end.release();
         d_partial.release();
@@ -239,6 +250,10 @@ struct pc_system {
         d_ssf_sq.release();
         d_grad_g.release();
         d_grad_out.release();
+        d_grad_items.release();
+        d_item_begin.release();
+        d_item_end.release();
+        d_grad_partial.release();
         for (auto& g : groups) {
             g.d_rep_index.release();
             g.d_sel_index.release();
@@ -340,13 +355,17 @@ int build_tables(pc_system* s, bool keep_zero, SlTable* out) {
 // each group carries one matrix, the structured kernels apply.
 void build_struct(pc_system* s) {
     s->structured = !s->force_generic;
+    s->grad_struct = s->structured && s->specs.size() <= 32;
     std::memset(&s->mats, 0, sizeof(s->mats));
+    std::memset(s->spec_mask, 0, sizeof(s->spec_mask));
     for (int sl = 0; sl < 16 && s->structured; ++sl) {
         const pc::SStruct T = pc::make_struct(sl);
         const int p = sl % 4;
         const auto r = r_sl(sl);
         double E[pc::kStructNb][9] = {};
-        for (const auto& c : s->specs)
+        uint32_t owners[pc::kStructNb] = {};  // specs owning each structural displacement
+        for (size_t ci = 0; ci < s->specs.size(); ++ci) {
+            const Coupling& c = s->specs[ci];
             for (const auto& v : c.rel[p]) {
                 const int g = pc::cs_group(sl, int(v[0]), int(v[1]), int(v[2]));
                 if (std::llabs(v[0]) > 4 || std::llabs(v[1]) > 4 || std::llabs(v[2]) > 4 || g < 0) {
@@ -368,8 +387,22 @@ void build_struct(pc_system* s) {
                 }
                 const double* M = (p <= sl2 % 4) ? c.J : c.Jt;
                 for (int i = 0; i < 9; ++i) E[e][i] += M[i];
+                if (ci < 32) owners[e] |= 1u << ci;
             }
+            if (!s->structured) break;
+        }
         if (!s->structured) break;
+        // the structured gradient needs one owner set per (group, bond side)
+        for (int g = 0; g < pc::kGroups; ++g)
+            for (int side = 0; side < 2; ++side) {
+                bool first = true;
+                for (int k = T.gbegin[g]; k < T.gbegin[g + 1]; ++k) {
+                    if ((p <= T.nb[k].sl % 4 ? 0 : 1) != side) continue;
+                    if (first) s->spec_mask[sl][g][side] = owners[k];
+                    else if (s->spec_mask[sl][g][side] != owners[k]) s->grad_struct = false;
+                    first = false;
+                }
+            }
         for (int g = 0; g < pc::kGroups; ++g) {
             const int b = T.gbegin[g], e1 = T.gbegin[g + 1];
             bool nonzero = false;
@@ -382,6 +415,7 @@ void build_struct(pc_system* s) {
             if (nonzero) s->mats.active[sl] |= 1u << g;
         }
     }
+    s->grad_struct = s->grad_struct && s->structured;
 }
 
 // Colour classes from the active bonds: sublattices joined by a nonzero bond
@@ -477,6 +511,11 @@ int build_tiles(pc_system* s) {
     s->n_all_tiles = int(all.size());
     PC_CK(s->d_all_tiles.alloc(all.size()));
     PC_CK(cudaMemcpy(s->d_all_tiles.p, all.data(), all.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    std::vector<int32_t> order(all.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return all[size_t(x)].y < all[size_t(y)].y; });
+    PC_CK(s->d_all_order.alloc(order.size()));
+    PC_CK(cudaMemcpy(s->d_all_order.p, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     PC_CK(s->d_tile_begin.alloc(size_t(s->R)));
     PC_CK(s->d_tile_end.alloc(size_t(s->R)));
     PC_CK(cudaMemcpy(s->d_tile_begin.p, s->tile_begin.data(), sizeof(int32_t) * size_t(s->R), cudaMemcpyHostToDevice));
@@ -484,6 +523,34 @@ int build_tiles(pc_system* s) {
     // partial sums: energy (4 per tile) and gradient (4 + 9*n_spec per tile)
     const size_t width = size_t(4 + 9 * std::max<size_t>(1, s->specs.size()));
     PC_CK(s->d_partial.alloc(size_t(s->n_all_tiles) * width));
+    // structured-gradient work items: runs of up to kGradK tiles of one
+    // (replica, sublattice). Their partial-sum slots are replica-contiguous (the
+    // per-replica finalize sums a slot range), but the items run sublattice by
+    // sublattice: CTAs resident together then execute the same sublattice's
+    // code, which keeps the instruction cache warm.
+    std::vector<int4> items;
+    s->item_begin.assign(size_t(s->R), 0);
+    s->item_end.assign(size_t(s->R), 0);
+    for (int r = 0; r < s->R; ++r) {
+        s->item_begin[size_t(r)] = int(items.size());
+        for (int t = s->tile_begin[size_t(r)]; t < s->tile_end[size_t(r)];) {
+            int n = 1;
+            while (n < pc::kGradK && t + n < s->tile_end[size_t(r)] && all[size_t(t + n)].y == all[size_t(t)].y) ++n;
+            items.push_back(make_int4(t, n, int(items.size()), 0));  // z: partial-sum slot
+            t += n;
+        }
+        s->item_end[size_t(r)] = int(items.size());
+    }
+    std::stable_sort(items.begin(), items.end(),
+                     [&](const int4& x, const int4& y) { return all[size_t(x.x)].y < all[size_t(y.x)].y; });
+    s->n_grad_items = int(items.size());
+    PC_CK(s->d_grad_items.alloc(items.size()));
+    PC_CK(cudaMemcpy(s->d_grad_items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    PC_CK(s->d_item_begin.alloc(size_t(s->R)));
+    PC_CK(s->d_item_end.alloc(size_t(s->R)));
+    PC_CK(cudaMemcpy(s->d_item_begin.p, s->item_begin.data(), sizeof(int32_t) * size_t(s->R), cudaMemcpyHostToDevice));
+    PC_CK(cudaMemcpy(s->d_item_end.p, s->item_end.data(), sizeof(int32_t) * size_t(s->R), cudaMemcpyHostToDevice));
+    PC_CK(s->d_grad_partial.alloc(items.size() * width));
     s->drop_graphs();
     return PC_OK;
 }
@@ -639,6 +706,7 @@ int enqueue_energy(pc_system* s) {
     a.reps = s->d_reps.p;
     a.tables = s->d_tab_active.p;
     a.tiles = s->d_all_tiles.p;
+    a.order = s->d_all_order.p;
     a.n_tiles = s->n_all_tiles;
     for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
     a.partial = s->d_partial.p;
@@ -1743,7 +1811,9 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
     int rc = check_sys(sys);
     if (rc) return rc;
     const int ns = int(sys->specs.size());
-    const int width = 4 + 9 * ns;
+    // the structured kernel forms the coupling products only when they are asked for
+    const bool structured = sys->grad_struct && sys->threads <= 256;
+    const int width = (structured && !grad_J) ? 4 : 4 + 9 * ns;
     if (sys->d_grad_g.n != size_t(sys->R)) PC_CK(sys->d_grad_g.alloc(size_t(sys->R)));
     if (sys->d_grad_out.n != size_t(sys->R) * size_t(width))
         PC_CK(sys->d_grad_out.alloc(size_t(sys->R) * size_t(width)));
@@ -1752,22 +1822,43 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
     std::vector<double> ones(size_t(sys->R), 1.0);
     PC_CK(cudaMemcpyAsync(d_g.p, g ? g : ones.data(), sizeof(double) * size_t(sys->R), cudaMemcpyHostToDevice,
                           sys->stream));
-    pc::GradArgs a;
-    a.spins = sys->d_spins.p;
-    a.reps = sys->d_reps.p;
-    a.tables = sys->d_tab_full.p;
-    a.tiles = sys->d_all_tiles.p;
-    a.n_tiles = sys->n_all_tiles;
-    a.n_spec = ns;
-    for (int i = 0; i < 3; ++i) a.B[i] = float(sys->B[i]);
-    a.g = d_g.p;
-    a.grad_S = static_cast<float4*>(grad_S_dev);
-    a.partial = sys->d_partial.p;
-    pc::launch_energy_grad_partials(a, sys->threads, sys->stream);
-    PC_LAUNCH_CK();
-    pc::launch_grad_finalize(sys->d_partial.p, width, sys->d_tile_begin.p, sys->d_tile_end.p, sys->R, d_out.p,
-                             sys->stream);
-    PC_LAUNCH_CK();
+    if (structured) {
+        pc::GradStructArgs a;
+        a.spins = sys->d_spins.p;
+        a.reps = sys->d_reps.p;
+        a.tiles = sys->d_all_tiles.p;
+        a.items = sys->d_grad_items.p;
+        a.n_items = sys->n_grad_items;
+        a.width = width;
+        for (int i = 0; i < 3; ++i) a.B[i] = float(sys->B[i]);
+        a.g = d_g.p;
+        a.grad_S = static_cast<float4*>(grad_S_dev);
+        a.partial = sys->d_grad_partial.p;
+        a.mats = sys->mats;
+        std::memcpy(a.spec_mask, sys->spec_mask, sizeof(a.spec_mask));
+        pc::launch_energy_grad_struct(a, grad_J != nullptr, sys->threads, sys->stream);
+        PC_LAUNCH_CK();
+        pc::launch_grad_finalize(sys->d_grad_partial.p, width, sys->d_item_begin.p, sys->d_item_end.p, sys->R,
+                                 d_out.p, sys->stream);
+        PC_LAUNCH_CK();
+    } else {
+        pc::GradArgs a;
+        a.spins = sys->d_spins.p;
+        a.reps = sys->d_reps.p;
+        a.tables = sys->d_tab_full.p;
+        a.tiles = sys->d_all_tiles.p;
+        a.n_tiles = sys->n_all_tiles;
+        a.n_spec = ns;
+        for (int i = 0; i < 3; ++i) a.B[i] = float(sys->B[i]);
+        a.g = d_g.p;
+        a.grad_S = static_cast<float4*>(grad_S_dev);
+        a.partial = sys->d_partial.p;
+        pc::launch_energy_grad_partials(a, sys->threads, sys->stream);
+        PC_LAUNCH_CK();
+        pc::launch_grad_finalize(sys->d_partial.p, width, sys->d_tile_begin.p, sys->d_tile_end.p, sys->R, d_out.p,
+                                 sys->stream);
+        PC_LAUNCH_CK();
+    }
     sys->launches += 2;
     std::vector<double> out(size_t(sys->R) * size_t(width));
     PC_CK(cudaMemcpyAsync(out.data(), d_out.p, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, sys->stream));

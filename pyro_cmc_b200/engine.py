@@ -380,17 +380,19 @@ class System:
         return s
 
     # -------------------------------------------------------- gradients
-    def energy_grad(self, g=None, grad_spins_ptr: int | None = None):
-        """Energy per cell, dE/dJ_spec (per replica, per spec, 3x3) and dE/dB,
-        scaled by upstream g[r]; writes dE/dS into grad_spins_ptr if given."""
+    def energy_grad(self, g=None, grad_spins_ptr: int | None = None, couplings: bool = True):
+        """Energy per cell, dE/dJ_spec (per replica, per spec, 3x3; None with
+        couplings=False, which skips forming them) and dE/dB, scaled by
+        upstream g[r]; writes dE/dS into grad_spins_ptr if given."""
         n_spec = len(self.spec_names)
         e = np.empty(self.R)
-        gJ = np.empty((self.R, n_spec, 9))
+        gJ = np.empty((self.R, n_spec, 9)) if couplings else None
         gB = np.empty((self.R, 3))
         gv = None if g is None else _c(np.broadcast_to(np.asarray(g, dtype=np.float64), (self.R,)), np.float64)
         call("pc_energy_grad", self._h, None if gv is None else _dp(gv), _dp(e),
-             None if grad_spins_ptr is None else C.c_void_p(grad_spins_ptr), _dp(gJ), _dp(gB))
-        return e, gJ.reshape(self.R, n_spec, 3, 3), gB
+             None if grad_spins_ptr is None else C.c_void_p(grad_spins_ptr), None if gJ is None else _dp(gJ),
+             _dp(gB))
+        return e, None if gJ is None else gJ.reshape(self.R, n_spec, 3, 3), gB
 
     # ---------------------------------------------------------------- tuning
     def autotune(self):

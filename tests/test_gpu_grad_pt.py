@@ -51,6 +51,47 @@ def test_energy_grad_matches_oracle():
     np.testing.assert_allclose(gB[0], -S.sum(axis=0) / Nc, atol=1e-6 * g.N())
 
 
+@pytest.mark.parametrize("L,R,threads", [(3, 1, 128), (8, 3, 128), (8, 2, 64), (12, 1, 256)])
+def test_structured_energy_grad_matches_generic_and_oracle(L, R, threads):
+    """The structured gradient kernel (work items of up to two tiles per
+    thread, per-warp rows) against the generic bond-table kernel and, for
+    replica 0, the oracle; without coupling gradients it gives the same energy,
+    spin gradient and field gradient."""
+    c = dict(J1=1.0, J2=0.1, J3=-0.05, Delta=0.6, B=(0.2, -0.1, 0.3))
+    g = pc.pyrochlore_system(L, n_replicas=R, **c)
+    g.set_tile(threads, 4)
+    rng = np.random.default_rng(L + R)
+    for r in range(R):
+        g.set_spins(unit(rng, g.N(r)), r)
+    up = np.linspace(1.0, -0.5, R)
+    res = {}
+    for generic in (False, True):
+        g.set_kernel_path(generic)
+        grad = torch.zeros((g.N_total, 4), dtype=torch.float32, device="cuda")
+        e, gJ, gB = g.energy_grad(up, grad.data_ptr())
+        res[generic] = (e, gJ, gB, grad.cpu().numpy())
+    g.set_kernel_path(False)
+    grad = torch.full((g.N_total, 4), 7.0, dtype=torch.float32, device="cuda")
+    e2, gJ2, gB2 = g.energy_grad(up, grad.data_ptr(), couplings=False)
+    assert gJ2 is None
+    (e, gJ, gB, gs), (eg, gJg, gBg, gsg) = res[False], res[True]
+    np.testing.assert_allclose(e, eg, rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(gB, gBg, rtol=1e-6, atol=1e-6)
+    assert np.abs(gs - gsg).max() <= 1e-5 * np.abs(gsg).max()
+    assert np.abs(gJ - gJg).max() <= 1e-5 * max(1.0, np.abs(gJg).max())
+    np.testing.assert_allclose(e2, e, rtol=1e-6, atol=1e-6)
+    np.testing.assert_array_equal(gB2, gB)
+    g2 = grad.cpu().numpy()
+    assert np.abs(g2 - gs).max() <= 1e-5 * np.abs(gs).max()  # every site written
+    assert np.all(g2[:, 3] == 0)
+    o = oracle.System(L, **c)
+    o.set_spins(g.spins(0))
+    Nc = L ** 3
+    ref_gJ = up[0] * o.coupling_grads() / Nc
+    assert np.abs(gJ[0] - ref_gJ).max() <= 1e-5 * max(1.0, np.abs(ref_gJ).max())
+    assert e[0] == pytest.approx(o.energy(), abs=1e-5 * 100)
+
+
 def test_energy_autograd_params_vs_finite_differences():
     L = 2
     g = pc.pyrochlore_system(L, n_replicas=2, **C4)
