@@ -125,6 +125,58 @@ __device__ __forceinline__ void field_groups(float3& h, const float4 (&v)[kStruc
     }
 }
 
+// Each bond once: the field of site i of sublattice SL restricted to the
+// neighbours on higher sublattices, h+_i = sum_G M_G sum_{e in G, s2 > SL} S_e.
+// Since the matrix seen from the other end is the transpose, the energy
+// 0.5 sum_i S_i.h_i equals sum_i S_i.h+_i: half the neighbour loads.
+template <int SL, int E>
+__device__ __forceinline__ void add_upper(float3& t, const float4* __restrict__ S, int Nc, const Coords& c) {
+    if constexpr (nb_sl(SL, E) > SL) {
+        const float4 v = load_nb<SL, E>(S, Nc, c);
+        t.x += v.x;
+        t.y += v.y;
+        t.z += v.z;
+    }
+}
+__host__ __device__ constexpr bool group_has_upper(int sl, int g) {
+    for (int e = grp_begin(sl, g); e < grp_begin(sl, g + 1); ++e)
+        if (nb_sl(sl, e) > sl) return true;
+    return false;
+}
+template <int SL, int G, int... K>
+__device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
+                                                const PyroMats& mats, std::integer_sequence<int, K...>) {
+    if constexpr (group_has_upper(SL, G)) {
+        if (mats.active[SL] & (1u << G)) {
+            constexpr int B = grp_begin(SL, G);
+            float3 t = make_float3(0.f, 0.f, 0.f);
+            (add_upper<SL, B + K>(t, S, Nc, c), ...);
+            const float* J = mats.M[SL][G];
+            h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
+            h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
+            h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+        }
+    }
+}
+template <int SL, int G>
+__device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
+                                                const PyroMats& mats) {
+    add_group_upper<SL, G>(h, S, Nc, c, mats, std::make_integer_sequence<int, grp_size(SL, G)>{});
+}
+template <int SL>
+__device__ __forceinline__ float3 struct_field_upper(const float4* __restrict__ S, const PyroMats& mats, int cell,
+                                                     int L, int Nc, uint64_t divL) {
+    const Coords c = cell_coords(cell, L, divL);
+    float3 h = make_float3(0.f, 0.f, 0.f);
+    add_group_upper<SL, 0>(h, S, Nc, c, mats);
+    add_group_upper<SL, 1>(h, S, Nc, c, mats);
+    add_group_upper<SL, 2>(h, S, Nc, c, mats);
+    add_group_upper<SL, 3>(h, S, Nc, c, mats);
+    add_group_upper<SL, 4>(h, S, Nc, c, mats);
+    add_group_upper<SL, 5>(h, S, Nc, c, mats);
+    return h;
+}
+
 template <int SL>
 __device__ __forceinline__ float3 struct_field(const float4* __restrict__ S, const PyroMats& mats, int cell,
                                                int L, int Nc, uint64_t divL) {

@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(512) energy_partials_kernel(const __grid_const
 
 template <int SL>
 __device__ __forceinline__ float3 struct_field_e(const EnergyArgs& a, const float4* S, const ReplicaDev& rep, int cell) {
-    return struct_field<SL>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
+    return struct_field_upper<SL>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
 }
 
 __global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constant__ EnergyArgs a) {
@@ -146,7 +146,8 @@ __global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constan
 #define PC_CALL(K) h = struct_field_e<K>(a, S, rep, cell)
             PC_SL_SWITCH(sl, PC_CALL)
 #undef PC_CALL
-            v[0] = 0.5 * double(s0.x * h.x + s0.y * h.y + s0.z * h.z) -
+            // h: the bonds to higher sublattices only, each bond counted once
+            v[0] = double(s0.x * h.x + s0.y * h.y + s0.z * h.z) -
                    double(s0.x * a.B[0] + s0.y * a.B[1] + s0.z * a.B[2]);
             v[1] = s0.x;
             v[2] = s0.y;

@@ -220,7 +220,23 @@ struct pc_system {
     std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> pt_graphs;  // (n_sweep, phase)
     uint64_t pt_sweeps_done = 0;
 
+    // pinned host staging for the small per-call transfers (upstream scalars,
+    // energies, gradient sums, the device error flag): one synchronisation per
+    // call instead of one per pageable copy
+    void* h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    cudaError_t stage(size_t bytes) {
+        if (bytes <= h_stage_bytes) return cudaSuccess;
+        if (h_stage) cudaFreeHost(h_stage);
+        h_stage = nullptr;
+        h_stage_bytes = 0;
+        const cudaError_t e = cudaMallocHost(&h_stage, bytes);
+        if (e == cudaSuccess) h_stage_bytes = bytes;
+        return e;
+    }
+
     ~pc_system() {
+        if (h_stage) cudaFreeHost(h_stage);
         for (auto& g : sweep_graphs) cudaGraphExecDestroy(g.second.first);
         for (auto& g : pt_graphs) cudaGraphExecDestroy(g.second.first);
         for (auto& e : ev_pool) {
@@ -1209,16 +1225,21 @@ int pc_set_sweep_counter(pc_system* sys, int replica, uint64_t sweep) {
     return PC_OK;
 }
 
-// Reads (and clears) the device error flag that a kernel sets when one of its
-// bounded waits runs out. Synchronises the system's stream.
-int device_error(pc_system* s) {
-    int flag = 0;
-    PC_CK(cudaMemcpyAsync(&flag, s->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-    PC_CK(cudaStreamSynchronize(s->stream));
+// The device error flag as read back (flag != 0: one of a kernel's bounded
+// waits ran out): clears it and reports the failure.
+int device_error_flag(pc_system* s, int flag) {
     if (!flag) return PC_OK;
     PC_CK(cudaMemsetAsync(s->d_err.p, 0, sizeof(int), s->stream));
     return fail(PC_ERR_TIMEOUT, "a colour pass stopped waiting for its staged neighbour rows (bounded wait ran out); "
                                 "the updates of that pass were skipped");
+}
+
+// Reads (and clears) the device error flag. Synchronises the system's stream.
+int device_error(pc_system* s) {
+    int flag = 0;
+    PC_CK(cudaMemcpyAsync(&flag, s->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    PC_CK(cudaStreamSynchronize(s->stream));
+    return device_error_flag(s, flag);
 }
 
 int pc_sweep(pc_system* sys, const double* T, int n_sweeps, int n_overrelax, uint64_t* accepted) {
@@ -1299,11 +1320,17 @@ int pc_energy(pc_system* sys, double* e_per_cell, double* mag) {
     if (rc) return rc;
     rc = enqueue_energy(sys);
     if (rc) return rc;
-    PC_CK(cudaMemcpyAsync(e_per_cell, sys->d_e.p, sizeof(double) * size_t(sys->R), cudaMemcpyDeviceToHost, sys->stream));
-    if (mag)
-        PC_CK(cudaMemcpyAsync(mag, sys->d_mag.p, sizeof(double) * 3 * size_t(sys->R), cudaMemcpyDeviceToHost,
-                              sys->stream));
-    return device_error(sys);
+    const size_t R = size_t(sys->R);
+    PC_CK(sys->stage(sizeof(double) * 4 * R + sizeof(int)));
+    double* st = static_cast<double*>(sys->h_stage);
+    int* flag = reinterpret_cast<int*>(st + 4 * R);
+    PC_CK(cudaMemcpyAsync(st, sys->d_e.p, sizeof(double) * R, cudaMemcpyDeviceToHost, sys->stream));
+    if (mag) PC_CK(cudaMemcpyAsync(st + R, sys->d_mag.p, sizeof(double) * 3 * R, cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaMemcpyAsync(flag, sys->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    std::memcpy(e_per_cell, st, sizeof(double) * R);
+    if (mag) std::memcpy(mag, st + R, sizeof(double) * 3 * R);
+    return device_error_flag(sys, *flag);
 }
 
 int pc_local_field(pc_system* sys, int replica, double* h) {
@@ -1815,13 +1842,16 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
     const bool structured = sys->grad_struct && sys->threads <= 256;
     const int width = (structured && !grad_J) ? 4 : 4 + 9 * ns;
     if (sys->d_grad_g.n != size_t(sys->R)) PC_CK(sys->d_grad_g.alloc(size_t(sys->R)));
-    if (sys->d_grad_out.n != size_t(sys->R) * size_t(width))
-        PC_CK(sys->d_grad_out.alloc(size_t(sys->R) * size_t(width)));
+    if (sys->d_grad_out.n < size_t(sys->R) * size_t(4 + 9 * ns))  // the widest form, kept across calls
+        PC_CK(sys->d_grad_out.alloc(size_t(sys->R) * size_t(4 + 9 * ns)));
     DevBuf<double>& d_g = sys->d_grad_g;
     DevBuf<double>& d_out = sys->d_grad_out;
-    std::vector<double> ones(size_t(sys->R), 1.0);
-    PC_CK(cudaMemcpyAsync(d_g.p, g ? g : ones.data(), sizeof(double) * size_t(sys->R), cudaMemcpyHostToDevice,
-                          sys->stream));
+    const size_t R = size_t(sys->R);
+    PC_CK(sys->stage(sizeof(double) * R * size_t(1 + width)));
+    double* st_g = static_cast<double*>(sys->h_stage);
+    double* st_out = st_g + R;
+    for (size_t r = 0; r < R; ++r) st_g[r] = g ? g[r] : 1.0;
+    PC_CK(cudaMemcpyAsync(d_g.p, st_g, sizeof(double) * R, cudaMemcpyHostToDevice, sys->stream));
     if (structured) {
         pc::GradStructArgs a;
         a.spins = sys->d_spins.p;
@@ -1860,11 +1890,10 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
         PC_LAUNCH_CK();
     }
     sys->launches += 2;
-    std::vector<double> out(size_t(sys->R) * size_t(width));
-    PC_CK(cudaMemcpyAsync(out.data(), d_out.p, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaMemcpyAsync(st_out, d_out.p, sizeof(double) * R * size_t(width), cudaMemcpyDeviceToHost, sys->stream));
     PC_CK(cudaStreamSynchronize(sys->stream));
     for (int r = 0; r < sys->R; ++r) {
-        const double* o = out.data() + size_t(r) * size_t(width);
+        const double* o = st_out + size_t(r) * size_t(width);
         const double nc = double(sys->Nc(r));
         const double gr = g ? g[r] : 1.0;
         if (e_per_cell) e_per_cell[r] = o[0] / nc;
