@@ -300,8 +300,9 @@ int pc_energy_noalloc(const void* spins_dev, int L, const double* params, void* 
 /* ------------------------------------------------------------------ tuning */
 
 /* Times the sweep over the candidate tile shapes (threads per CTA x CTAs per
- * SM) and neighbour-load variants on this system and keeps the fastest (spin
- * state and sweep counter are saved and restored). */
+ * SM) and neighbour-load variants on this system, and the cluster-resident
+ * sweep where it applies, and keeps the fastest (spin state and sweep counter
+ * are saved and restored). */
 int pc_autotune(pc_system* sys);
 /* How the structured kernels issue the 30 neighbour loads of a site:
  * 0 group by group (fewest registers), 1 all at once, 2 in two batches, 3 staged:
@@ -348,6 +349,18 @@ int pc_set_kernel_timing(pc_system* sys, int on);
  * loaded), hence the default. Results are identical either way. No
  * counterpart in the reference (a launch setting). */
 int pc_set_launch_overlap(pc_system* sys, int on);
+/* Cluster-resident sweeps (off by default; pc_autotune turns them on where
+ * they are faster): for replicas of one size L <= 16, one thread-block cluster
+ * of L CTAs per replica holds the lattice in distributed shared memory (one z
+ * plane of all 16 sublattices per CTA) and runs every colour pass of a
+ * pc_sweep call in one launch, with a cluster barrier between passes. Same
+ * passes, draws and arithmetic as the per-pass kernels: the same chain.
+ * PC_ERR_UNSUPPORTED when the system does not qualify (other sizes, lifted
+ * moves, non-pyrochlore couplings, no cluster of that size fits). No
+ * counterpart in the reference (an execution strategy of
+ * MC_runner::sweep_local_Metropolis, src/MC.cpp:155-163). */
+int pc_set_cluster_sweeps(pc_system* sys, int on);
+int pc_get_cluster_sweeps(pc_system* sys, int* on);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,8 @@ _SIGNATURES = {
     "pc_last_kernel_times": (_I, [_P, _DP, _DP]),
     "pc_set_kernel_timing": (_I, [_P, _I]),
     "pc_set_launch_overlap": (_I, [_P, _I]),
+    "pc_set_cluster_sweeps": (_I, [_P, _I]),
+    "pc_get_cluster_sweeps": (_I, [_P, _IP]),
 }
 
 

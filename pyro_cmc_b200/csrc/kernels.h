@@ -58,6 +58,37 @@ void staged_prepare();
 void launch_staged(PassMode mode, const PassArgs& a, int threads, cudaStream_t st, bool pdl);
 void launch_lifted_pass(PassMode mode, const PassArgs& a, int grid, int threads, cudaStream_t st, bool pdl);
 
+// Cluster-resident sweeps (sweep_cluster.cu): one thread-block cluster per
+// replica holds the whole lattice in distributed shared memory, one z plane of
+// all 16 sublattices per CTA (cluster size L, L*L threads per CTA), and runs
+// every colour pass of n_sweeps sweeps in one launch, a cluster barrier
+// between passes. For replicas of one size L <= 16.
+struct ClusterArgs {
+    float4* spins;
+    const ReplicaDev* reps;
+    const double* T_rep;
+    const uint64_t* sweep_base;  // device sweep counter (sweeps run at *sweep_base + 0 .. n_sweeps-1)
+    uint64_t seed;
+    float inv_T_ref;
+    float B[3];
+    unsigned long long* acc;  // per-replica accepted Metropolis moves
+    PyroMats mats;
+    int L;
+    int n_sweeps;
+    int n_or;       // overrelaxation moves per site per sweep
+    int fused;      // 1: first round fused Metropolis + overrelaxation (n_or >= 1)
+    int reflect;    // overrelaxation by reflection instead of a random-angle rotation
+    int n_classes;  // colour classes in order, each up to 4 mutually unbonded sublattices
+    int class_n[16];
+    int class_sl[16][4];
+};
+// Shared memory per CTA of the cluster kernels for lattice size L.
+size_t cluster_smem_bytes(int L);
+// Prepares the kernels (cluster size and shared-memory attributes) and
+// reports how many clusters of this size can be resident (0: not launchable).
+int cluster_capacity(int L, int fused, int reflect);
+void launch_cluster_sweeps(const ClusterArgs& a, int R, cudaStream_t st);
+
 struct EnergyArgs {
     const float4* spins;
     const ReplicaDev* reps;

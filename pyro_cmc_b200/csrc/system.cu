@@ -187,6 +187,8 @@ struct pc_system {
     // sweep graph cache, keyed by n_overrelax
     std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> sweep_graphs;  // (n_or, sweeps) -> (graph, nodes)
     bool pdl = false;  // colour passes launched with programmatic dependent launch (measured: no gain)
+    bool cluster_sweep = false;  // sweeps of small lattices in one cluster-resident launch (sweep_cluster.cu)
+    std::map<std::array<int, 3>, int> cluster_cap;  // (L, fused, reflect) -> resident clusters (0: not launchable)
     int update = 0;   // 0 Metropolis, 1 lifted (u-form), 2 lifted (rotation form)
 
     // kernel timing
@@ -690,7 +692,60 @@ int sweep_graph(pc_system* s, int n_or, int k, cudaGraphExec_t* exec, int* nodes
     return PC_OK;
 }
 
+// Whether the sweeps of this system can run cluster-resident: the structured
+// couplings, standard (not lifted) moves, all replicas of one size L <= 16,
+// and the GPU able to hold a cluster of L CTAs with 16 L^2 float4 each.
+bool cluster_eligible(pc_system* s, int n_or) {
+    if (!s->structured || s->update != 0 || s->R < 1) return false;
+    const int L = s->L[0];
+    for (int r = 1; r < s->R; ++r)
+        if (s->L[size_t(r)] != L) return false;
+    if (L < 2 || L > 16) return false;
+    const int fused = (s->schedule == 1 && n_or >= 1) ? 1 : 0;
+    const std::array<int, 3> key = {L, fused, s->or_mode == 1 ? 1 : 0};
+    auto it = s->cluster_cap.find(key);
+    if (it == s->cluster_cap.end()) it = s->cluster_cap.emplace(key, pc::cluster_capacity(L, key[1], key[2])).first;
+    return it->second > 0;
+}
+
+int launch_cluster(pc_system* s, int n_sweeps, int n_or) {
+    pc::ClusterArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.spins = s->d_spins.p;
+    a.reps = s->d_reps.p;
+    a.T_rep = s->d_T.p;
+    a.sweep_base = s->d_sweep.p;
+    a.seed = s->seed;
+    a.inv_T_ref = float(1.0 / s->T_ref);
+    for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
+    a.acc = s->d_acc.p;
+    a.mats = s->mats;
+    a.L = s->L[0];
+    a.n_sweeps = n_sweeps;
+    a.n_or = n_or;
+    a.fused = (s->schedule == 1 && n_or >= 1) ? 1 : 0;
+    a.reflect = s->or_mode == 1 ? 1 : 0;
+    a.n_classes = s->n_colours;
+    for (int c = 0; c < s->n_colours; ++c) {
+        const auto& sls = s->colour_sls[size_t(c)];
+        a.class_n[c] = int(sls.size());
+        for (size_t k = 0; k < sls.size(); ++k) a.class_sl[c][k] = sls[k];
+    }
+    pc::launch_cluster_sweeps(a, s->R, s->stream);
+    PC_LAUNCH_CK();
+    pc::launch_advance_counter(s->d_sweep.p, uint64_t(n_sweeps), s->stream);
+    PC_LAUNCH_CK();
+    s->launches += 2;
+    return PC_OK;
+}
+
 int run_sweeps(pc_system* s, int n_sweeps, int n_or) {
+    if (s->cluster_sweep && !s->timing && n_sweeps > 0 && cluster_eligible(s, n_or)) {
+        const int rc = launch_cluster(s, n_sweeps, n_or);
+        if (rc) return rc;
+        s->host_sweep += uint64_t(n_sweeps);
+        return PC_OK;
+    }
     if (s->timing) {
         for (int i = 0; i < n_sweeps; ++i) {
             int rc = enqueue_sweep(s, uint64_t(i), n_or, true);
@@ -975,6 +1030,22 @@ int pc_set_launch_overlap(pc_system* sys, int on) {
     if (rc) return rc;
     sys->pdl = on != 0;
     sys->drop_graphs();
+    return PC_OK;
+}
+
+int pc_set_cluster_sweeps(pc_system* sys, int on) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (on && !cluster_eligible(sys, 1))
+        return fail(PC_ERR_UNSUPPORTED, "cluster-resident sweeps need the structured pyrochlore couplings, standard "
+                                        "moves and replicas of one size L <= 16 that fit a thread-block cluster");
+    sys->cluster_sweep = on != 0;
+    return PC_OK;
+}
+int pc_get_cluster_sweeps(pc_system* sys, int* on) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    *on = sys->cluster_sweep ? 1 : 0;
     return PC_OK;
 }
 
@@ -1965,6 +2036,7 @@ int pc_autotune(pc_system* sys) {
     PC_CK(cudaEventCreate(&e1));
     const bool timing = sys->timing;
     sys->timing = false;
+    sys->cluster_sweep = false;
     const int n_var = sys->structured ? 4 : 1;
     for (int vi = 0; vi < n_var; ++vi)
         for (int ti = 0; ti < 4; ++ti)
@@ -1996,6 +2068,24 @@ int pc_autotune(pc_system* sys) {
                     best_v = vi;
                 }
             }
+    // cluster-resident sweeps (small lattices): one more candidate
+    if (cluster_eligible(sys, 1)) {
+        sys->cluster_sweep = true;
+        rc = run_sweeps(sys, 2, 1);
+        if (rc) return rc;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            PC_CK(cudaEventRecord(e0, sys->stream));
+            rc = run_sweeps(sys, 4, 1);
+            if (rc) return rc;
+            PC_CK(cudaEventRecord(e1, sys->stream));
+            PC_CK(cudaEventSynchronize(e1));
+            float t = 0.f;
+            PC_CK(cudaEventElapsedTime(&t, e0, e1));
+            ms = std::min(ms, t);
+        }
+        sys->cluster_sweep = ms < best_ms;
+    }
     sys->timing = timing;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -174,6 +174,19 @@ class System:
         """Programmatic dependent launch between colour passes (default off)."""
         call("pc_set_launch_overlap", self._h, int(bool(on)))
 
+    def set_cluster_sweeps(self, on: bool):
+        """Cluster-resident sweeps for replicas of one size L <= 16 (one
+        thread-block cluster per replica holds the lattice in distributed
+        shared memory and runs all colour passes of a sweep call in one
+        launch); raises PyroCMCError (code 4, unsupported) where the system
+        does not qualify."""
+        call("pc_set_cluster_sweeps", self._h, int(bool(on)))
+
+    def cluster_sweeps(self) -> bool:
+        v = C.c_int()
+        call("pc_get_cluster_sweeps", self._h, C.byref(v))
+        return bool(v.value)
+
     def set_kernel_path(self, force_generic: bool):
         """Force the generic bond-table kernels (True) or allow the structured
         pyrochlore kernels (False, default)."""
