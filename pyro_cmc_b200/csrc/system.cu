@@ -237,7 +237,14 @@ struct pc_system {
         return e;
     }
 
+    // second stream for pc_step_host's result copy, which runs concurrently with
+    // the last S(q) sample and the energy (they read the spins, never write them)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_swept = nullptr;
+
     ~pc_system() {
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (ev_swept) cudaEventDestroy(ev_swept);
         if (h_stage) cudaFreeHost(h_stage);
         for (auto& g : sweep_graphs) cudaGraphExecDestroy(g.second.first);
         for (auto& g : pt_graphs) cudaGraphExecDestroy(g.second.first);
@@ -2113,9 +2120,19 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     if (do_ssf && (!sys->ssf_ready || ssf_slot >= sys->n_slots || sys->L_of_slot[size_t(ssf_slot)] != sys->L[0]))
         return fail(PC_ERR_STATE, "ssf slot not configured for replica 0");
     const size_t bytes = sizeof(float4) * size_t(sys->N(0));
+    if (!sys->copy_stream) {
+        PC_CK(cudaStreamCreateWithFlags(&sys->copy_stream, cudaStreamNonBlocking));
+        PC_CK(cudaEventCreateWithFlags(&sys->ev_swept, cudaEventDisableTiming));
+    }
+    const size_t R = size_t(sys->R);
+    PC_CK(sys->stage(sizeof(double) * R + 2 * sizeof(uint64_t) + sizeof(int)));
+    double* st_T = static_cast<double*>(sys->h_stage);
+    double* st_e = st_T + R;
+    uint64_t* st_acc = reinterpret_cast<uint64_t*>(st_e + 1);
+    int* st_flag = reinterpret_cast<int*>(st_acc + 1);
     PC_CK(cudaMemcpyAsync(sys->d_spins.p, S4_in, bytes, cudaMemcpyHostToDevice, sys->stream));
-    std::vector<double> Tv(size_t(sys->R), T);
-    PC_CK(cudaMemcpyAsync(sys->d_T.p, Tv.data(), sizeof(double) * Tv.size(), cudaMemcpyHostToDevice, sys->stream));
+    for (size_t r = 0; r < R; ++r) st_T[r] = T;
+    PC_CK(cudaMemcpyAsync(sys->d_T.p, st_T, sizeof(double) * R, cudaMemcpyHostToDevice, sys->stream));
     PC_CK(cudaMemsetAsync(sys->d_acc.p, 0, sizeof(unsigned long long) * size_t(sys->R), sys->stream));
     SsfGroup* grp = nullptr;
     if (do_ssf) {
@@ -2127,11 +2144,20 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
             if (g.L == sys->L[0]) grp = &g;
     }
     int done = 0;
-    while (done < n_sweep) {
+    bool copying = false;
+    while (done < n_sweep || !copying) {
         const int chunk = do_ssf ? std::min(ssf_every, n_sweep - done) : n_sweep - done;
-        rc = run_sweeps(sys, chunk, 1);
-        if (rc) return rc;
-        done += chunk;
+        if (chunk > 0) {
+            rc = run_sweeps(sys, chunk, 1);
+            if (rc) return rc;
+            done += chunk;
+        }
+        if (done == n_sweep && !copying) {  // spins final: copy them out while S(q) and the energy run
+            PC_CK(cudaEventRecord(sys->ev_swept, sys->stream));
+            PC_CK(cudaStreamWaitEvent(sys->copy_stream, sys->ev_swept, 0));
+            PC_CK(cudaMemcpyAsync(S4_out, sys->d_spins.p, bytes, cudaMemcpyDeviceToHost, sys->copy_stream));
+            copying = true;
+        }
         if (do_ssf && chunk == ssf_every) {
             pc::SsfOut o = ssf_out_base(sys);
             o.acc_sum = sys->d_ssf_sum.p;
@@ -2148,11 +2174,14 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     }
     rc = enqueue_energy(sys);
     if (rc) return rc;
-    PC_CK(cudaMemcpyAsync(S4_out, sys->d_spins.p, bytes, cudaMemcpyDeviceToHost, sys->stream));
-    if (e_out) PC_CK(cudaMemcpyAsync(e_out, sys->d_e.p, sizeof(double), cudaMemcpyDeviceToHost, sys->stream));
-    if (accepted)
-        PC_CK(cudaMemcpyAsync(accepted, sys->d_acc.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, sys->stream));
-    return device_error(sys);
+    PC_CK(cudaMemcpyAsync(st_e, sys->d_e.p, sizeof(double), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaMemcpyAsync(st_acc, sys->d_acc.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaMemcpyAsync(st_flag, sys->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->copy_stream));
+    if (e_out) *e_out = *st_e;
+    if (accepted) *accepted = *st_acc;
+    return device_error_flag(sys, *st_flag);
 }
 
 int pc_set_kernel_timing(pc_system* sys, int on) {

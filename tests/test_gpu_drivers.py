@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
+import pyro_cmc_b200 as pc
 from pyro_cmc_b200 import build
 from pyro_cmc_b200.anneal import anneal_batch, generate_T_profile
 from pyro_cmc_b200.h5compat import File
@@ -145,3 +146,37 @@ def test_ltgs_driver(tmp_path):
         np.testing.assert_allclose(f["/k_star_vec"][:], 2 * np.pi * np.array(k_ref) / 24.0)
         assert (f["/geometry/index_cell"] == 24 * np.eye(3)).all()
         assert list(f.attrs["k_dims"]) == [3, 3, 3]
+
+
+@pytest.mark.parametrize("n_sweep,ssf_every", [(32, 16), (20, 16), (5, 0), (0, 16)])
+def test_step_host_matches_the_same_calls(n_sweep, ssf_every):
+    """pc_step_host (host spins in and out, the result copy overlapped with the
+    last S(q) sample and the energy on a second stream) against the same work
+    through separate calls: spins, energy, accepted moves and S(q) sums
+    identical, twice in a row (the second call reuses its staging)."""
+    L, T = 8, 0.7
+    kw = dict(J1=1.0, J2=0.1, J3=0.05, B=(0.0, 0.0, 0.5), seed=31, schedule=1)
+    a = pc.pyrochlore_system(L, **kw)
+    b = pc.pyrochlore_system(L, **kw)
+    for s in (a, b):
+        s.ssf_configure(["xx", "zz", "xy"], 1)
+    a.random_spins(2)
+    S_in = np.ascontiguousarray(a.spins_f4())
+    for _ in range(2):
+        S_out = np.zeros_like(S_in)
+        e, acc = a.step_host(S_in, S_out, T, n_sweep, ssf_every, 0 if ssf_every else -1)
+        b.set_spins_f4(S_in)
+        acc_b, done = 0, 0
+        while done < n_sweep:
+            k = min(ssf_every, n_sweep - done) if ssf_every else n_sweep
+            acc_b += int(b.sweep([T], k, 1)[0])
+            done += k
+            if ssf_every and k == ssf_every:
+                b.ssf_sample([0])
+        e_b, _ = b.energy()
+        np.testing.assert_array_equal(S_out, b.spins_f4())
+        assert e == e_b[0]
+        assert acc == acc_b
+        for x, y in zip(a.ssf_read(0), b.ssf_read(0)):
+            np.testing.assert_array_equal(np.asarray(x), np.asarray(y))
+        S_in = S_out
