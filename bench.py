@@ -221,6 +221,29 @@ def run_profile_case(args):
     del s
 
 
+def run_profile_grad(args):
+    """One forward and backward of the gradient form (256 x L=8: energy with
+    its spin gradient, S^zz(q) with its adjoint) after one warm-up, for ncu
+    captures of the gradient kernels."""
+    import torch
+
+    import pyro_cmc_b200 as pc
+    from pyro_cmc_b200 import autograd as ag
+    torch.cuda.set_device(0)
+    B = 256
+    g = pc.pyrochlore_system(8, n_replicas=B, J1=1.0, J2=0.1, J3=-0.05, B=(0.2, 0, 0), seed=3)
+    g.ssf_configure(["zz"], 0, [])
+    g.random_spins(11)
+    spins = ag.spins_tensor(g).clone().requires_grad_(True)
+    w = torch.rand((B, 1, 512), device="cuda", dtype=torch.float64)
+    for _ in range(2):
+        e = ag.energy(g, spins)
+        S = ag.ssf(g, spins)
+        ((w * S[..., 0] ** 2).sum() * 1e-8 + e.sum()).backward()
+    torch.cuda.synchronize()
+    print(f"profile grad: 256 x L=8, launches={g.launch_count()}", flush=True)
+
+
 def cpu_baseline_one_core():
     import oracle
     b = oracle.Bench(WL["L"], WL["J1"], WL["J2"], WL["J3"], WL["B"], 1, seed=3)
@@ -244,6 +267,8 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="run one step of the workload with a fixed tile and no autotuning or warm-up, for ncu "
                          "captures (prints a launch summary, no JSON line)")
+    ap.add_argument("--profile-grad", action="store_true",
+                    help="one warm-up and one forward + backward of the gradient form, for ncu captures (no JSON line)")
     ap.add_argument("--tile", type=int, nargs=3, default=[128, 7, 0], metavar=("THREADS", "CTAS", "VARIANT"),
                     help="tile for --profile-case")
     args = ap.parse_args()
@@ -258,6 +283,9 @@ def main():
         return
     if args.profile_case:
         run_profile_case(args)
+        return
+    if args.profile_grad:
+        run_profile_grad(args)
         return
 
     import numpy as np
