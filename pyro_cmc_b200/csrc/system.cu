@@ -380,6 +380,10 @@ int build_tables(pc_system* s, bool keep_zero, SlTable* out) {
 // each group carries one matrix, the structured kernels apply.
 void build_struct(pc_system* s) {
     s->structured = !s->force_generic;
+    // the structured kernels address a replica's spins with unsigned 32-bit
+    // byte offsets: 16 sublattices x Nc cells x 16 B must stay below 4 GB
+    for (int r = 0; r < s->R; ++r)
+        if (256.0 * double(s->Nc(r)) >= 4294967296.0) s->structured = false;
     s->grad_struct = s->structured && s->specs.size() <= 32;
     std::memset(&s->mats, 0, sizeof(s->mats));
     std::memset(s->spec_mask, 0, sizeof(s->spec_mask));
