@@ -20,8 +20,6 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
-#include <mutex>
-#include <set>
 #include <utility>
 
 #include "common.cuh"
