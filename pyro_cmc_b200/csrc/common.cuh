@@ -68,6 +68,40 @@ __device__ __forceinline__ uint4 site_draw(uint64_t seed, uint32_t replica, uint
                          make_uint2(uint32_t(seed), uint32_t(seed >> 32)));
 }
 
+// The ten round keys of the Weyl schedule for a 64-bit seed (round r:
+// seed + r x (0x9E3779B9, 0xBB67AE85) per 32-bit half), formed once on the
+// host: kernels that take them as parameters read each round's key as an
+// operand instead of adding the schedule constants per site.
+struct PhiloxKeys {
+    uint2 k[10];
+};
+inline PhiloxKeys philox_round_keys(uint64_t seed) {
+    PhiloxKeys rk;
+    uint32_t kx = uint32_t(seed), ky = uint32_t(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        rk.k[r] = make_uint2(kx, ky);
+        kx += 0x9E3779B9u;
+        ky += 0xBB67AE85u;
+    }
+    return rk;
+}
+// philox4x32_10 with the round keys given (same output)
+__device__ __forceinline__ uint4 philox4x32_10_rk(uint4 c, const PhiloxKeys& rk) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ rk.k[r].x, lo1, hi0 ^ c.w ^ rk.k[r].y, lo0);
+    }
+    return c;
+}
+__device__ __forceinline__ uint4 site_draw_rk(const PhiloxKeys& rk, uint32_t replica, uint64_t sweep, uint32_t draw,
+                                              uint32_t site) {
+    return philox4x32_10_rk(make_uint4(site, uint32_t(sweep), draw | (uint32_t(sweep >> 32) << 8), replica), rk);
+}
+
 __device__ __forceinline__ float u24_open0(uint32_t x) { return float((x >> 8) + 1u) * (1.0f / 16777216.0f); }
 __device__ __forceinline__ float u24(uint32_t x) { return float(x >> 8) * (1.0f / 16777216.0f); }
 __device__ __forceinline__ float u24_lowbytes(uint4 w) {

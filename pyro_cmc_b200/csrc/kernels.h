@@ -31,6 +31,7 @@ struct PassArgs {
     const uint64_t* sweep_base;  // device sweep counter
     uint64_t sweep_offset;       // added to *sweep_base
     uint64_t seed;
+    PhiloxKeys rkeys;  // the seed's Philox round keys (philox_round_keys)
     float inv_T_ref;
     float B[3];
     const SlTable* tables;  // 16 sublattice tables (device)

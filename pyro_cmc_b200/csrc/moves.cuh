@@ -349,11 +349,11 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
         const double T = a.T_rep[r];
         sigma = sqrtf(float(T) * a.inv_T_ref);
         invT = float(1.0 / T);
-        w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
+        w = site_draw_rk(a.rkeys, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
     }
     float sn = 0.f, cs = 1.f;
     if (kRot) {
-        const uint4 wo = site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
+        const uint4 wo = site_draw_rk(a.rkeys, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
         sincospif(2.f * u24(wo.x), &sn, &cs);
     } else if (MODE == kOverrelaxTheta) {
         sincosf(float(a.theta[i]), &sn, &cs);

@@ -593,6 +593,7 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.sweep_base = s->d_sweep.p;
     a.sweep_offset = sweep_offset;
     a.seed = s->seed;
+    a.rkeys = pc::philox_round_keys(s->seed);
     a.inv_T_ref = float(1.0 / s->T_ref);
     for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
     a.tables = s->d_tab_active.p;
