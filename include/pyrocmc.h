@@ -24,8 +24,11 @@
  *                unnormalised DFT).
  *   RNG          Philox4x32-10, key = seed, counter = (site, sweep lo32,
  *                draw | sweep hi32 << 8, replica); draw 0 = Metropolis,
- *                2+k = overrelaxation pass k, 250 = random initial state,
- *                251 = replica exchange.
+ *                1 = lifted Metropolis, 2+k = overrelaxation pass k,
+ *                250 = random initial state, 251 = replica exchange. With
+ *                u = top 24 bits / 2^24 of a word: Gaussian pair radius
+ *                sqrt(-2 ln(u + 2^-24)), angles 2 pi (u - 1/2); Metropolis
+ *                acceptance uniform = low bytes of words 0..2 / 2^24.
  */
 #ifndef PYROCMC_H
 #define PYROCMC_H

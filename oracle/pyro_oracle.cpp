@@ -132,9 +132,10 @@ static inline void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in
 // Draw layout shared with the GPU sweep kernels (documented in the C ABI header):
 //   key  = (seed lo32, seed hi32)
 //   ctr  = (site index within replica, sweep lo32, draw | (sweep hi32 << 8), replica)
-//   draw 0: Metropolis -- words 0..3 give two Box-Muller pairs (top 24 bits each),
+//   draw 0: Metropolis -- words 0..3 give two Box-Muller pairs (top 24 bits each:
+//           radius sqrt(-2 ln u) from words 0, 2, angle 2 pi (u - 1/2) from words 1, 3),
 //           the acceptance uniform is the low bytes of words 0,1,2 (24 bits);
-//   draw 2+k: overrelaxation pass k -- word 0's top 24 bits give the angle.
+//   draw 2+k: overrelaxation pass k -- word 0's top 24 bits give the angle 2 pi (u - 1/2).
 static inline void philox_site(uint64_t seed, uint32_t replica, uint64_t sweep, uint32_t draw, uint32_t site,
                                uint32_t out[4]) {
     const uint32_t key[2] = {uint32_t(seed), uint32_t(seed >> 32)};
@@ -520,7 +521,7 @@ struct Runner {
                     philox_site(seed, replica, sweep, 0, site, w);
                     const double r0 = std::sqrt(-2.0 * std::log(u24_open0(w[0])));
                     const double r1 = std::sqrt(-2.0 * std::log(u24_open0(w[2])));
-                    const double t0 = 2 * M_PI * u24(w[1]), t1 = 2 * M_PI * u24(w[3]);
+                    const double t0 = 2 * M_PI * (u24(w[1]) - 0.5), t1 = 2 * M_PI * (u24(w[3]) - 0.5);
                     const vec3 g = {r0 * std::cos(t0), r0 * std::sin(t0), r1 * std::cos(t1)};
                     const double u = u24_lowbytes(w);
                     const vec3 h = sub(local_field(spin), B);
@@ -537,7 +538,7 @@ struct Runner {
                         } else {
                             uint32_t wo[4];
                             philox_site(seed, replica, sweep, 2, site, wo);
-                            rotate_about_vector(spin->S, h, 2 * M_PI * u24(wo[0]));
+                            rotate_about_vector(spin->S, h, 2 * M_PI * (u24(wo[0]) - 0.5));
                         }
                     }
                 }
@@ -554,7 +555,7 @@ struct Runner {
                         } else {
                             uint32_t w[4];
                             philox_site(seed, replica, sweep, uint32_t(2 + k), site, w);
-                            rotate_about_vector(spin->S, h, 2 * M_PI * u24(w[0]));
+                            rotate_about_vector(spin->S, h, 2 * M_PI * (u24(w[0]) - 0.5));
                         }
                     }
         return acc;

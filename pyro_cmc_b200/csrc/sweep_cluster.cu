@@ -92,15 +92,15 @@ __device__ __forceinline__ Proposal cl_prepare(const ClusterArgs& a, const float
     p.cs = 1.f;
     if (kRot) {
         const uint4 wo = site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(or_pass), uint32_t(i));
-        sincospif(2.f * u24(wo.x), &p.sn, &p.cs);
+        uniform_angle(wo.x, &p.sn, &p.cs);
     }
     p.nx = p.ny = p.nz = p.u = 0.f;
     if (kMet) {
-        const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
-        const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
+        const float r0 = bm_radius(w.x);
+        const float r1 = bm_radius(w.z);
         float s_a, c_a, s_b, c_b;
-        sincospif(2.f * u24(w.y), &s_a, &c_a);
-        sincospif(2.f * u24(w.w), &s_b, &c_b);
+        uniform_angle(w.y, &s_a, &c_a);
+        uniform_angle(w.w, &s_b, &c_b);
         float nx = s0.x + sigma * (r0 * c_a);
         float ny = s0.y + sigma * (r0 * s_a);
         float nz = s0.z + sigma * (r1 * c_b);

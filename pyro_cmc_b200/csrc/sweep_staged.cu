@@ -151,11 +151,11 @@ __device__ __forceinline__ unsigned staged_tile(const PassArgs& a, const Tile ti
         const float sigma = sqrtf(float(T) * a.inv_T_ref);
         invT = float(1.0 / T);
         const uint4 w = site_draw(a.seed, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
-        const float r0 = sqrtf(-2.f * logf(u24_open0(w.x)));
-        const float r1 = sqrtf(-2.f * logf(u24_open0(w.z)));
+        const float r0 = bm_radius(w.x);
+        const float r1 = bm_radius(w.z);
         float s_a, c_a, s_b, c_b;
-        sincospif(2.f * u24(w.y), &s_a, &c_a);
-        sincospif(2.f * u24(w.w), &s_b, &c_b);
+        uniform_angle(w.y, &s_a, &c_a);
+        uniform_angle(w.w, &s_b, &c_b);
         nx = s0.x + sigma * (r0 * c_a);
         ny = s0.y + sigma * (r0 * s_a);
         nz = s0.z + sigma * (r1 * c_b);
@@ -169,7 +169,7 @@ __device__ __forceinline__ unsigned staged_tile(const PassArgs& a, const Tile ti
     if (live) {
         if (kRot) {
             const uint4 wo = site_draw(a.seed, uint32_t(r), sweep, kDrawOverrelax0 + uint32_t(a.or_pass), uint32_t(i));
-            sincospif(2.f * u24(wo.x), &sn, &cs);
+            uniform_angle(wo.x, &sn, &cs);
         } else if (MODE == kOverrelaxTheta) {
             sincosf(float(a.theta[i]), &sn, &cs);
         }
