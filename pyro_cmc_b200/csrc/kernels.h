@@ -24,6 +24,9 @@ enum PassMode {
     kLiftedRot = 7   // lifted Metropolis, rotation form (src/MC.cpp:194-244)
 };
 
+// Internal load variant: variant 0 with the isotropic group-matrix path,
+// used by the host when every group matrix is j I.
+constexpr int kVarIso = 5;
 struct PassArgs {
     float4* spins;
     const ReplicaDev* reps;

@@ -314,7 +314,9 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
 //   VAR 0: group by group (six short load batches, fewest registers);
 //   VAR 1: all 30 at once, before the Philox draw and the proposal (which do
 //          not depend on the local field) are computed;
-//   VAR 2: J1 + J2 neighbours (18) before the draw, J3 (12) after it.
+//   VAR 2: J1 + J2 neighbours (18) before the draw, J3 (12) after it;
+//   kVarIso: VAR 0 for systems whose group matrices are all j I (chosen by
+//          the host in place of VAR 0; the same bits, fewer instructions).
 template <int SL, int VAR>
 __device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const PassArgs& a, const ReplicaDev& rep,
                                              const Coords& c, float4 (&v)[kStructNb], int phase) {
@@ -328,6 +330,15 @@ __device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const
             add_group<SL, 3>(h, S, rep.Nc, c, a.mats);
             add_group<SL, 4>(h, S, rep.Nc, c, a.mats);
             add_group<SL, 5>(h, S, rep.Nc, c, a.mats);
+        }
+    } else if constexpr (VAR == kVarIso) {
+        if (phase == 1) {
+            add_group_iso<SL, 0>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 1>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 2>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 3>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 4>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 5>(h, S, rep.Nc, c, a.mats);
         }
     } else if constexpr (VAR == 1) {
         if (phase == 0)

@@ -47,6 +47,8 @@ void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads,
             launch_struct<1>(mode, a, grid, threads, st, pdl);
         else if (a.load_variant == 2)
             launch_struct<2>(mode, a, grid, threads, st, pdl);
+        else if (a.load_variant == kVarIso)
+            launch_struct<kVarIso>(mode, a, grid, threads, st, pdl);
         else
             launch_struct<0>(mode, a, grid, threads, st, pdl);
         return;

@@ -174,6 +174,7 @@ struct pc_system {
     // structured energy gradient: specs per (sublattice, group, bond side) and
     // work items of up to kGradK tiles of one (replica, sublattice)
     bool grad_struct = false;
+    bool all_iso = false;  // every structured group matrix is j I (the isotropic pass variant)
     uint32_t spec_mask[16][pc::kGroups][2] = {};
     DevBuf<int4> d_grad_items;
     int n_grad_items = 0;
@@ -385,6 +386,7 @@ void build_struct(pc_system* s) {
     for (int r = 0; r < s->R; ++r)
         if (256.0 * double(s->Nc(r)) >= 4294967296.0) s->structured = false;
     s->grad_struct = s->structured && s->specs.size() <= 32;
+    s->all_iso = true;
     std::memset(&s->mats, 0, sizeof(s->mats));
     std::memset(s->spec_mask, 0, sizeof(s->spec_mask));
     for (int sl = 0; sl < 16 && s->structured; ++sl) {
@@ -442,9 +444,14 @@ void build_struct(pc_system* s) {
                 }
             for (int i = 0; i < 9; ++i) s->mats.M[sl][g][i] = float(E[b][i]);
             if (nonzero) s->mats.active[sl] |= 1u << g;
+            const float* m = s->mats.M[sl][g];
+            if (!(m[1] == 0.f && m[2] == 0.f && m[3] == 0.f && m[5] == 0.f && m[6] == 0.f && m[7] == 0.f &&
+                  m[4] == m[0] && m[8] == m[0]))
+                s->all_iso = false;
         }
     }
     s->grad_struct = s->grad_struct && s->structured;
+    s->all_iso = s->all_iso && s->structured;
 }
 
 // Colour classes from the active bonds: sublattices joined by a nonzero bond
@@ -606,6 +613,7 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.or_pass = or_pass;
     a.structured = s->structured ? 1 : 0;
     a.load_variant = use_staged(s) ? 3 : (s->load_variant == 3 ? 0 : s->load_variant);
+    if (a.load_variant == 0 && s->all_iso) a.load_variant = pc::kVarIso;
     a.mats = s->mats;
     a.staged_rl = s->staged_rl;
     a.err = s->d_err.p;
