@@ -25,7 +25,7 @@ enum PassMode {
 };
 
 // Internal load variant: variant 0 with the isotropic group-matrix path,
-// used by the host when every group matrix is j I.
+// used by the host when every group matrix is j I with j != 0.
 constexpr int kVarIso = 5;
 struct PassArgs {
     float4* spins;

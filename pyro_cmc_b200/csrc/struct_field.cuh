@@ -71,21 +71,20 @@ __device__ __forceinline__ void add_group(float3& h, const float4* __restrict__ 
     }
 }
 
-// add_group for a group whose matrix is j I (every group of a system with
-// isotropic couplings: J2, J3, and J1 with Delta = 1): three multiplies and
-// three adds instead of nine multiply-adds and three adds. add_group gives
-// the same bits on such a matrix: its two zero terms add exact zeros to the
-// rounded j t, and the sum is added to h unfused, as here.
+// add_group for a group whose matrix is j I, j != 0 (every group of a system
+// with nonzero isotropic couplings: J2, J3, and J1 with Delta = 1): three
+// multiplies and three adds instead of nine multiply-adds and three adds, and
+// no test of the group's activity. add_group gives the same bits on such a
+// matrix: its two zero terms add exact zeros to the rounded j t, and the sum
+// is added to h unfused, as here.
 template <int SL, int G>
 __device__ __forceinline__ void add_group_iso(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                               const PyroMats& mats) {
-    if (mats.active[SL] & (1u << G)) {
-        const float3 t = group_sum<SL, G>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
-        const float j = mats.M[SL][G][0];
-        h.x = __fadd_rn(h.x, __fmul_rn(j, t.x));
-        h.y = __fadd_rn(h.y, __fmul_rn(j, t.y));
-        h.z = __fadd_rn(h.z, __fmul_rn(j, t.z));
-    }
+    const float3 t = group_sum<SL, G>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
+    const float j = mats.M[SL][G][0];
+    h.x = __fadd_rn(h.x, __fmul_rn(j, t.x));
+    h.y = __fadd_rn(h.y, __fmul_rn(j, t.y));
+    h.z = __fadd_rn(h.z, __fmul_rn(j, t.z));
 }
 
 __device__ __forceinline__ Coords cell_coords(int cell, int L, uint64_t divL) {

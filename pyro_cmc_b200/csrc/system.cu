@@ -174,7 +174,7 @@ struct pc_system {
     // structured energy gradient: specs per (sublattice, group, bond side) and
     // work items of up to kGradK tiles of one (replica, sublattice)
     bool grad_struct = false;
-    bool all_iso = false;  // every structured group matrix is j I (the isotropic pass variant)
+    bool all_iso = false;  // every structured group matrix is j I, j != 0 (the isotropic pass variant)
     uint32_t spec_mask[16][pc::kGroups][2] = {};
     DevBuf<int4> d_grad_items;
     int n_grad_items = 0;
@@ -446,8 +446,8 @@ void build_struct(pc_system* s) {
             if (nonzero) s->mats.active[sl] |= 1u << g;
             const float* m = s->mats.M[sl][g];
             if (!(m[1] == 0.f && m[2] == 0.f && m[3] == 0.f && m[5] == 0.f && m[6] == 0.f && m[7] == 0.f &&
-                  m[4] == m[0] && m[8] == m[0]))
-                s->all_iso = false;
+                  m[4] == m[0] && m[8] == m[0] && m[0] != 0.f))
+                s->all_iso = false;  // the isotropic variant also assumes every group active
         }
     }
     s->grad_struct = s->grad_struct && s->structured;
