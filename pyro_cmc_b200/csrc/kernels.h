@@ -103,6 +103,7 @@ struct EnergyArgs {
     float B[3];
     double* partial;  // [n_tiles][4] by tile index: sum (0.5 S.h - S.B), sum S
     int structured;
+    int iso;  // every group matrix is j I with j != 0 (the isotropic variant)
     PyroMats mats;
 };
 void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st);

@@ -166,37 +166,45 @@ __host__ __device__ constexpr bool group_has_upper(int sl, int g) {
         if (nb_sl(sl, e) > sl) return true;
     return false;
 }
-template <int SL, int G, int... K>
+// ISO: every group matrix is j I with j != 0 (as add_group_iso: no activity
+// test, three multiplies and three unfused adds per group, the same bits).
+template <int SL, int G, bool ISO, int... K>
 __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                                 const PyroMats& mats, std::integer_sequence<int, K...>) {
     if constexpr (group_has_upper(SL, G)) {
-        if (mats.active[SL] & (1u << G)) {
+        if (ISO || (mats.active[SL] & (1u << G))) {
             constexpr int B = grp_begin(SL, G);
             float3 t = make_float3(0.f, 0.f, 0.f);
             (add_upper<SL, B + K>(t, S, Nc, c), ...);
             const float* J = mats.M[SL][G];
-            h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
-            h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
-            h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+            if constexpr (ISO) {
+                h.x = __fadd_rn(h.x, __fmul_rn(J[0], t.x));
+                h.y = __fadd_rn(h.y, __fmul_rn(J[0], t.y));
+                h.z = __fadd_rn(h.z, __fmul_rn(J[0], t.z));
+            } else {
+                h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
+                h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
+                h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+            }
         }
     }
 }
-template <int SL, int G>
+template <int SL, int G, bool ISO>
 __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                                 const PyroMats& mats) {
-    add_group_upper<SL, G>(h, S, Nc, c, mats, std::make_integer_sequence<int, grp_size(SL, G)>{});
+    add_group_upper<SL, G, ISO>(h, S, Nc, c, mats, std::make_integer_sequence<int, grp_size(SL, G)>{});
 }
-template <int SL>
+template <int SL, bool ISO = false>
 __device__ __forceinline__ float3 struct_field_upper(const float4* __restrict__ S, const PyroMats& mats, int cell,
                                                      int L, int Nc, uint64_t divL) {
     const Coords c = cell_coords(cell, L, divL);
     float3 h = make_float3(0.f, 0.f, 0.f);
-    add_group_upper<SL, 0>(h, S, Nc, c, mats);
-    add_group_upper<SL, 1>(h, S, Nc, c, mats);
-    add_group_upper<SL, 2>(h, S, Nc, c, mats);
-    add_group_upper<SL, 3>(h, S, Nc, c, mats);
-    add_group_upper<SL, 4>(h, S, Nc, c, mats);
-    add_group_upper<SL, 5>(h, S, Nc, c, mats);
+    add_group_upper<SL, 0, ISO>(h, S, Nc, c, mats);
+    add_group_upper<SL, 1, ISO>(h, S, Nc, c, mats);
+    add_group_upper<SL, 2, ISO>(h, S, Nc, c, mats);
+    add_group_upper<SL, 3, ISO>(h, S, Nc, c, mats);
+    add_group_upper<SL, 4, ISO>(h, S, Nc, c, mats);
+    add_group_upper<SL, 5, ISO>(h, S, Nc, c, mats);
     return h;
 }
 

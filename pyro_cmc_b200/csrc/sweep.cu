@@ -127,11 +127,13 @@ __global__ void __launch_bounds__(512) energy_partials_kernel(const __grid_const
     }
 }
 
-template <int SL>
+template <int SL, bool ISO>
 __device__ __forceinline__ float3 struct_field_e(const EnergyArgs& a, const float4* S, const ReplicaDev& rep, int cell) {
-    return struct_field_upper<SL>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
+    return struct_field_upper<SL, ISO>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
 }
 
+// ISO: every group matrix is j I, j != 0 (the host's all_iso)
+template <bool ISO>
 __global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constant__ EnergyArgs a) {
     __shared__ double red[4 * 32];
     for (int u = blockIdx.x; u < a.n_tiles; u += gridDim.x) {
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constan
             const int cell = tile.z + int(threadIdx.x);
             const float4 s0 = S[size_t(sl) * rep.Nc + cell];
             float3 h = make_float3(0.f, 0.f, 0.f);
-#define PC_CALL(K) h = struct_field_e<K>(a, S, rep, cell)
+#define PC_CALL(K) h = struct_field_e<K, ISO>(a, S, rep, cell)
             PC_SL_SWITCH(sl, PC_CALL)
 #undef PC_CALL
             // h: the bonds to higher sublattices only, each bond counted once
@@ -165,8 +167,13 @@ void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st) {
     // one CTA per tile: many resident CTAs per SM hide the neighbour-gather latency
     const int grid = a.n_tiles;
     if (a.structured && threads <= 256) {
-        prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel));
-        energy_struct_kernel<<<grid, threads, 0, st>>>(a);
+        if (a.iso) {
+            prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel<true>));
+            energy_struct_kernel<true><<<grid, threads, 0, st>>>(a);
+        } else {
+            prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel<false>));
+            energy_struct_kernel<false><<<grid, threads, 0, st>>>(a);
+        }
     } else {
         prefer_l1(reinterpret_cast<const void*>(energy_partials_kernel));
         energy_partials_kernel<<<grid, threads, 0, st>>>(a);

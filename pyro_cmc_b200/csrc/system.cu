@@ -802,6 +802,7 @@ int enqueue_energy(pc_system* s) {
     for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
     a.partial = s->d_partial.p;
     a.structured = s->structured ? 1 : 0;
+    a.iso = s->all_iso ? 1 : 0;
     a.mats = s->mats;
     pc::launch_energy_partials(a, s->threads, s->stream);
     PC_LAUNCH_CK();
