@@ -24,9 +24,11 @@ enum PassMode {
     kLiftedRot = 7   // lifted Metropolis, rotation form (src/MC.cpp:194-244)
 };
 
-// Internal load variant: variant 0 with the isotropic group-matrix path,
-// used by the host when every group matrix is j I with j != 0.
-constexpr int kVarIso = 5;
+// Internal load variants: variant 0 with the isotropic group-matrix path and
+// no per-group activity test, used by the host when every group matrix is
+// j I with j != 0 (kVarIso), or when that holds for every group but the J2
+// group, whose matrix is 0 everywhere (kVarIsoNoJ2: J2 = 0).
+constexpr int kVarIso = 5, kVarIsoNoJ2 = 6;
 struct PassArgs {
     float4* spins;
     const ReplicaDev* reps;
@@ -103,7 +105,7 @@ struct EnergyArgs {
     float B[3];
     double* partial;  // [n_tiles][4] by tile index: sum (0.5 S.h - S.B), sum S
     int structured;
-    int iso;  // every group matrix is j I with j != 0 (the isotropic variant)
+    int iso;  // 1: every group matrix is j I with j != 0; 2: so but the J2 group, which is 0
     PyroMats mats;
 };
 void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st);

@@ -315,8 +315,9 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
 //   VAR 1: all 30 at once, before the Philox draw and the proposal (which do
 //          not depend on the local field) are computed;
 //   VAR 2: J1 + J2 neighbours (18) before the draw, J3 (12) after it;
-//   kVarIso: VAR 0 for systems whose group matrices are all j I (chosen by
-//          the host in place of VAR 0; the same bits, fewer instructions).
+//   kVarIso, kVarIsoNoJ2: VAR 0 for systems whose group matrices are all j I
+//          (or all but a zero J2 group), chosen by the host in place of VAR 0:
+//          the same bits, fewer instructions, no per-group branches.
 template <int SL, int VAR>
 __device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const PassArgs& a, const ReplicaDev& rep,
                                              const Coords& c, float4 (&v)[kStructNb], int phase) {
@@ -331,12 +332,12 @@ __device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const
             add_group<SL, 4>(h, S, rep.Nc, c, a.mats);
             add_group<SL, 5>(h, S, rep.Nc, c, a.mats);
         }
-    } else if constexpr (VAR == kVarIso) {
+    } else if constexpr (VAR == kVarIso || VAR == kVarIsoNoJ2) {
         if (phase == 1) {
             add_group_iso<SL, 0>(h, S, rep.Nc, c, a.mats);
             add_group_iso<SL, 1>(h, S, rep.Nc, c, a.mats);
             add_group_iso<SL, 2>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 3>(h, S, rep.Nc, c, a.mats);
+            if constexpr (VAR == kVarIso) add_group_iso<SL, 3>(h, S, rep.Nc, c, a.mats);
             add_group_iso<SL, 4>(h, S, rep.Nc, c, a.mats);
             add_group_iso<SL, 5>(h, S, rep.Nc, c, a.mats);
         }

@@ -166,12 +166,13 @@ __host__ __device__ constexpr bool group_has_upper(int sl, int g) {
         if (nb_sl(sl, e) > sl) return true;
     return false;
 }
-// ISO: every group matrix is j I with j != 0 (as add_group_iso: no activity
-// test, three multiplies and three unfused adds per group, the same bits).
-template <int SL, int G, bool ISO, int... K>
+// ISO 1: every group matrix is j I with j != 0; ISO 2: so but the J2 group
+// (group 3), which is 0 and skipped (as add_group_iso: no activity test,
+// three multiplies and three unfused adds per group, the same bits).
+template <int SL, int G, int ISO, int... K>
 __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                                 const PyroMats& mats, std::integer_sequence<int, K...>) {
-    if constexpr (group_has_upper(SL, G)) {
+    if constexpr (group_has_upper(SL, G) && !(ISO == 2 && G == 3)) {
         if (ISO || (mats.active[SL] & (1u << G))) {
             constexpr int B = grp_begin(SL, G);
             float3 t = make_float3(0.f, 0.f, 0.f);
@@ -189,12 +190,12 @@ __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restr
         }
     }
 }
-template <int SL, int G, bool ISO>
+template <int SL, int G, int ISO>
 __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                                 const PyroMats& mats) {
     add_group_upper<SL, G, ISO>(h, S, Nc, c, mats, std::make_integer_sequence<int, grp_size(SL, G)>{});
 }
-template <int SL, bool ISO = false>
+template <int SL, int ISO = 0>
 __device__ __forceinline__ float3 struct_field_upper(const float4* __restrict__ S, const PyroMats& mats, int cell,
                                                      int L, int Nc, uint64_t divL) {
     const Coords c = cell_coords(cell, L, divL);

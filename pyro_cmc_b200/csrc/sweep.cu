@@ -49,6 +49,8 @@ void launch_colour_pass(PassMode mode, const PassArgs& a, int grid, int threads,
             launch_struct<2>(mode, a, grid, threads, st, pdl);
         else if (a.load_variant == kVarIso)
             launch_struct<kVarIso>(mode, a, grid, threads, st, pdl);
+        else if (a.load_variant == kVarIsoNoJ2)
+            launch_struct<kVarIsoNoJ2>(mode, a, grid, threads, st, pdl);
         else
             launch_struct<0>(mode, a, grid, threads, st, pdl);
         return;
@@ -127,13 +129,13 @@ __global__ void __launch_bounds__(512) energy_partials_kernel(const __grid_const
     }
 }
 
-template <int SL, bool ISO>
+template <int SL, int ISO>
 __device__ __forceinline__ float3 struct_field_e(const EnergyArgs& a, const float4* S, const ReplicaDev& rep, int cell) {
     return struct_field_upper<SL, ISO>(S, a.mats, cell, rep.L, rep.Nc, rep.divL);
 }
 
-// ISO: every group matrix is j I, j != 0 (the host's all_iso)
-template <bool ISO>
+// ISO: EnergyArgs::iso (0 general, 1 all groups j I, 2 all but a zero J2 group)
+template <int ISO>
 __global__ void __launch_bounds__(256) energy_struct_kernel(const __grid_constant__ EnergyArgs a) {
     __shared__ double red[4 * 32];
     for (int u = blockIdx.x; u < a.n_tiles; u += gridDim.x) {
@@ -167,12 +169,15 @@ void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st) {
     // one CTA per tile: many resident CTAs per SM hide the neighbour-gather latency
     const int grid = a.n_tiles;
     if (a.structured && threads <= 256) {
-        if (a.iso) {
-            prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel<true>));
-            energy_struct_kernel<true><<<grid, threads, 0, st>>>(a);
+        if (a.iso == 1) {
+            prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel<1>));
+            energy_struct_kernel<1><<<grid, threads, 0, st>>>(a);
+        } else if (a.iso == 2) {
+            prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel<2>));
+            energy_struct_kernel<2><<<grid, threads, 0, st>>>(a);
         } else {
-            prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel<false>));
-            energy_struct_kernel<false><<<grid, threads, 0, st>>>(a);
+            prefer_l1(reinterpret_cast<const void*>(energy_struct_kernel<0>));
+            energy_struct_kernel<0><<<grid, threads, 0, st>>>(a);
         }
     } else {
         prefer_l1(reinterpret_cast<const void*>(energy_partials_kernel));

@@ -174,7 +174,7 @@ struct pc_system {
     // structured energy gradient: specs per (sublattice, group, bond side) and
     // work items of up to kGradK tiles of one (replica, sublattice)
     bool grad_struct = false;
-    bool all_iso = false;  // every structured group matrix is j I, j != 0 (the isotropic pass variant)
+    int iso_kind = 0;  // 1: every group matrix j I, j != 0; 2: so but a zero J2 group (isotropic variants)
     uint32_t spec_mask[16][pc::kGroups][2] = {};
     DevBuf<int4> d_grad_items;
     int n_grad_items = 0;
@@ -386,7 +386,8 @@ void build_struct(pc_system* s) {
     for (int r = 0; r < s->R; ++r)
         if (256.0 * double(s->Nc(r)) >= 4294967296.0) s->structured = false;
     s->grad_struct = s->structured && s->specs.size() <= 32;
-    s->all_iso = true;
+    bool iso_nz[pc::kGroups], zero[pc::kGroups];  // per group, over all sublattices
+    for (int g = 0; g < pc::kGroups; ++g) iso_nz[g] = zero[g] = true;
     std::memset(&s->mats, 0, sizeof(s->mats));
     std::memset(s->spec_mask, 0, sizeof(s->spec_mask));
     for (int sl = 0; sl < 16 && s->structured; ++sl) {
@@ -447,11 +448,15 @@ void build_struct(pc_system* s) {
             const float* m = s->mats.M[sl][g];
             if (!(m[1] == 0.f && m[2] == 0.f && m[3] == 0.f && m[5] == 0.f && m[6] == 0.f && m[7] == 0.f &&
                   m[4] == m[0] && m[8] == m[0] && m[0] != 0.f))
-                s->all_iso = false;  // the isotropic variant also assumes every group active
+                iso_nz[g] = false;
+            if (nonzero) zero[g] = false;
         }
     }
     s->grad_struct = s->grad_struct && s->structured;
-    s->all_iso = s->all_iso && s->structured;
+    bool others = true;  // every group but J2 (group 3) isotropic and nonzero
+    for (int g = 0; g < pc::kGroups; ++g)
+        if (g != 3) others = others && iso_nz[g];
+    s->iso_kind = !s->structured ? 0 : (others && iso_nz[3]) ? 1 : (others && zero[3]) ? 2 : 0;
 }
 
 // Colour classes from the active bonds: sublattices joined by a nonzero bond
@@ -613,7 +618,7 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.or_pass = or_pass;
     a.structured = s->structured ? 1 : 0;
     a.load_variant = use_staged(s) ? 3 : (s->load_variant == 3 ? 0 : s->load_variant);
-    if (a.load_variant == 0 && s->all_iso) a.load_variant = pc::kVarIso;
+    if (a.load_variant == 0 && s->iso_kind) a.load_variant = s->iso_kind == 1 ? pc::kVarIso : pc::kVarIsoNoJ2;
     a.mats = s->mats;
     a.staged_rl = s->staged_rl;
     a.err = s->d_err.p;
@@ -802,7 +807,7 @@ int enqueue_energy(pc_system* s) {
     for (int i = 0; i < 3; ++i) a.B[i] = float(s->B[i]);
     a.partial = s->d_partial.p;
     a.structured = s->structured ? 1 : 0;
-    a.iso = s->all_iso ? 1 : 0;
+    a.iso = s->iso_kind;
     a.mats = s->mats;
     pc::launch_energy_partials(a, s->threads, s->stream);
     PC_LAUNCH_CK();
