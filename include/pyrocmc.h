@@ -304,8 +304,9 @@ int pc_energy_noalloc(const void* spins_dev, int L, const double* params, void* 
 
 /* Times the sweep over the candidate tile shapes (threads per CTA x CTAs per
  * SM) and neighbour-load variants on this system, and the cluster-resident
- * sweep where it applies, and keeps the fastest (spin state and sweep counter
- * are saved and restored). */
+ * sweep where it applies, then launch overlap off and on for the chosen tile,
+ * and keeps the fastest (spin state and sweep counter are saved and
+ * restored). */
 int pc_autotune(pc_system* sys);
 /* How the structured kernels issue the 30 neighbour loads of a site:
  * 0 group by group (fewest registers), 1 all at once, 2 in two batches, 3 staged:
@@ -344,13 +345,13 @@ int pc_lt_minimum(int L, double J1, double J2, double J3, double Delta, double* 
                   int64_t* k_star, double* eigvec);
 /* Enables per-kernel CUDA-event timing (off by default). */
 int pc_set_kernel_timing(pc_system* sys, int on);
-/* Launch overlap of consecutive colour passes (off by default): with 1 each
- * pass is launched with programmatic dependent launch and waits in-kernel for
- * the previous kernel's completion before reading spins, so its launch
- * overlaps the previous pass's last CTAs. Measured on B200 at L=64 it gains
- * nothing over plain stream order (and loses a few % once the S(q) kernels are
- * loaded), hence the default. Results are identical either way. No
- * counterpart in the reference (a launch setting). */
+/* Launch overlap of consecutive colour passes (off by default; pc_autotune
+ * turns it on where it is faster): with 1 each pass is launched with
+ * programmatic dependent launch and waits in-kernel for the previous kernel's
+ * completion before reading spins, so its launch overlaps the previous pass's
+ * last CTAs. Measured on B200: 3-4 % faster sweeps for L = 8..32, nothing at
+ * L = 64. Results are identical either way. No counterpart in the reference
+ * (a launch setting). */
 int pc_set_launch_overlap(pc_system* sys, int on);
 /* Cluster-resident sweeps (off by default; pc_autotune turns them on where
  * they are faster): for replicas of one size L <= 16, one thread-block cluster

@@ -2112,14 +2112,37 @@ int pc_autotune(pc_system* sys) {
         }
         sys->cluster_sweep = ms < best_ms;
     }
-    sys->timing = timing;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     sys->threads = best_t;
     sys->ctas_per_sm = best_c;
     sys->load_variant = best_v;
     rc = build_tiles(sys);
     if (rc) return rc;
+    // launch overlap of the colour passes, off and on, on the chosen tile (it
+    // pays where passes are short: small lattices); the same moves either way
+    if (!sys->cluster_sweep) {
+        float ms_pdl[2] = {1e30f, 1e30f};
+        for (int on = 0; on < 2; ++on) {
+            sys->pdl = on != 0;
+            sys->drop_graphs();
+            rc = run_sweeps(sys, 2, 1);
+            if (rc) return rc;
+            for (int rep = 0; rep < 3; ++rep) {
+                PC_CK(cudaEventRecord(e0, sys->stream));
+                rc = run_sweeps(sys, 4, 1);
+                if (rc) return rc;
+                PC_CK(cudaEventRecord(e1, sys->stream));
+                PC_CK(cudaEventSynchronize(e1));
+                float t = 0.f;
+                PC_CK(cudaEventElapsedTime(&t, e0, e1));
+                ms_pdl[on] = std::min(ms_pdl[on], t);
+            }
+        }
+        sys->pdl = ms_pdl[1] < ms_pdl[0];
+        sys->drop_graphs();
+    }
+    sys->timing = timing;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     PC_CK(cudaMemcpyAsync(sys->d_spins.p, saved.p, bytes, cudaMemcpyDeviceToDevice, sys->stream));
     PC_CK(cudaMemcpyAsync(sys->d_sweep.p, &sweep0, sizeof(uint64_t), cudaMemcpyHostToDevice, sys->stream));
     PC_CK(cudaStreamSynchronize(sys->stream));
