@@ -244,6 +244,28 @@ def run_profile_grad(args):
     print(f"profile grad: 256 x L=8, launches={g.launch_count()}", flush=True)
 
 
+def run_profile_batched(args):
+    """The batched tempering form (128 replicas, L in {8,12,16,24} x 32 T,
+    exchange every 10 sweeps, S(q) every 16) with a fixed tile and no
+    autotuning: 4 rounds of 10 sweeps, for ncu launch lists."""
+    import numpy as np
+    import torch
+
+    import pyro_cmc_b200 as pc
+    torch.cuda.set_device(0)
+    Ls = [8] * 32 + [12] * 32 + [16] * 32 + [24] * 32
+    T = np.concatenate([np.geomspace(2.0, 0.02, 32)] * 4)
+    b = pc.pyrochlore_system(Ls, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=7, schedule=WL["schedule"])
+    b.set_tile(args.tile[0], args.tile[1])
+    b.set_load_variant(args.tile[2])
+    b.random_spins(5)
+    b.pt_configure(T)
+    b.ssf_configure(["xx", "yy", "zz"], len(Ls), sorted(Ls))
+    b.pt_run(4, 10, 16)
+    torch.cuda.synchronize()
+    print(f"profile batched: 128 replicas, tile={args.tile}, launches={b.launch_count()}", flush=True)
+
+
 def cpu_baseline_one_core():
     import oracle
     b = oracle.Bench(WL["L"], WL["J1"], WL["J2"], WL["J3"], WL["B"], 1, seed=3)
@@ -267,6 +289,8 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="run one step of the workload with a fixed tile and no autotuning or warm-up, for ncu "
                          "captures (prints a launch summary, no JSON line)")
+    ap.add_argument("--profile-batched", action="store_true",
+                    help="4 tempering rounds of the batched form with a fixed tile, for ncu captures (no JSON line)")
     ap.add_argument("--profile-grad", action="store_true",
                     help="one warm-up and one forward + backward of the gradient form, for ncu captures (no JSON line)")
     ap.add_argument("--tile", type=int, nargs=3, default=[128, 7, 0], metavar=("THREADS", "CTAS", "VARIANT"),
@@ -286,6 +310,9 @@ def main():
         return
     if args.profile_grad:
         run_profile_grad(args)
+        return
+    if args.profile_batched:
+        run_profile_batched(args)
         return
 
     import numpy as np
