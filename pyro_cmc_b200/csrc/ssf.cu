@@ -639,7 +639,9 @@ void launch_plane(const SsfGeom& g, const float4* spins, const ReplicaDev* reps,
     switch (g.L) {
         case 64: ssf_plane_kernel<64, true, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
         case 32: ssf_plane_kernel<32, true, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+        case 24: ssf_plane_kernel<24, false, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
         case 16: ssf_plane_kernel<16, true, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
+        case 12: ssf_plane_kernel<12, false, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
         case 8: ssf_plane_kernel<8, false, RES><<<grid, threads, smem, st>>>(g, spins, reps, G); break;
         default:
             if (g.L % 16 == 0)
@@ -773,7 +775,9 @@ void launch_ssf_z(const SsfGeom& g, const float2* G, const SsfOut& o, cudaStream
         switch (L) {
             case 64: ssf_line_kernel<64><<<grid, threads, smem, st>>>(g, G, o); break;
             case 32: ssf_line_kernel<32><<<grid, threads, smem, st>>>(g, G, o); break;
+            case 24: ssf_line_kernel<24><<<grid, threads, smem, st>>>(g, G, o); break;
             case 16: ssf_line_kernel<16><<<grid, threads, smem, st>>>(g, G, o); break;
+            case 12: ssf_line_kernel<12><<<grid, threads, smem, st>>>(g, G, o); break;
             case 8: ssf_line_kernel<8><<<grid, threads, smem, st>>>(g, G, o); break;
             default: ssf_line_kernel<0><<<grid, threads, smem, st>>>(g, G, o);
         }
@@ -890,6 +894,8 @@ void prepare_plane(int smem_max) {
     cudaFuncSetAttribute(ssf_plane_kernel<32, true, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_plane_kernel<16, true, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_plane_kernel<8, false, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<12, false, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_plane_kernel<24, false, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_plane_kernel<0, true, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_plane_kernel<0, false, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
 }
@@ -907,6 +913,8 @@ void ssf_prepare() {
     cudaFuncSetAttribute(ssf_line_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ssf_line_kernel<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_adj_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     cudaFuncSetAttribute(ssf_line_adj_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);

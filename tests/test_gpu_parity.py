@@ -302,12 +302,13 @@ def test_ssf_matches_oracle(L):
         assert np.abs(got - ref).max() <= REL * scale, (name, np.abs(got - ref).max() / scale)
 
 
-@pytest.mark.parametrize("L", [11, 16, 32, 64])
+@pytest.mark.parametrize("L", [11, 12, 16, 24, 32, 64])
 def test_ssf_large_L_matches_fft_restatement(L):
     """S(q) of random spins at sizes beyond the direct-sum oracle: L = 11
-    (a prime line length, the runtime-radix path), 16 / 32 / 64 (the swizzled
-    shared-memory layout; 64 is the field-cool size), against the numpy-FFT
-    restatement of ssf_manager::sample."""
+    (a prime line length, the runtime-radix path), 12 and 24 (the tempering
+    ladder sizes, unswizzled), 16 / 32 / 64 (the swizzled shared-memory
+    layout; 64 is the field-cool size), against the numpy-FFT restatement of
+    ssf_manager::sample."""
     from oracle import ssf_fft
     g = pc.pyrochlore_system(L, **COUPLINGS[0])
     g.ssf_configure(CORR9, 1)
