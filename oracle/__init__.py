@@ -7,8 +7,10 @@ include/ssf_manager.hpp, src/temper.cpp). Only ``tests/``,
 ``--impl reference`` arm) may import this package, and only as the checker or
 the CPU baseline. The product (``pyro_cmc_b200``) never imports it.
 
-Parity status: pinned by the reference's own geometry tables and by draws of
-the reference's own RNG header (tests/golden/), plus analytic known answers.
+Parity status: pinned on the reference's own src/MC.cpp, compiled unchanged
+into oracle/_ref/libref_mc.so (``oracle.ref``; tests/test_oracle_ref.py and the
+fixture tests/golden/ref_mc_chains.npz), on the reference's geometry tables and
+RNG header draws (tests/golden/), and on analytic known answers.
 The lattice_lib conventions (DFT sign, flat-k order) are assumptions: parity
 for the sign of Im S^{ab}(q) of off-diagonal correlators is unpinned.
 """

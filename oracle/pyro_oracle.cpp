@@ -5,8 +5,14 @@
 // the checker and the CPU baseline. Nothing in the product links, loads or calls
 // this file.
 //
-// Parity status: the reference itself cannot be compiled here (lattice_lib,
-// FFTW3, HDF5, argparse and Eigen are absent), so this restatement is pinned by
+// Parity status: pinned on the reference's own code. oracle/make_ref.sh
+// compiles the reference's src/MC.cpp unchanged (against the lattice_lib /
+// HDF5 stand-ins in oracle/ref_shim/) into oracle/_ref/libref_mc.so, and
+// tests/test_oracle_ref.py checks this restatement against it: positions and
+// bond shells exactly, energy and local field to FP64 rounding, and whole
+// sequential Metropolis + overrelaxation and lifted chains from the same
+// Xoroshiro seed with identical accepted counts (committed as
+// tests/golden/ref_mc_chains.npz). Further pins:
 // (1) the reference's own geometry tables, parsed from
 //     include/pyrochlore_geometry.hpp into tests/golden/geometry_tables.json,
 // (2) Xoroshiro128++/SplitMix64 streams and libstdc++ distribution draws
@@ -50,6 +56,8 @@ using ipos = std::array<int64_t, 3>;
 static inline vec3 add(const vec3& a, const vec3& b) { return {a[0] + b[0], a[1] + b[1], a[2] + b[2]}; }
 static inline vec3 sub(const vec3& a, const vec3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
 static inline vec3 scale(double s, const vec3& a) { return {s * a[0], s * a[1], s * a[2]}; }
+// v /= s of the reference's vec3 (a division per component, not a multiply by 1/s)
+static inline vec3 vdiv(const vec3& a, double s) { return {a[0] / s, a[1] / s, a[2] / s}; }
 static inline double dot(const vec3& a, const vec3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 static inline vec3 cross(const vec3& a, const vec3& b) {
     return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
@@ -355,11 +363,16 @@ struct Runner {
     size_t local_Metropolis(double T, Spin* spin) {
         const vec3 h = sub(local_field(spin), B);
         const double curr_E = dot(spin->S, h);
-        const double g0 = normal_dist(rng), g1 = normal_dist(rng), g2 = normal_dist(rng);
+        // vector3::vec3d(normal_dist(rng), normal_dist(rng), normal_dist(rng)):
+        // the order in which a constructor's arguments are evaluated is
+        // unspecified in C++; GCC on x86-64 evaluates them right to left, so the
+        // reference as built draws the z component first. Pinned against the
+        // reference's own MC.cpp compiled here (oracle/_ref/libref_mc.so).
+        const double g2 = normal_dist(rng), g1 = normal_dist(rng), g0 = normal_dist(rng);
         vec3 nS = scale(std::sqrt(T / T_ref), vec3{g0, g1, g2});
         nS = add(nS, spin->S);
         const double n = std::sqrt(dot(nS, nS));
-        nS = scale(1.0 / n, nS);
+        nS = vdiv(nS, n);
         const double dE = dot(nS, h) - curr_E;
         if (dE < 0 || rand01(rng) < std::exp(-dE / T)) {
             spin->S = nS;
@@ -389,7 +402,7 @@ struct Runner {
     // E ~ Exp(1), keep the azimuth; out of [-1, 1] or at a pole: flip dir.
     bool lifted_u_move(double T, Spin* spin, const vec3& h, double e1, double u01) const {
         const double curr_E = dot(spin->S, h);
-        const vec3 hh = scale(1.0 / std::sqrt(dot(h, h)), h);
+        const vec3 hh = vdiv(h, std::sqrt(dot(h, h)));
         const double u = dot(hh, spin->S);
         const double du = spin->lifted_dir * std::sqrt(T / T_ref) * e1;
         const double nu = u + du;
@@ -398,7 +411,7 @@ struct Runner {
             return false;
         }
         vec3 nS = add(scale(nu, hh), scale(std::sqrt((1 - nu * nu) / (1 - u * u)), sub(spin->S, scale(u, hh))));
-        nS = scale(1.0 / std::sqrt(dot(nS, nS)), nS);
+        nS = vdiv(nS, std::sqrt(dot(nS, nS)));
         const double dE = dot(nS, h) - curr_E;
         if (u01 < std::exp(-dE / T)) {
             spin->S = nS;
@@ -421,7 +434,7 @@ struct Runner {
         }
         vec3 nS = spin->S;
         rotate_about_vector(nS, axis, spin->lifted_dir * delta);
-        nS = scale(1.0 / std::sqrt(dot(nS, nS)), nS);
+        nS = vdiv(nS, std::sqrt(dot(nS, nS)));
         const vec3 axis_new = cross(nS, h);
         const double n2_new = dot(axis_new, axis_new);
         if (dot(axis, axis_new) < 0) {
@@ -441,7 +454,7 @@ struct Runner {
     size_t local_lifted_Metropolis(double T, Spin* spin) {
         const vec3 h = sub(local_field(spin), B);
         const double e1 = exp_dist(rng);
-        const vec3 hh = scale(1.0 / std::sqrt(dot(h, h)), h);
+        const vec3 hh = vdiv(h, std::sqrt(dot(h, h)));
         const double u = dot(hh, spin->S);
         const double nu = u + spin->lifted_dir * std::sqrt(T / T_ref) * e1;
         if (nu > 1 || nu < -1 || std::abs(1 - u * u) < 1e-16) {
@@ -460,7 +473,7 @@ struct Runner {
         }
         vec3 nS = spin->S;
         rotate_about_vector(nS, axis, spin->lifted_dir * std::sqrt(T / T_ref));
-        nS = scale(1.0 / std::sqrt(dot(nS, nS)), nS);
+        nS = vdiv(nS, std::sqrt(dot(nS, nS)));
         if (dot(axis, cross(nS, h)) < 0) {
             spin->lifted_dir = int8_t(-spin->lifted_dir);
             return 0;

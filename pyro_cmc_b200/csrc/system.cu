@@ -2187,6 +2187,15 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     }
     int done = 0;
     bool copying = false;
+    // once the result copy is enqueued, every return (error paths included)
+    // waits for it: the caller may reuse or free S4_out as soon as we return
+    struct CopyWait {
+        const bool& active;
+        cudaStream_t s;
+        ~CopyWait() {
+            if (active) cudaStreamSynchronize(s);
+        }
+    } copy_wait{copying, sys->copy_stream};
     while (done < n_sweep || !copying) {
         const int chunk = do_ssf ? std::min(ssf_every, n_sweep - done) : n_sweep - done;
         if (chunk > 0) {

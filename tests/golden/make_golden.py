@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Regenerates the golden fixtures in tests/golden/ from the reference tree.
 
-Run in a container that has the reference mounted (default /root/reference,
-override with PYRO_REFERENCE_DIR). Nothing under tests/ reads the reference at
+Run in a container that has the reference tree, named by the environment
+variable PYRO_REFERENCE_DIR (required). Nothing under tests/ reads the reference at
 test time: the tests read only the JSON files this script writes.
 
 * geometry_tables.json -- the reference's own integer tables, parsed as text
@@ -24,7 +24,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("PYRO_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("PYRO_REFERENCE_DIR", "")
 
 
 def _strip_comments(src):
@@ -106,6 +106,8 @@ PHILOX_KAT = [
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        sys.exit("set PYRO_REFERENCE_DIR to the reference tree")
     geo = parse_geometry(os.path.join(REF, "include", "pyrochlore_geometry.hpp"))
     geo["_source"] = "include/pyrochlore_geometry.hpp (parsed as text by tests/golden/make_golden.py)"
     with open(os.path.join(HERE, "geometry_tables.json"), "w") as f:
