@@ -2,14 +2,13 @@
 // any device allocation (pc_energy_noalloc in include/pyrocmc.h).
 //
 // Who needs it: callers that must not call cudaMalloc or cudaFree. Examples:
-// a thread that is capturing a CUDA graph in global capture mode (allocation
-// calls are illegal there), a program whose device memory is owned by a
-// framework's caching allocator (a cudaMalloc behind its back fragments the
-// pool, and cudaFree synchronises the whole device), or a tight loop that
-// cannot afford that implicit synchronisation. The regular entry points keep
-// their scratch in buffers allocated with the system; this one keeps its
-// scratch -- the per-tile partial sums of the reduction -- in a fixed array
-// compiled into the library.
+// a program whose device memory is owned by a framework's caching allocator
+// (a cudaMalloc behind its back fragments the pool and can fail once the pool
+// has taken the free memory), or a tight loop that cannot afford the implicit
+// device-wide synchronisation of cudaFree. The regular entry points keep their
+// scratch in buffers allocated with the system; this one keeps its scratch --
+// the per-tile partial sums of the reduction -- in a fixed array compiled into
+// the library.
 //
 // Limits and sharing:
 //  * L <= 64 (4,194,304 spins): 16 sublattices x L^3/256 tiles x 4 doubles
@@ -19,8 +18,12 @@
 //    contents there; each call overwrites every partial it reads, so nothing
 //    needs to start at zero. Two calls whose kernels overlap on the GPU (for
 //    example on two streams) race on the array and give wrong results.
-//  * The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress; make that first call before any stream capture.
+//  * The array's device address is looked up with cudaGetSymbolAddress by the
+//    first call in each CUDA context (the first call on a device, and the
+//    first call after that device's context was destroyed and re-created,
+//    e.g. by cudaDeviceReset, which reloads the module at a new address).
+//    Make that first call before any stream capture.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -137,17 +140,65 @@ __global__ void __launch_bounds__(kTileCells) noalloc_energy_sum(const __grid_co
 }
 
 std::mutex g_mu;
-double* g_scratch[kMaxDevices] = {};
+// Per device: the context the address was looked up in, and the address.
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;
+    bool valid = false;
+    double* ptr = nullptr;
+};
+ScratchAddr g_scratch[kMaxDevices];
 
 int noalloc_fail(int code, const std::string& msg) {
     pc::set_last_error(msg);
     return code;
 }
 
+// Identity of the calling thread's current context on `dev`. The driver
+// entry points are fetched through the runtime, so the library does not
+// link against libcuda. A thread that has not yet made a runtime call has no
+// current context: cudaSetDevice binds (and if needed creates) the primary
+// context of `dev`, which the following runtime calls would use anyway.
+int current_context_id(int dev, unsigned long long* id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        cudaError_t e1 = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+        cudaError_t e2 = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+            q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+            return noalloc_fail(PC_ERR_CUDA, "pc_energy_noalloc: driver entry points cuCtxGetCurrent/cuCtxGetId "
+                                             "not available");
+        get_current = reinterpret_cast<GetCurrent>(f1);
+        get_id = reinterpret_cast<GetId>(f2);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return noalloc_fail(PC_ERR_CUDA, "pc_energy_noalloc: cuCtxGetCurrent failed");
+    if (!ctx) {
+        const cudaError_t e = cudaSetDevice(dev);
+        if (e != cudaSuccess)
+            return noalloc_fail(PC_ERR_CUDA, std::string("pc_energy_noalloc: cudaSetDevice: ") + cudaGetErrorString(e));
+        if (get_current(&ctx) != CUDA_SUCCESS || !ctx)
+            return noalloc_fail(PC_ERR_CUDA, "pc_energy_noalloc: no current CUDA context");
+    }
+    if (get_id(ctx, id) != CUDA_SUCCESS) return noalloc_fail(PC_ERR_CUDA, "pc_energy_noalloc: cuCtxGetId failed");
+    return PC_OK;
+}
+
 }  // namespace
 
 extern "C" int pc_energy_noalloc(const void* spins_dev, int L, const double* params, void* out_dev, void* stream) {
     if (!spins_dev || !params || !out_dev) return noalloc_fail(PC_ERR_INVALID, "pc_energy_noalloc: null argument");
+    // the kernels read float4 spins and write doubles: misaligned pointers
+    // (e.g. an offset view into a larger buffer) are rejected, not faulted on
+    if (reinterpret_cast<uintptr_t>(spins_dev) % 16 != 0)
+        return noalloc_fail(PC_ERR_INVALID, "pc_energy_noalloc: spins_dev is not 16-byte aligned (float4 spins)");
+    if (reinterpret_cast<uintptr_t>(out_dev) % 8 != 0)
+        return noalloc_fail(PC_ERR_INVALID, "pc_energy_noalloc: out_dev is not 8-byte aligned (doubles)");
     if (L < 1 || L > kNoallocMaxL)
         return noalloc_fail(PC_ERR_INVALID, "pc_energy_noalloc: L = " + std::to_string(L) +
                                                 " is outside 1..64, the size its fixed scratch array holds");
@@ -158,17 +209,23 @@ extern "C" int pc_energy_noalloc(const void* spins_dev, int L, const double* par
     double* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch[dev]) {
-            // once per device: the host-side symbol is only a stand-in, the
-            // kernels need the array's device address
+        unsigned long long ctx_id = 0;
+        const int rc = current_context_id(dev, &ctx_id);
+        if (rc) return rc;
+        ScratchAddr& slot = g_scratch[dev];
+        if (!slot.valid || slot.ctx_id != ctx_id) {
+            // once per context: the host-side symbol is only a stand-in, the
+            // kernels need the array's device address in this context
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_partials);
             if (e != cudaSuccess)
                 return noalloc_fail(PC_ERR_CUDA, std::string("pc_energy_noalloc: cudaGetSymbolAddress: ") +
                                                      cudaGetErrorString(e));
-            g_scratch[dev] = static_cast<double*>(p);
+            slot.ptr = static_cast<double*>(p);
+            slot.ctx_id = ctx_id;
+            slot.valid = true;
         }
-        scratch = g_scratch[dev];
+        scratch = slot.ptr;
     }
     NoallocArgs a;
     std::memset(&a, 0, sizeof(a));
