@@ -59,6 +59,7 @@ def lib():
         l.orc_set_spins.argtypes = [_P, _DP]
         l.orc_get_spins.argtypes = [_P, _DP]
         l.orc_random_spins.argtypes = [_P, _U64]
+        l.orc_reseed.argtypes = [_P, _U64]
         l.orc_set_field.argtypes = [_P, _DP]
         l.orc_positions.argtypes = [_P, _I64P, _I32P]
         l.orc_neighbours.argtypes = [_P, _I, _I, _I32P]
@@ -84,7 +85,7 @@ def lib():
         l.orc_ssf.argtypes = [_P, _I32P, _I, _I, _DP, _DP]
         l.orc_T_profile.argtypes = [_D, _D, _DP, _I, _I, _DP, _I32P, _I]
         l.orc_anneal.argtypes = [_P, _D, _D, _DP, _I, _I, _I, _I, _I, _I32P, _I, _DP, _DP, _DP, _DP, _I]
-        l.orc_temper.argtypes = [_I, _D, _D, _D, _D, _DP, _D, _U64, _DP, _I, _I, _I, _I, _I, _DP, _DP, _U64P, _U64P]
+        l.orc_temper.argtypes = [_I, _D, _D, _D, _D, _DP, _D, _U64, _DP, _I, _I, _I, _I, _I, _I, _DP, _DP, _U64P, _U64P]
         l.orc_bench_create.restype = _P
         l.orc_bench_create.argtypes = [_I, _D, _D, _D, _DP, _I, _U64]
         l.orc_bench_run.restype = _D
@@ -143,6 +144,11 @@ class System:
 
     def random_spins(self, seed):
         lib().orc_random_spins(self._h, seed)
+
+    def reseed(self, seed):
+        """Restart the runner's Xoroshiro stream from `seed` (a new chain on
+        the same lattice, without rebuilding the bond shells)."""
+        lib().orc_reseed(self._h, seed)
 
     def set_field(self, B):
         Bv = _arr(B, np.float64)
@@ -260,7 +266,11 @@ def T_profile(T_hot, T_cold, T_sample, total_steps):
 
 
 def temper(L, T, J1=1.0, J2=0.0, J3=0.0, Delta=1.0, B=(0, 0, 0), T_ref=1.0, seed=0, n_burn_in=100,
-           n_rounds=100, n_sweep=10, init_random=True):
+           n_rounds=100, n_sweep=10, init_random=True, n_burn_rounds=0):
+    """src/temper.cpp's tempering emulated in one process: n_burn_in sweeps
+    per replica without exchanges, n_burn_rounds unmeasured rounds with
+    exchanges, then n_rounds measured rounds. Returns per-slot sums of e and
+    e^2 and the exchange attempts / accepts of each pair (slot, slot + 1)."""
     Tv = _arr(T, np.float64)
     R = len(Tv)
     Bv = _arr(B, np.float64)
@@ -268,7 +278,8 @@ def temper(L, T, J1=1.0, J2=0.0, J3=0.0, Delta=1.0, B=(0, 0, 0), T_ref=1.0, seed
     e2 = np.empty(R)
     att = np.empty(R, dtype=np.uint64)
     acc = np.empty(R, dtype=np.uint64)
-    rc = lib().orc_temper(L, J1, J2, J3, Delta, _dp(Bv), T_ref, seed, _dp(Tv), R, n_burn_in, n_rounds, n_sweep,
+    rc = lib().orc_temper(L, J1, J2, J3, Delta, _dp(Bv), T_ref, seed, _dp(Tv), R, n_burn_in, n_burn_rounds, n_rounds,
+                          n_sweep,
                           int(init_random), _dp(es), _dp(e2), att.ctypes.data_as(_U64P), acc.ctypes.data_as(_U64P))
     if rc:
         raise RuntimeError(lib().orc_last_error().decode())

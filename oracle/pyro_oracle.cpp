@@ -696,6 +696,52 @@ static void ssf_sublattice(const Lattice& lat, const std::vector<std::pair<int, 
         }
 }
 
+// Separable form: the same per-sublattice DFT over cells as ssf_sublattice,
+// done as three passes of 1-D DFTs along x, y and z (O(Nc L) per sublattice
+// and component instead of O(Nc^2)), then the phase contraction written as
+// S^{ab}(K) = conj(B^a(K)) B^b(K) with B^a(K) = sum_mu exp(-i q.r_mu) A^a_mu(K)
+// (the mu-nu double sum of ssf_sublattice factorises). Used by the anneal
+// protocol at larger L; equal to ssf_direct to FP64 rounding (tested).
+static void ssf_separable(const Lattice& lat, const std::vector<std::pair<int, int>>& corr, double* out) {
+    const int L = lat.L, nk = lat.Nc;
+    std::vector<cplx> w(static_cast<size_t>(L));
+    for (int m = 0; m < L; ++m) w[size_t(m)] = cplx(std::cos(-2 * M_PI * m / L), std::sin(-2 * M_PI * m / L));
+    const double q0 = 2 * M_PI / (8.0 * L);
+    std::vector<cplx> Bk(size_t(3) * nk, cplx(0, 0));
+    std::vector<cplx> A(static_cast<size_t>(nk)), tmp(static_cast<size_t>(nk));
+    for (int a = 0; a < 3; ++a)
+        for (int sl = 0; sl < 16; ++sl) {
+            for (int cell = 0; cell < nk; ++cell) A[size_t(cell)] = lat.spins[size_t(sl) * nk + cell].S[a];
+            // axis d: stride 1 (x), L (y), L*L (z)
+            for (int d = 0; d < 3; ++d) {
+                const int stride = d == 0 ? 1 : (d == 1 ? L : L * L);
+                for (int base = 0; base < nk; ++base) {
+                    if ((base / stride) % L != 0) continue;  // base = start of a line along d
+                    for (int K = 0; K < L; ++K) {
+                        cplx acc = 0;
+                        for (int n = 0; n < L; ++n) acc += w[size_t((K * n) % L)] * A[size_t(base + n * stride)];
+                        tmp[size_t(base + K * stride)] = acc;
+                    }
+                }
+                std::swap(A, tmp);
+            }
+            for (int Kz = 0; Kz < L; ++Kz)
+                for (int Ky = 0; Ky < L; ++Ky)
+                    for (int Kx = 0; Kx < L; ++Kx) {
+                        const double ph = -q0 * (Kx * double(lat.r_sl[size_t(sl)][0]) + Ky * double(lat.r_sl[size_t(sl)][1]) +
+                                                 Kz * double(lat.r_sl[size_t(sl)][2]));
+                        const int k = (Kx * L + Ky) * L + Kz;
+                        Bk[size_t(a) * nk + k] += cplx(std::cos(ph), std::sin(ph)) * A[size_t(Kx + L * (Ky + L * Kz))];
+                    }
+        }
+    for (size_t c = 0; c < corr.size(); ++c)
+        for (int k = 0; k < nk; ++k) {
+            const cplx v = std::conj(Bk[size_t(corr[c].first) * nk + k]) * Bk[size_t(corr[c].second) * nk + k];
+            out[(c * nk + k) * 2] = v.real();
+            out[(c * nk + k) * 2 + 1] = v.imag();
+        }
+}
+
 // generate_T_profile (include/cli_bits.hpp:250-289)
 static std::pair<std::vector<double>, std::set<size_t>> generate_T_profile(double T_hot, double T_cold,
                                                                           std::vector<double> T_sample,
@@ -787,6 +833,16 @@ void orc_get_spins(void* h, double* S) {
         for (int a = 0; a < 3; ++a) S[3 * i + a] = sp[i].S[a];
 }
 void orc_random_spins(void* h, uint64_t seed) { random_unit_spins(static_cast<System*>(h)->lat, seed); }
+// A fresh MC_runner stream on the same lattice: Xoroshiro128++ re-seeded and
+// the distributions' cached state cleared (normal_distribution keeps the
+// second value of each polar pair), as if the runner were constructed anew.
+void orc_reseed(void* h, uint64_t seed) {
+    auto& mc = static_cast<System*>(h)->mc;
+    mc.rng = Xoroshiro128pp(seed);
+    mc.normal_dist.reset();
+    mc.rand01.reset();
+    mc.exp_dist.reset();
+}
 void orc_set_field(void* h, const double* B) { static_cast<System*>(h)->mc.B = {B[0], B[1], B[2]}; }
 
 void orc_positions(void* h, int64_t* pos, int32_t* sl) {
@@ -943,6 +999,8 @@ void orc_ssf(void* h, const int32_t* corr, int n_corr, int mode, double* out, do
     for (int i = 0; i < n_corr; ++i) c.push_back({corr[2 * i], corr[2 * i + 1]});
     if (mode == 0)
         ssf_direct(s->lat, c, out);
+    else if (mode == 2)
+        ssf_separable(s->lat, c, out);
     else
         ssf_sublattice(s->lat, c, out, resolved);
 }
@@ -991,7 +1049,7 @@ int orc_anneal(void* h, double T_hot, double T_cold, const double* T_sample, int
             for (int smp = 0; smp < n_samp; ++smp) {
                 for (int n = 0; n < n_sweep; ++n) s->mc.sweep_local_Metropolis(T, 1);
                 if (n_corr > 0) {
-                    ssf_direct(s->lat, c, tmp.data());
+                    ssf_separable(s->lat, c, tmp.data());
                     for (size_t j = 0; j < size_t(n_corr) * nk * 2; ++j) {
                         sum[j] += tmp[j];
                         sq[j] += tmp[j] * tmp[j];
@@ -1013,9 +1071,12 @@ int orc_anneal(void* h, double T_hot, double T_cold, const double* T_sample, int
 // sweep per round, :426-429: pass n_sweep+1 for that), then one energy sample
 // per slot, then the exchange. e_sum/e2_sum per temperature slot;
 // attempts/accepts per lower slot of each pair.
+// n_burn_in sweeps per replica without exchanges, then n_burn_rounds full
+// rounds (sweeps, energy, exchange) whose statistics are discarded, then the
+// n_rounds measured rounds; the pair parity counts every round.
 int orc_temper(int L, double J1, double J2, double J3, double Delta, const double* B, double T_ref, uint64_t seed,
-               const double* T, int R, int n_burn_in, int n_rounds, int n_sweep, int init_random, double* e_sum,
-               double* e2_sum, uint64_t* attempts, uint64_t* accepts) {
+               const double* T, int R, int n_burn_in, int n_burn_rounds, int n_rounds, int n_sweep, int init_random,
+               double* e_sum, double* e2_sum, uint64_t* attempts, uint64_t* accepts) {
     try {
         std::vector<std::unique_ptr<System>> sys;
         std::vector<Xoroshiro128pp> swap_rng;
@@ -1037,20 +1098,23 @@ int orc_temper(int L, double J1, double J2, double J3, double Delta, const doubl
             for (int i = 0; i < n_burn_in; ++i) sys[r]->mc.sweep_local_Metropolis(T[r], 1);
         const double Np = double(sys[0]->lat.Nc);
         std::vector<double> e(static_cast<size_t>(R));
-        for (int round = 0; round < n_rounds; ++round) {
+        for (int round = 0; round < n_burn_rounds + n_rounds; ++round) {
+            const bool measured = round >= n_burn_rounds;
             for (int r = 0; r < R; ++r) {
                 for (int sw = 0; sw < n_sweep; ++sw) sys[r]->mc.sweep_local_Metropolis(T[r], 1);
                 e[r] = sys[r]->mc.total_energy_per_unit_cell();
-                e_sum[r] += e[r];
-                e2_sum[r] += e[r] * e[r];
+                if (measured) {
+                    e_sum[r] += e[r];
+                    e2_sum[r] += e[r] * e[r];
+                }
             }
             const int start = round % 2;
             for (int r = start; r + 1 < R; r += 2) {
                 const double arg = (1.0 / T[r] - 1.0 / T[r + 1]) * (e[r] * Np - e[r + 1] * Np);
                 const bool acc = arg >= 0.0 || rand01(swap_rng[r]) < std::exp(arg);
-                attempts[r]++;
+                if (measured) attempts[r]++;
                 if (acc) {
-                    accepts[r]++;
+                    if (measured) accepts[r]++;
                     for (size_t i = 0; i < sys[r]->lat.spins.size(); ++i)
                         std::swap(sys[r]->lat.spins[i].S, sys[r + 1]->lat.spins[i].S);
                 }

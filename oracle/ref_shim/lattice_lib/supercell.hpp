@@ -14,7 +14,8 @@
 //  * Supercell<T> built by build_supercell(cell, L*I): objects stored
 //    sublattice-major, objects[sl * Nc + cell] with cell = cx + L*(cy + L*cz)
 //    and ipos = cell_object.ipos + a*(cx, cy, cz) (a = cell side, 8);
-//    get_object_at wraps positions periodically (mod a*L).
+//    get_object_at wraps positions periodically (mod a*L): the residues mod a
+//    identify the sublattice, the exact quotient the cell.
 // Only diagonal supercells (L*I) are supported.
 //
 // Which `abs` the unqualified call in MC.cpp's local_lifted_Metropolis
@@ -35,7 +36,6 @@
 #include <cstdint>
 #include <stdexcept>
 #include <tuple>
-#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -176,7 +176,7 @@ struct Supercell {
     SupercellLattice lattice;
     std::tuple<std::vector<T>> objects;
     std::tuple<SlPos<T>> sl_positions;
-    std::unordered_map<int64_t, size_t> index_of;
+    std::vector<int> sl_of_mod;  // [a^3]: sublattice of a position by its residues mod a, -1 if none
 
     template <typename U>
     std::vector<U>& get_objects() {
@@ -188,17 +188,19 @@ struct Supercell {
     }
     size_t size() const { return std::get<0>(objects).size(); }
 
-    int64_t key(const ipos_t& x) const {
-        const int64_t n = lattice.a * lattice.L;
-        int64_t w[3];
-        for (int i = 0; i < 3; ++i) w[i] = ((x[size_t(i)] % n) + n) % n;
-        return (w[0] * n + w[1]) * n + w[2];
+    static int64_t pmod(int64_t v, int64_t m) { return ((v % m) + m) % m; }
+    int64_t index_of(const ipos_t& x) const {
+        const int64_t a = lattice.a, L = lattice.L;
+        const int sl = sl_of_mod[size_t((pmod(x[0], a) * a + pmod(x[1], a)) * a + pmod(x[2], a))];
+        if (sl < 0) throw std::out_of_range("get_object_at: no object at this position");
+        const ipos_t& r = std::get<0>(sl_positions)[size_t(sl)];
+        int64_t c[3];
+        for (int i = 0; i < 3; ++i) c[i] = pmod((x[size_t(i)] - r[size_t(i)]) / a, L);  // exact division
+        return int64_t(sl) * L * L * L + c[0] + L * (c[1] + L * c[2]);
     }
     template <typename U>
     U* get_object_at(const ipos_t& x) {
-        auto it = index_of.find(key(x));
-        if (it == index_of.end()) throw std::out_of_range("get_object_at: no object at this position");
-        return &std::get<std::vector<U>>(objects)[it->second];
+        return &std::get<std::vector<U>>(objects)[size_t(index_of(x))];
     }
 };
 
@@ -213,15 +215,18 @@ Supercell<T> build_supercell(const UnitCellSpecifier<T>& cell, const imat33_t& s
     sc.lattice.a = cell.cell(0, 0);
     auto& objs = std::get<0>(sc.objects);
     auto& slp = std::get<0>(sc.sl_positions);
-    const int64_t Nc = L * L * L;
+    const int64_t a = sc.lattice.a, Nc = L * L * L;
+    sc.sl_of_mod.assign(size_t(a * a * a), -1);
     objs.reserve(size_t(Nc) * cell.objects.size());
     for (const T& proto : cell.objects) {
-        slp.push_back(proto.ipos);
+        const ipos_t& r = proto.ipos;
+        sc.sl_of_mod[size_t((Supercell<T>::pmod(r[0], a) * a + Supercell<T>::pmod(r[1], a)) * a +
+                            Supercell<T>::pmod(r[2], a))] = int(slp.size());
+        slp.push_back(r);
         for (int64_t c = 0; c < Nc; ++c) {
             const int64_t cx = c % L, cy = (c / L) % L, cz = c / (L * L);
             T o = proto;
-            o.ipos = proto.ipos + ipos_t{sc.lattice.a * cx, sc.lattice.a * cy, sc.lattice.a * cz};
-            sc.index_of[sc.key(o.ipos)] = objs.size();
+            o.ipos = r + ipos_t{a * cx, a * cy, a * cz};
             objs.push_back(std::move(o));
         }
     }

@@ -9,7 +9,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpyrocmc.so")
 SOURCES = ["system.cu", "sweep.cu", "sweep_lifted.cu", "sweep_staged.cu", "sweep_cluster.cu", "grad.cu", "ssf.cu",
-           "pt.cu", "noalloc.cu", "lt.cu", "merge.cu"]
+           "pt.cu", "noalloc.cu", "lt.cu", "merge.cu", "energy_cell.cu"]
 HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh", "struct_field.cuh", "moves.cuh", "dft.cuh"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,258 @@
+// energy_cell.cu -- energy per cubic cell and magnetisation with one thread
+// per cubic cell (total_energy_per_unit_cell, src/MC.cpp:305-312).
+//
+// The reference sums 0.5 S_i.h_i - S_i.B over sites, i.e. every bond twice
+// from its two ends. Here every bond is counted once, by one of its ends: a
+// thread owns the 16 sites of one cubic cell and the bonds from them whose cell
+// offset to the other end is "forward" (dz > 0; else dy > 0; else dx > 0; a
+// bond inside the cell belongs to its lower sublattice). The matrix seen from
+// the other end is the transpose, so the bond energy S_i.J S_j is the same
+// from either end and the sum equals the reference's.
+//
+// Why per cell: of the 240 bonds a cell owns, 78 join two of its own sites
+// (read once, kept in registers) and the other 162 reach only 48 distinct
+// sites of neighbouring cells (pyro_struct.cuh's offsets: 9 forward cell
+// offsets with 4 or 8 target sublattices each). A cell therefore issues 16 + 48
+// coalesced float4 loads instead of the 16 x 16 of a per-site thread that
+// gathers its neighbours on higher sublattices. Consecutive threads take
+// consecutive cells along x, so every load of a warp is a 512-byte row segment.
+//
+// Bond energies accumulate in FP32 (four sums per cell, as the per-site
+// local field of the other kernels is FP32), the field and magnetisation
+// terms and everything above the cell in FP64; per-CTA FP64 partials are summed per replica
+// in fixed order by energy_finalize_kernel (deterministic).
+#include <cuda_runtime.h>
+
+#include <utility>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "struct_field.cuh"
+
+namespace pc {
+
+__host__ __device__ constexpr bool bond_owned(int sl, int e) {
+    const int dx = nb_dx(sl, e), dy = nb_dy(sl, e), dz = nb_dz(sl, e);
+    if (dz != 0) return dz > 0;
+    if (dy != 0) return dy > 0;
+    if (dx != 0) return dx > 0;
+    return sl < nb_sl(sl, e);
+}
+
+constexpr int kMaxIntra = 128;
+constexpr int kMaxTargets = 64;
+constexpr int kMaxRemote = 256;
+
+struct CellBonds {
+    int n_intra;
+    int isl[kMaxIntra], is2[kMaxIntra], ig[kMaxIntra];  // own site, other own site, group (of isl)
+    int n_tgt;
+    int ts2[kMaxTargets], tdx[kMaxTargets], tdy[kMaxTargets], tdz[kMaxTargets];
+    int tb[kMaxTargets + 1];  // bonds of target t: [tb[t], tb[t+1]) of the remote list
+    int n_rem;
+    int rsl[kMaxRemote], rg[kMaxRemote];  // own site and group of each remote bond
+};
+
+__host__ __device__ constexpr int target_key(int s2, int dx, int dy, int dz) {
+    return (((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1)) * 16 + s2;
+}
+
+__host__ __device__ constexpr CellBonds make_cell_bonds() {
+    CellBonds b{};
+    int key[kMaxRemote] = {};
+    // intra-cell bonds in (sl, e) order; remote bonds collected with their key
+    for (int sl = 0; sl < 16; ++sl)
+        for (int e = 0; e < kStructNb; ++e) {
+            if (!bond_owned(sl, e)) continue;
+            const int dx = nb_dx(sl, e), dy = nb_dy(sl, e), dz = nb_dz(sl, e);
+            const int g = group_of(sl, e);
+            if (dx == 0 && dy == 0 && dz == 0) {
+                b.isl[b.n_intra] = sl;
+                b.is2[b.n_intra] = nb_sl(sl, e);
+                b.ig[b.n_intra] = g;
+                ++b.n_intra;
+            } else {
+                key[b.n_rem] = target_key(nb_sl(sl, e), dx, dy, dz);
+                b.rsl[b.n_rem] = sl;
+                b.rg[b.n_rem] = g;
+                ++b.n_rem;
+            }
+        }
+    // stable insertion sort of the remote bonds by target: increasing
+    // (dz, dy, dx, s2), and (sl, e) order inside one target
+    for (int i = 1; i < b.n_rem; ++i) {
+        const int k = key[i], sl = b.rsl[i], g = b.rg[i];
+        int j = i - 1;
+        while (j >= 0 && key[j] > k) {
+            key[j + 1] = key[j];
+            b.rsl[j + 1] = b.rsl[j];
+            b.rg[j + 1] = b.rg[j];
+            --j;
+        }
+        key[j + 1] = k;
+        b.rsl[j + 1] = sl;
+        b.rg[j + 1] = g;
+    }
+    for (int i = 0; i < b.n_rem; ++i)
+        if (i == 0 || key[i] != key[i - 1]) {
+            const int k = key[i];
+            b.ts2[b.n_tgt] = k % 16;
+            b.tdx[b.n_tgt] = (k / 16) % 3 - 1;
+            b.tdy[b.n_tgt] = (k / 48) % 3 - 1;
+            b.tdz[b.n_tgt] = k / 144 - 1;
+            b.tb[b.n_tgt] = i;
+            ++b.n_tgt;
+        }
+    b.tb[b.n_tgt] = b.n_rem;
+    return b;
+}
+
+constexpr CellBonds kCB = make_cell_bonds();
+static_assert(kCB.n_intra <= kMaxIntra && kCB.n_tgt <= kMaxTargets && kCB.n_rem <= kMaxRemote, "cell bond tables");
+static_assert(2 * (kCB.n_intra + kCB.n_rem) == 16 * kStructNb, "every bond owned by exactly one end");
+
+__host__ __device__ constexpr int cb_n_intra() { return kCB.n_intra; }
+__host__ __device__ constexpr int cb_n_tgt() { return kCB.n_tgt; }
+__host__ __device__ constexpr int cb_isl(int k) { return kCB.isl[k]; }
+__host__ __device__ constexpr int cb_is2(int k) { return kCB.is2[k]; }
+__host__ __device__ constexpr int cb_ig(int k) { return kCB.ig[k]; }
+__host__ __device__ constexpr int cb_ts2(int t) { return kCB.ts2[t]; }
+__host__ __device__ constexpr int cb_tdx(int t) { return kCB.tdx[t]; }
+__host__ __device__ constexpr int cb_tdy(int t) { return kCB.tdy[t]; }
+__host__ __device__ constexpr int cb_tdz(int t) { return kCB.tdz[t]; }
+__host__ __device__ constexpr int cb_tb(int t) { return kCB.tb[t]; }
+__host__ __device__ constexpr int cb_rsl(int k) { return kCB.rsl[k]; }
+__host__ __device__ constexpr int cb_rg(int k) { return kCB.rg[k]; }
+
+// Bond energies accumulate in kAcc FP32 sums per cell (site sl into sum
+// sl % kAcc): fewer live registers than one sum per site.
+constexpr int kAcc = 4;
+
+// acc += S_SL . M[SL][G] n  (ISO: M = j I; ISO 2: the J2 group is zero and skipped)
+template <int SL, int G, int ISO>
+__device__ __forceinline__ void bond_term(float (&acc)[kAcc], const float3 (&own)[16], const float3& n,
+                                          const PyroMats& mats) {
+    if constexpr (ISO == 2 && G == 3) {
+        return;
+    } else if constexpr (ISO != 0) {
+        const float d = own[SL].x * n.x + own[SL].y * n.y + own[SL].z * n.z;
+        acc[SL % kAcc] = fmaf(mats.M[SL][G][0], d, acc[SL % kAcc]);
+    } else {
+        const float* J = mats.M[SL][G];
+        const float tx = J[0] * n.x + J[1] * n.y + J[2] * n.z;
+        const float ty = J[3] * n.x + J[4] * n.y + J[5] * n.z;
+        const float tz = J[6] * n.x + J[7] * n.y + J[8] * n.z;
+        acc[SL % kAcc] += own[SL].x * tx + own[SL].y * ty + own[SL].z * tz;
+    }
+}
+
+template <int ISO, int... K>
+__device__ __forceinline__ void intra_bonds(float (&acc)[kAcc], const float3 (&own)[16], const PyroMats& mats,
+                                            std::integer_sequence<int, K...>) {
+    (bond_term<cb_isl(K), cb_ig(K), ISO>(acc, own, own[cb_is2(K)], mats), ...);
+}
+
+template <int T, int ISO, int... K>
+__device__ __forceinline__ void target_bonds(float (&acc)[kAcc], const float3 (&own)[16], const float3& n,
+                                             const PyroMats& mats, std::integer_sequence<int, K...>) {
+    (bond_term<cb_rsl(cb_tb(T) + K), cb_rg(cb_tb(T) + K), ISO>(acc, own, n, mats), ...);
+}
+
+template <int T>
+__device__ __forceinline__ float3 load_target(const char* base, uint32_t sl_bytes, const Coords& c) {
+    const uint32_t off = uint32_t(cb_ts2(T)) * sl_bytes + uint32_t(pick<cb_tdx(T)>(c.x)) +
+                         uint32_t(pick<cb_tdy(T)>(c.y)) + uint32_t(pick<cb_tdz(T)>(c.z));
+    const float4 v = __ldg(reinterpret_cast<const float4*>(base + off));
+    return make_float3(v.x, v.y, v.z);
+}
+
+// Targets [T0, T0 + sizeof...(K)) loaded together (one round trip), then their bonds.
+template <int T0, int ISO, int... K>
+__device__ __forceinline__ void target_batch(float (&acc)[kAcc], const float3 (&own)[16], const char* base,
+                                             uint32_t sl_bytes, const Coords& c, const PyroMats& mats,
+                                             std::integer_sequence<int, K...>) {
+    const float3 n[sizeof...(K)] = {load_target<T0 + K>(base, sl_bytes, c)...};
+    (target_bonds<T0 + K, ISO>(acc, own, n[K], mats,
+                               std::make_integer_sequence<int, cb_tb(T0 + K + 1) - cb_tb(T0 + K)>{}),
+     ...);
+}
+
+constexpr int kTargetBatch = 8;
+
+template <int T0, int ISO>
+__device__ __forceinline__ void remote_bonds(float (&acc)[kAcc], const float3 (&own)[16], const char* base,
+                                             uint32_t sl_bytes, const Coords& c, const PyroMats& mats) {
+    if constexpr (T0 < cb_n_tgt()) {
+        constexpr int n = (cb_n_tgt() - T0) < kTargetBatch ? (cb_n_tgt() - T0) : kTargetBatch;
+        target_batch<T0, ISO>(acc, own, base, sl_bytes, c, mats, std::make_integer_sequence<int, n>{});
+        remote_bonds<T0 + n, ISO>(acc, own, base, sl_bytes, c, mats);
+    }
+}
+
+template <int... SL>
+__device__ __forceinline__ void load_own(float3 (&own)[16], const char* base, uint32_t sl_bytes, const Coords& c,
+                                         std::integer_sequence<int, SL...>) {
+    const float4 v[16] = {__ldg(reinterpret_cast<const float4*>(base + uint32_t(SL) * sl_bytes + uint32_t(c.x[1]) +
+                                                                uint32_t(c.y[1]) + uint32_t(c.z[1])))...};
+    ((own[SL] = make_float3(v[SL].x, v[SL].y, v[SL].z)), ...);
+}
+
+template <int ISO>
+__global__ void __launch_bounds__(kEnergyCellThreads, 3) energy_cell_kernel(const __grid_constant__ EnergyCellArgs a) {
+    __shared__ double red[4 * 32];
+    const int4 tile = a.tiles[blockIdx.x];  // (replica, first cell, cells, -)
+    const ReplicaDev rep = a.reps[tile.x];
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (int(threadIdx.x) < tile.z) {
+        const int cell = tile.y + int(threadIdx.x);
+        const Coords c = cell_coords(cell, rep.L, rep.divL);
+        const char* base = reinterpret_cast<const char*>(a.spins + rep.off);
+        const uint32_t sl_bytes = uint32_t(rep.Nc) << 4;
+        float3 own[16];
+        load_own(own, base, sl_bytes, c, std::make_integer_sequence<int, 16>{});
+        float acc[kAcc];
+#pragma unroll
+        for (int k = 0; k < kAcc; ++k) acc[k] = 0.f;
+        intra_bonds<ISO>(acc, own, a.mats, std::make_integer_sequence<int, cb_n_intra()>{});
+        remote_bonds<0, ISO>(acc, own, base, sl_bytes, c, a.mats);
+#pragma unroll
+        for (int k = 0; k < kAcc; ++k) v[0] += double(acc[k]);
+#pragma unroll
+        for (int sl = 0; sl < 16; ++sl) {
+            v[0] -= double(own[sl].x * a.B[0] + own[sl].y * a.B[1] + own[sl].z * a.B[2]);
+            v[1] += double(own[sl].x);
+            v[2] += double(own[sl].y);
+            v[3] += double(own[sl].z);
+        }
+    }
+    // block-wide FP64 sum: warp shuffles, then one warp over the warp sums
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+        if (lane == 0) red[j * 32 + warp] = v[j];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double x = lane < nw ? red[j * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) a.partial[size_t(blockIdx.x) * 4 + j] = x;
+        }
+    }
+}
+
+void launch_energy_cells(const EnergyCellArgs& a, cudaStream_t st) {
+    if (a.n_tiles <= 0) return;
+    if (a.iso == 1)
+        energy_cell_kernel<1><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+    else if (a.iso == 2)
+        energy_cell_kernel<2><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+    else
+        energy_cell_kernel<0><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+}
+
+}  // namespace pc

@@ -113,6 +113,22 @@ void launch_energy_partials(const EnergyArgs& a, int threads, cudaStream_t st);
 void launch_energy_finalize(const double* partial, const int32_t* tile_begin, const int32_t* tile_end,
                             const ReplicaDev* reps, int R, double* e, double* mag, cudaStream_t st);
 
+// Energy with one thread per cubic cell (energy_cell.cu): tiles of up to
+// kEnergyCellThreads consecutive cells of one replica, (replica, first cell,
+// cells, 0); partial[tile][4] = sum of the owned bond energies - S.B, sum S.
+constexpr int kEnergyCellThreads = 128;
+struct EnergyCellArgs {
+    const float4* spins;
+    const ReplicaDev* reps;
+    const int4* tiles;
+    int n_tiles;
+    float B[3];
+    double* partial;
+    int iso;  // as EnergyArgs::iso
+    PyroMats mats;
+};
+void launch_energy_cells(const EnergyCellArgs& a, cudaStream_t st);
+
 struct FieldArgs {
     const float4* spins;
     const ReplicaDev* reps;

@@ -1,0 +1,332 @@
+"""Parity at the sizes and couplings the benchmark configurations run, through
+the C ABI, against the FP64 oracle (pinned on the reference's own src/MC.cpp,
+tests/test_oracle_ref.py).
+
+Deterministic (one configuration, no randomness in the comparison):
+  energy per cell and local field at L = 8, 12, 16, 24, 64 with each
+  configuration's couplings (1e-5 relative to the quantity's scale); one
+  overrelaxation pass with given angles at L = 12, 16, 24, 64 (FP32 bound of
+  the small-L test: 99.5 % of components within 1e-5, all within 2e-4); one
+  sweep site by site against the oracle's Philox mirror at L = 12, 16, 64 (at
+  these sizes a handful of the 10^4..10^6 accept decisions sit within FP32
+  rounding of their threshold and may flip, so: accepted counts within 1e-5 of
+  the proposals, 99.9 % of spins within 1e-4).
+
+Stochastic (K independent chains per side; the GPU chain uses Philox draws,
+the oracle the reference's Xoroshiro128++ and sequential sweep):
+  anneal with J = (1, -0.1, 0.05) at L = 8 and 16 (T_hot = 10 sqrt(1.0125) ->
+  0.02, shortened to 20 log steps; <e>(T), cross-seed C_v, S(q) at the sample
+  temperatures); uneven-L batched tempering with J3 = 0.02, B = (0, 0, 0.1):
+  an L = 8 and an L = 12 ladder of 8 temperatures each geometric in
+  [0.02, 2.0] in one system, against the oracle's emulation of temper.cpp;
+  the L = 64 field-cool model J = (1, 0.1, 0.05), B = (0, 0, 0.5) at
+  T = 2.0 and 0.5: e after each of the first sweeps from a uniform start and
+  the radially binned S(q); the fused sweep schedule (the benchmark's) in
+  equilibrium at L = 8 with the same model.
+Where both sides run the same protocol from the same start distribution
+(reference-order schedule), out-of-equilibrium expectations match too; the
+fused schedule is a different Markov chain with the same stationary
+distribution, so it is compared in equilibrium only.
+
+Criterion (deviation from "within 3 sigma at every temperature", stated as
+such): at least 95 % of the compared quantities within 3 sigma of the combined
+error and none beyond 5 sigma. With tens of temperatures a strict 3-sigma cut
+on every one fails a few percent of correct runs.
+"""
+import concurrent.futures as cf
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import pyro_cmc_b200 as pc
+from oracle import ssf_fft
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-5
+CONFIG2 = dict(J1=1.0, J2=-0.1, J3=0.05, Delta=1.0, B=(0.0, 0.0, 0.0))
+CONFIG3 = dict(J1=1.0, J2=0.0, J3=0.02, Delta=1.0, B=(0.0, 0.0, 0.1))
+CONFIG4 = dict(J1=1.0, J2=0.1, J3=-0.05, Delta=1.0, B=(0.2, 0.0, 0.0))
+CONFIG5 = dict(J1=1.0, J2=0.1, J3=0.05, Delta=1.0, B=(0.0, 0.0, 0.5))
+THREADS = max(1, min(16, os.cpu_count() or 1))
+
+
+def _unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _scale(c):
+    return 16 * (6 * abs(c["J1"]) + 12 * abs(c["J2"]) + 12 * abs(c["J3"]) + np.linalg.norm(c["B"]))
+
+
+def _spiral(o, Kq=3):
+    pos, _ = o.positions()
+    q = 2 * np.pi * Kq / (8 * o.L)
+    return np.stack([np.zeros(len(pos)), np.cos(q * pos[:, 2]), np.sin(q * pos[:, 2])], axis=1)
+
+
+_L64 = {}
+
+
+def _pair(L, c, **kw):
+    """GPU system and oracle with the same couplings; the L = 64 pair (13 s to
+    build the oracle's pointer shells) is kept for the module."""
+    key = (L, tuple(sorted((k, v if not isinstance(v, tuple) else tuple(v)) for k, v in c.items())),
+           tuple(sorted(kw.items())))
+    if L == 64 and key in _L64:
+        return _L64[key]
+    g = pc.pyrochlore_system(L, seed=kw.get("seed", 0), **c, schedule=kw.get("schedule", 0))
+    o = oracle.System(L, seed=kw.get("seed", 0), **c)
+    if L == 64:
+        _L64.clear()
+        _L64[key] = (g, o)
+    return g, o
+
+
+@pytest.mark.parametrize("L,c", [(8, CONFIG4), (12, CONFIG3), (16, CONFIG2), (24, CONFIG3), (64, CONFIG5)])
+def test_energy_and_local_field_at_config_sizes(L, c):
+    g, o = _pair(L, c)
+    rng = np.random.default_rng(L)
+    for name, S in (("random", _unit(rng, o.N)), ("spiral", _spiral(o))):
+        g.set_spins(S)
+        S32 = g.spins()
+        o.set_spins(S32)
+        e, m = g.energy()
+        e_ref = o.energy()
+        assert abs(e[0] - e_ref) <= REL * _scale(c), (name, e[0], e_ref)
+        np.testing.assert_allclose(m[0], S32.sum(axis=0), rtol=0, atol=1e-6 * o.N)
+        h_ref = o.local_fields()
+        h = g.local_field()
+        err = np.abs(h - h_ref).max() / max(1.0, np.abs(h_ref).max())
+        assert err <= REL, (name, err)
+
+
+@pytest.mark.parametrize("L,c", [(12, CONFIG3), (16, CONFIG2), (24, CONFIG3), (64, CONFIG5)])
+def test_overrelax_pass_with_given_angles_at_config_sizes(L, c):
+    g, o = _pair(L, c)
+    rng = np.random.default_rng(100 + L)
+    g.set_spins(_unit(rng, o.N))
+    o.set_spins(g.spins())
+    _, col = g.colours()
+    theta = rng.uniform(0, 2 * np.pi, o.N)
+    e0 = o.energy()
+    g.overrelax_theta(theta)
+    o.overrelax(theta, colour_of_sl=col)
+    d = np.abs(g.spins() - o.spins())
+    assert np.mean(d <= 1e-5) >= 0.995, np.sort(d.ravel())[-10:]
+    assert d.max() <= 2e-4
+    e, _ = g.energy()
+    assert abs(e[0] - e0) <= REL * _scale(c)  # overrelaxation keeps the energy
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("L,c,T", [(12, CONFIG3, 0.3), (16, CONFIG2, 0.5), (64, CONFIG5, 0.5)])
+def test_sweep_follows_oracle_mirror_at_config_sizes(L, c, T, schedule):
+    seed = 4321
+    g, o = _pair(L, c, seed=seed, schedule=schedule)
+    g.set_sweep_counter(0)
+    rng = np.random.default_rng(L + schedule)
+    g.set_spins(_unit(rng, o.N))
+    o.set_spins(g.spins())
+    _, col = g.colours()
+    acc_g = int(g.sweep(T, 1, 1)[0])
+    acc_o = int(o.sweep_philox(T, seed, 0, 0, col, n_overrelax=1, or_mode=0, fused=bool(schedule)))
+    assert abs(acc_g - acc_o) <= max(2, 1e-5 * o.N), (acc_g, acc_o)
+    d = np.abs(g.spins() - o.spins()).max(axis=1)
+    assert np.mean(d <= 1e-4) >= 0.999, np.sort(d)[-10:]
+
+
+# --------------------------------------------------------------- stochastic
+def _z(a, sa, b, sb):
+    return np.abs(a - b) / np.sqrt(sa ** 2 + sb ** 2 + 1e-300)
+
+
+def _check(z, what):
+    z = np.asarray(z).ravel()
+    frac = np.mean(z <= 3)
+    assert frac >= 0.95 and z.max() <= 5, (what, frac, z.max(), int(np.argmax(z)))
+
+
+def _pooled_z(a, b):
+    """Per column: |mean(a) - mean(b)| over the pooled-variance error of the
+    difference (a: [Ka, ...], b: [Kb, ...] independent chains)."""
+    na, nb = len(a), len(b)
+    sp2 = ((na - 1) * a.var(0, ddof=1) + (nb - 1) * b.var(0, ddof=1)) / (na + nb - 2)
+    return np.abs(a.mean(0) - b.mean(0)) / np.sqrt(sp2 * (1 / na + 1 / nb) + 1e-300)
+
+
+def _variance_z(a, b):
+    """Cross-seed C_v = var(e)/T^2 compared per temperature by the F test of
+    the two sample variances (the ratio is F(Ka-1, Kb-1) distributed when
+    they agree), its two-sided p-value written as the equivalent normal |z|.
+    A jackknife error on a variance from 32 seeds is itself too noisy for a
+    3-sigma cut."""
+    from scipy import stats
+    va, vb = a.var(0, ddof=1), b.var(0, ddof=1)
+    F = va / np.maximum(vb, 1e-300)
+    cdf = stats.f.cdf(F, len(a) - 1, len(b) - 1)
+    p = np.clip(2 * np.minimum(cdf, 1 - cdf), 1e-300, 1.0)
+    return stats.norm.isf(p / 2)
+
+
+@pytest.mark.parametrize("L", [8, 16])
+def test_config2_anneal_statistical_parity(L):
+    """Config 2's model and temperature range: K = 32 seeds per side of the
+    anneal protocol (src/anneal.cpp:193-227) with the reference's move order,
+    the 200 log steps shortened to 20 (16 sweeps each, 16 burn-in sweeps),
+    S(q) xx/yy/zz at T in {0.5, 0.1, 0.02} from 8 samples."""
+    from pyro_cmc_b200.anneal import anneal_batch
+
+    K, n_steps, n_sweep, n_burn, n_samp = 32, 20, 16, 16, 8
+    T_hot, T_cold, T_s = 10 * np.sqrt(1.0125), 0.02, [0.5, 0.1, 0.02]
+    corr = ["xx", "yy", "zz"]
+    res = anneal_batch(K=K, L=L, J1=1.0, J2=-0.1, J3=0.05, T_hot=T_hot, T_cold=T_cold, T_sample=T_s,
+                       n_steps=n_steps, n_sweep=n_sweep, n_burn_in=n_burn, n_sample=n_samp, corr=corr,
+                       seed=0x5eed + L, schedule=0)
+
+    def run(k):
+        o = oracle.System(L, seed=0xdeadbeef + 7919 * k, **CONFIG2)
+        o.random_spins(31 + k)
+        return o.anneal(T_hot, T_cold, T_s, n_steps, n_sweep, n_burn, n_samp, corr)
+
+    with cf.ThreadPoolExecutor(THREADS) as ex:
+        out = list(ex.map(run, range(K)))
+    T = out[0][0]
+    np.testing.assert_allclose(res["T"], T, rtol=1e-14)
+    e_gpu, e_cpu = res["e"], np.array([o[1] for o in out])
+    _check(_z(e_gpu.mean(0), e_gpu.std(0, ddof=1) / np.sqrt(K), e_cpu.mean(0), e_cpu.std(0, ddof=1) / np.sqrt(K)),
+           "<e>")
+
+    _check(_variance_z(e_gpu, e_cpu), "C_v")
+    s_gpu = res["ssf_sum"][..., 0] / n_samp  # [K, nT, corr, nk]
+    s_cpu = np.array([o[2][..., 0] for o in out]) / n_samp
+    _check(_z(s_gpu.mean(0), s_gpu.std(0, ddof=1) / np.sqrt(K), s_cpu.mean(0), s_cpu.std(0, ddof=1) / np.sqrt(K)),
+           "S(q)")
+
+
+def test_config3_uneven_ladders_statistical_parity():
+    """Config 3's model in one uneven-L batched system: an L = 8 and an L = 12
+    ladder of 8 temperatures each, geometric in [0.02, 2.0], exchange after
+    every round of 4 sweeps (checkerboard pairs, src/temper.cpp:437-473),
+    30 burn-in and 90 measured rounds from a uniform start, reference move
+    order; per-slot <e> of K = 16 runs per side against the oracle's temper
+    emulation of each ladder, which runs the same rounds (its burn-in too with
+    exchanges: at T = 0.02 the 120 sweeps do not equilibrate, so the two
+    protocols must be the same round for round)."""
+    T = list(np.geomspace(2.0, 0.02, 8))
+    K, n_burn, n_rounds, n_sweep = 16, 30, 90, 4
+    gpu = {8: [], 12: []}
+    for k in range(K):
+        s = pc.pyrochlore_system([8] * 8 + [12] * 8, seed=500 + k, schedule=0, **CONFIG3)
+        s.random_spins(900 + k)
+        s.pt_configure(T + T)
+        s.pt_run(n_burn, n_sweep)
+        s.pt_reset_stats()
+        s.pt_run(n_rounds, n_sweep)
+        Ts, E, _, n = s.pt_energy()
+        assert (n == n_rounds).all()
+        gpu[8].append(E[:8] / n[:8])
+        gpu[12].append(E[8:] / n[8:])
+        s.close()
+
+    def run(arg):
+        L, k = arg
+        es, _, _, _ = oracle.temper(L, T, seed=7000 + 31 * k + L, n_burn_in=0, n_burn_rounds=n_burn,
+                                    n_rounds=n_rounds, n_sweep=n_sweep, **CONFIG3)
+        return es / n_rounds
+
+    with cf.ThreadPoolExecutor(THREADS) as ex:
+        cpu12 = list(ex.map(run, [(12, k) for k in range(K)]))
+        cpu8 = list(ex.map(run, [(8, k) for k in range(K)]))
+    z = []
+    for L, cpu in ((8, cpu8), (12, cpu12)):
+        a, b = np.array(gpu[L]), np.array(cpu)
+        z.append(_z(a.mean(0), a.std(0, ddof=1) / np.sqrt(K), b.mean(0), b.std(0, ddof=1) / np.sqrt(K)))
+    _check(np.concatenate(z), "PT <e>(T), L = 8 and 12")
+
+
+def _radial_bins(S3, L, n_bins=12):
+    """Diagonal S(q) summed over the three components (xx + yy + zz) and zz
+    alone, averaged in shells of |K| (K folded into [-L/2, L/2))."""
+    K = np.arange(L)
+    Kf = np.where(K < L // 2, K, K - L)
+    r = np.sqrt(Kf[:, None, None] ** 2 + Kf[None, :, None] ** 2 + Kf[None, None, :] ** 2).ravel()
+    edges = np.linspace(0, r.max() + 1e-9, n_bins + 1)
+    idx = np.clip(np.digitize(r, edges) - 1, 0, n_bins - 1)
+    cnt = np.bincount(idx, minlength=n_bins)
+    tot = np.bincount(idx, weights=S3[..., 0].sum(axis=0), minlength=n_bins) / cnt
+    zz = np.bincount(idx, weights=S3[2, :, 0], minlength=n_bins) / cnt
+    return np.concatenate([tot, zz])
+
+
+@pytest.mark.parametrize("T", [2.0, 0.5])
+def test_config5_fieldcool_L64_statistical_parity(T):
+    """Config 5's model at its size, L = 64 (4,194,304 spins): e after each of
+    the first 4 sweeps from a uniform start at fixed T and the radially binned
+    S(q) (xx + yy + zz, zz) after the last, for 32 GPU chains (batched
+    replicas) and 8 oracle chains, reference move order. Errors from the
+    pooled chain-to-chain variance."""
+    L, Kg, Ko, n_sw = 64, 32, 8, 4
+    corr = ["xx", "yy", "zz"]
+    g = pc.pyrochlore_system(L, n_replicas=Kg, seed=77, schedule=0, **CONFIG5)
+    g.random_spins(78)
+    g.ssf_configure(corr, 0, [])
+    eg = np.zeros((Kg, n_sw))
+    for k in range(n_sw):
+        g.sweep(T, 1, 1)
+        eg[:, k], _ = g.energy()
+    sg = np.array([_radial_bins(g.ssf_current(r), L) for r in range(Kg)])
+    g.close()
+
+    def run(k):
+        o = oracle.System(L, seed=1000 + k, **CONFIG5)
+        o.random_spins(2000 + k)
+        e = np.zeros(n_sw)
+        for j in range(n_sw):
+            o.sweep(T, 1, 1)
+            e[j] = o.energy()
+        s = _radial_bins(ssf_fft.ssf(o.spins(), L, corr), L)
+        return e, s
+
+    with cf.ThreadPoolExecutor(min(THREADS, Ko)) as ex:
+        out = list(ex.map(run, range(Ko)))
+    eo = np.array([x[0] for x in out])
+    so = np.array([x[1] for x in out])
+    _check(_pooled_z(eg, eo), "e(sweep)")
+    _check(_pooled_z(sg, so), "binned S(q)")
+
+
+@pytest.mark.parametrize("T", [2.0, 0.5, 0.25])
+def test_fused_schedule_equilibrium_matches_reference_order(T):
+    """The benchmark's fused Metropolis + overrelaxation schedule samples the
+    same equilibrium as the reference's sweep: config 5's model at L = 8,
+    <e> over 400 sweeps after 400 burn-in sweeps, 32 GPU chains (fused)
+    against 16 oracle chains (reference order, Xoroshiro)."""
+    L, Kg, Ko, n_burn, n_meas = 8, 32, 16, 400, 400
+    g = pc.pyrochlore_system(L, n_replicas=Kg, seed=55, schedule=1, **CONFIG5)
+    g.random_spins(56)
+    g.sweep(T, n_burn, 1, count=False)
+    eg = np.zeros(Kg)
+    for _ in range(n_meas // 10):
+        g.sweep(T, 10, 1, count=False)
+        eg += g.energy()[0]
+    eg /= n_meas // 10
+    g.close()
+
+    def run(k):
+        o = oracle.System(L, seed=3000 + k, **CONFIG5)
+        o.random_spins(4000 + k)
+        o.sweep(T, n_burn, 1)
+        e = 0.0
+        for _ in range(n_meas // 10):
+            o.sweep(T, 10, 1)
+            e += o.energy()
+        return e / (n_meas // 10)
+
+    with cf.ThreadPoolExecutor(THREADS) as ex:
+        eo = np.array(list(ex.map(run, range(Ko))))
+    z = _pooled_z(eg[:, None], eo[:, None])
+    assert z.max() <= 3.5, (T, eg.mean(), eo.mean(), z)

@@ -251,7 +251,8 @@ def test_pt_equilibrium_matches_reference_tempering(schedule):
     gpu_means = np.array(gpu_means)
 
     def run(k):
-        es, e2, att, acc = oracle.temper(L, T, seed=1000 + 7 * k, n_burn_in=200, n_rounds=200, n_sweep=5, **c)
+        es, e2, att, acc = oracle.temper(L, T, seed=1000 + 7 * k, n_burn_in=0, n_burn_rounds=40, n_rounds=200,
+                                         n_sweep=5, **c)
         return es / 200
 
     with cf.ThreadPoolExecutor(8) as ex:
