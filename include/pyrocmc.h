@@ -272,6 +272,18 @@ int pc_pt_slots(pc_system* sys, int32_t* slot_of_replica);
  * all (the spin gradient alone costs about one energy evaluation). */
 int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* grad_S_dev, double* grad_J,
                    double* grad_B);
+/* pc_energy_grad evaluated on an arbitrary field instead of the system's
+ * spins: field_dev (device, float4[N_total], 16-byte aligned, any length per
+ * site) stands for S in every formula above, with the system's couplings and
+ * field. With g[r] = Nc the outputs are h_i(field) - B and the bond sums
+ * sum field_src[a] field_tgt[b]; the differentiable gradient quench uses it
+ * for the local field of an upstream gradient (the energy's Hessian is the
+ * coupling matrix) and, through (P(S + v) - P(S) - P(v)), for the mixed bond
+ * sums of its coupling gradient. No counterpart in the reference (the
+ * backward of MC_runner::local_field, src/MC.cpp:87-96). grad_S_dev must not
+ * alias field_dev. */
+int pc_energy_grad_field(pc_system* sys, const void* field_dev, const double* g, double* e_per_cell,
+                         void* grad_S_dev, double* grad_J, double* grad_B);
 /* S(q) for every replica into a device buffer out_dev[R][n_corr][n_k][2]
  * (float64), no accumulation. Uses the correlators of pc_ssf_configure. */
 int pc_ssf_forward(pc_system* sys, void* out_dev);
@@ -283,21 +295,27 @@ int pc_ssf_backward(pc_system* sys, const void* grad_out_dev, void* grad_S_dev);
 /* ------------------------------------------------------ allocation-free */
 
 /* No counterpart in the reference. Energy per cubic cell and magnetisation of
- * one pyrochlore lattice for callers that may not allocate device memory (a
- * thread capturing a CUDA graph in global mode, a program whose memory belongs
- * to a framework's caching allocator, a loop that cannot absorb the device-wide
- * synchronisation of cudaFree). Nothing is allocated: the reduction's partial
+ * one pyrochlore lattice for callers that may not allocate device memory: a
+ * program whose device memory belongs to a framework's caching allocator (an
+ * allocation behind its back fragments the pool, or fails once the pool holds
+ * the free memory), or a loop that cannot absorb the device-wide
+ * synchronisation of cudaFree. Nothing is allocated: the reduction's partial
  * sums live in a 512 KiB array compiled into the library, shared by all calls
  * on a device and kept until the process exits.
- *   spins_dev  device, float4[16 L^3] in this library's site order
+ *   spins_dev  device, float4[16 L^3] in this library's site order, 16-byte
+ *              aligned
  *   L          1..64 (larger L is rejected with PC_ERR_INVALID before any work)
  *   params     host, 7 doubles: J1, J2, J3, Delta, Bx, By, Bz (the coupling set
  *              of build_J1J2J3_h)
- *   out_dev    device, 4 doubles: energy per cubic cell, sum_i S_i (x, y, z)
+ *   out_dev    device, 4 doubles, 8-byte aligned: energy per cubic cell,
+ *              sum_i S_i (x, y, z)
  *   stream     cudaStream_t to launch on (NULL: the default stream)
- * Asynchronous on `stream`. The first call on a device looks up the scratch
- * array's address; make it before any stream capture. Calls that overlap on
- * the GPU (e.g. on two streams) race on the shared array. */
+ * Misaligned pointers are rejected with PC_ERR_INVALID. Asynchronous on
+ * `stream`. The first call in a CUDA context (the first on a device, and the
+ * first after that device's context is re-created, e.g. by cudaDeviceReset)
+ * looks up the scratch array's address; make it before any stream capture.
+ * Calls that overlap on the GPU (e.g. on two streams) race on the shared
+ * array. */
 int pc_energy_noalloc(const void* spins_dev, int L, const double* params, void* out_dev, void* stream);
 
 /* ------------------------------------------------------------------ tuning */

@@ -167,6 +167,12 @@ struct pc_system {
     std::vector<int32_t> tile_begin, tile_end;
     DevBuf<int32_t> d_tile_begin, d_tile_end;
     DevBuf<double> d_partial;
+    // energy with one thread per cubic cell (energy_cell.cu): tiles of cells
+    // per replica, their ranges and FP64 partials
+    DevBuf<int4> d_cell_tiles;
+    int n_cell_tiles = 0;
+    DevBuf<int32_t> d_cell_begin, d_cell_end;
+    DevBuf<double> d_cell_partial;
     DevBuf<double> d_e, d_mag;
     DevBuf<double> d_theta;
     DevBuf<float4> d_field;
@@ -268,6 +274,10 @@ struct pc_system {
         d_tile_begin.release();
         d_tile_end.release();
         d_partial.release();
+        d_cell_tiles.release();
+        d_cell_begin.release();
+        d_cell_end.release();
+        d_cell_partial.release();
         d_e.release();
         d_mag.release();
         d_theta.release();
@@ -561,6 +571,25 @@ int build_tiles(pc_system* s) {
     PC_CK(s->d_tile_end.alloc(size_t(s->R)));
     PC_CK(cudaMemcpy(s->d_tile_begin.p, s->tile_begin.data(), sizeof(int32_t) * size_t(s->R), cudaMemcpyHostToDevice));
     PC_CK(cudaMemcpy(s->d_tile_end.p, s->tile_end.data(), sizeof(int32_t) * size_t(s->R), cudaMemcpyHostToDevice));
+    // cell tiles of the per-cell energy kernel, replica by replica
+    {
+        std::vector<int4> ct;
+        std::vector<int32_t> cb(size_t(s->R)), ce(size_t(s->R));
+        for (int r = 0; r < s->R; ++r) {
+            cb[size_t(r)] = int32_t(ct.size());
+            for (int64_t c0 = 0; c0 < s->Nc(r); c0 += pc::kEnergyCellThreads)
+                ct.push_back(make_int4(r, int(c0), int(std::min<int64_t>(pc::kEnergyCellThreads, s->Nc(r) - c0)), 0));
+            ce[size_t(r)] = int32_t(ct.size());
+        }
+        s->n_cell_tiles = int(ct.size());
+        PC_CK(s->d_cell_tiles.alloc(ct.size()));
+        PC_CK(cudaMemcpy(s->d_cell_tiles.p, ct.data(), ct.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        PC_CK(s->d_cell_begin.alloc(size_t(s->R)));
+        PC_CK(s->d_cell_end.alloc(size_t(s->R)));
+        PC_CK(cudaMemcpy(s->d_cell_begin.p, cb.data(), sizeof(int32_t) * cb.size(), cudaMemcpyHostToDevice));
+        PC_CK(cudaMemcpy(s->d_cell_end.p, ce.data(), sizeof(int32_t) * ce.size(), cudaMemcpyHostToDevice));
+        PC_CK(s->d_cell_partial.alloc(ct.size() * 4));
+    }
     // partial sums: energy (4 per tile) and gradient (4 + 9*n_spec per tile)
     const size_t width = size_t(4 + 9 * std::max<size_t>(1, s->specs.size()));
     PC_CK(s->d_partial.alloc(size_t(s->n_all_tiles) * width));
@@ -797,6 +826,24 @@ int run_sweeps(pc_system* s, int n_sweeps, int n_or) {
 }
 
 int enqueue_energy(pc_system* s) {
+    if (s->structured) {  // one thread per cubic cell, each bond once (energy_cell.cu)
+        pc::EnergyCellArgs c;
+        c.spins = s->d_spins.p;
+        c.reps = s->d_reps.p;
+        c.tiles = s->d_cell_tiles.p;
+        c.n_tiles = s->n_cell_tiles;
+        for (int i = 0; i < 3; ++i) c.B[i] = float(s->B[i]);
+        c.partial = s->d_cell_partial.p;
+        c.iso = s->iso_kind;
+        c.mats = s->mats;
+        pc::launch_energy_cells(c, s->stream);
+        PC_LAUNCH_CK();
+        pc::launch_energy_finalize(s->d_cell_partial.p, s->d_cell_begin.p, s->d_cell_end.p, s->d_reps.p, s->R,
+                                   s->d_e.p, s->d_mag.p, s->stream);
+        PC_LAUNCH_CK();
+        s->launches += 2;
+        return PC_OK;
+    }
     pc::EnergyArgs a;
     a.spins = s->d_spins.p;
     a.reps = s->d_reps.p;
@@ -1930,10 +1977,35 @@ int pc_pt_slots(pc_system* sys, int32_t* slot_of_replica) {
 }
 
 // -------------------------------------------------------------- gradients
+namespace {
+int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double* e_per_cell, void* grad_S_dev,
+                   double* grad_J, double* grad_B);
+}
+
 int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* grad_S_dev, double* grad_J,
                    double* grad_B) {
     int rc = check_sys(sys);
     if (rc) return rc;
+    return energy_grad_of(sys, sys->d_spins.p, g, e_per_cell, grad_S_dev, grad_J, grad_B);
+}
+
+int pc_energy_grad_field(pc_system* sys, const void* field_dev, const double* g, double* e_per_cell,
+                         void* grad_S_dev, double* grad_J, double* grad_B) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!field_dev) return fail(PC_ERR_INVALID, "pc_energy_grad_field: null field");
+    if (reinterpret_cast<uintptr_t>(field_dev) % 16 != 0)
+        return fail(PC_ERR_INVALID, "pc_energy_grad_field: field is not 16-byte aligned (float4)");
+    if (grad_S_dev == field_dev) return fail(PC_ERR_INVALID, "pc_energy_grad_field: output aliases the field");
+    return energy_grad_of(sys, static_cast<const float4*>(field_dev), g, e_per_cell, grad_S_dev, grad_J, grad_B);
+}
+
+}  // extern "C"
+
+namespace {
+int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double* e_per_cell, void* grad_S_dev,
+                   double* grad_J, double* grad_B) {
+    int rc = PC_OK;
     const int ns = int(sys->specs.size());
     // the structured kernel forms the coupling products only when they are asked for
     const bool structured = sys->grad_struct && sys->threads <= 256;
@@ -1951,7 +2023,7 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
     PC_CK(cudaMemcpyAsync(d_g.p, st_g, sizeof(double) * R, cudaMemcpyHostToDevice, sys->stream));
     if (structured) {
         pc::GradStructArgs a;
-        a.spins = sys->d_spins.p;
+        a.spins = spins;
         a.reps = sys->d_reps.p;
         a.tiles = sys->d_all_tiles.p;
         a.items = sys->d_grad_items.p;
@@ -1970,7 +2042,7 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
         PC_LAUNCH_CK();
     } else {
         pc::GradArgs a;
-        a.spins = sys->d_spins.p;
+        a.spins = spins;
         a.reps = sys->d_reps.p;
         a.tables = sys->d_tab_full.p;
         a.tiles = sys->d_all_tiles.p;
@@ -1999,8 +2071,12 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
         if (grad_J)
             for (int k = 0; k < 9 * ns; ++k) grad_J[size_t(r) * 9 * size_t(ns) + size_t(k)] = gr * o[4 + k] / nc;
     }
+    (void)rc;
     return PC_OK;
 }
+}  // namespace
+
+extern "C" {
 
 // ---------------------------------------------------------------- tuning
 int pc_get_tile(pc_system* sys, int* threads, int* ctas_per_sm) {
