@@ -144,6 +144,77 @@ class SSFFunction(torch.autograd.Function):
         return grad_spins, None
 
 
+def _nc_vector(system: System) -> np.ndarray:
+    return np.array([system.Nc(r) for r in range(system.R)], dtype=np.float64)
+
+
+def _field_of(system: System, field: torch.Tensor, couplings: bool):
+    """h(field) - B per site (float32 [N_total, 4], fourth component 0) and,
+    with couplings, the per-replica bond sums P(field)[spec] = sum over the
+    spec's bonds of field_src field_tgt^T (pc_energy_grad_field with g = Nc)."""
+    field = field.detach().contiguous()
+    out = torch.empty_like(field)
+    torch.cuda.current_stream().synchronize()
+    _, P, _ = system.energy_grad_field(field.data_ptr(), _nc_vector(system), out.data_ptr(), couplings=couplings)
+    return out, P
+
+
+class LocalFieldFunction(torch.autograd.Function):
+    """h_i(S; J) - B for every site (MC_runner::local_field minus the global
+    field, src/MC.cpp:87-96,113): the energy's spin gradient times Nc. Its
+    backward is exact for the bilinear energy: with upstream u,
+    d(sum u.h)/dS = h(u) (the coupling matrix is the Hessian), d/dJ_spec =
+    sum over the spec's bonds of u_src S_tgt^T + S_src u_tgt^T (formed from
+    the bond sums as P(S + a u) - P(S) - P(a u), divided by a, with a scaling
+    u to the spins' magnitude), d/dB = -sum_i u_i."""
+
+    @staticmethod
+    def forward(ctx, spins, params, system):
+        if params is not None:
+            _apply_params(system, params)
+        h, _ = _field_of(system, spins, couplings=False)
+        ctx.system = system
+        ctx.has_params = params is not None
+        ctx.params_device = params.device if params is not None else None
+        ctx.save_for_backward(spins)
+        return h
+
+    @staticmethod
+    def backward(ctx, grad_h):
+        system = ctx.system
+        (spins,) = ctx.saved_tensors
+        u = grad_h.detach().clone()
+        u[:, 3] = 0
+        B = torch.as_tensor(system.get_global_field(), dtype=torch.float32, device=u.device)
+        hu, _ = _field_of(system, u, couplings=False)
+        grad_spins = hu
+        grad_spins[:, :3] += B  # h(u), without the field
+        gp = None
+        if ctx.has_params:
+            s = spins.detach().clone()
+            s[:, 3] = 0
+            a = float(s[:, :3].norm()) / max(float(u[:, :3].norm()), 1e-30)
+            _, P_sum = _field_of(system, s + a * u, couplings=True)
+            _, P_s = _field_of(system, s, couplings=True)
+            _, P_u = _field_of(system, a * u, couplings=True)
+            mixed = (P_sum - P_s - P_u) / a  # [R, spec, 3, 3]
+            R = system.R
+            gB = np.zeros((R, 3))
+            off = 0
+            for r in range(R):
+                n = system.N(r)
+                gB[r] = -u[off:off + n, :3].sum(dim=0).double().cpu().numpy()
+                off += n
+            gp = torch.as_tensor(_param_grads(system, mixed, gB).sum(axis=0), dtype=torch.float64,
+                                 device=ctx.params_device)
+        return grad_spins, gp, None
+
+
+def local_field(system: System, spins: torch.Tensor, params: torch.Tensor | None = None) -> torch.Tensor:
+    """h_i - B of every site, differentiable in the spins and params."""
+    return LocalFieldFunction.apply(spins, params, system)
+
+
 def energy(system: System, spins: torch.Tensor, params: torch.Tensor | None = None) -> torch.Tensor:
     return EnergyFunction.apply(spins, params, system)
 

@@ -407,6 +407,18 @@ class System:
              _dp(gB))
         return e, None if gJ is None else gJ.reshape(self.R, n_spec, 3, 3), gB
 
+    def energy_grad_field(self, field_ptr: int, g=None, grad_ptr: int | None = None, couplings: bool = True):
+        """energy_grad evaluated on the device field at field_ptr (float4
+        [N_total]) instead of the system's spins (pc_energy_grad_field)."""
+        n_spec = len(self.spec_names)
+        e = np.empty(self.R)
+        gJ = np.empty((self.R, n_spec, 9)) if couplings else None
+        gB = np.empty((self.R, 3))
+        gv = None if g is None else _c(np.broadcast_to(np.asarray(g, dtype=np.float64), (self.R,)), np.float64)
+        call("pc_energy_grad_field", self._h, C.c_void_p(field_ptr), None if gv is None else _dp(gv), _dp(e),
+             None if grad_ptr is None else C.c_void_p(grad_ptr), None if gJ is None else _dp(gJ), _dp(gB))
+        return e, None if gJ is None else gJ.reshape(self.R, n_spec, 3, 3), gB
+
     # ---------------------------------------------------------------- tuning
     def autotune(self):
         """Picks the fastest tile shape and neighbour-load variant by timing
@@ -430,6 +442,11 @@ class System:
 
     def set_tile(self, threads: int, ctas_per_sm: int):
         call("pc_set_tile", self._h, threads, ctas_per_sm)
+
+    def set_wait_limit(self, polls: int):
+        """Bound of the staged colour pass's first wait on its copies
+        (pc_set_wait_limit; < 0 restores the default)."""
+        call("pc_set_wait_limit", self._h, int(polls))
 
     def set_kernel_timing(self, on: bool):
         call("pc_set_kernel_timing", self._h, int(bool(on)))

@@ -1,0 +1,168 @@
+"""The differentiable form as the gradient configuration specifies it, through
+the C ABI: a batch of uniform random configurations at L = 8 with
+J = (1, 0.1, -0.05), B = (0.2, 0, 0); loss = sum_q w(q) |S^zz(q) - S_target(q)|^2
+with w ~ U[0, 1] and S_target the S^zz(q) of the spiral_byhand state at a
+seeded random Q (test/spiral_byhand.cpp:100-107); gradients with respect to
+the spins (projected onto the tangent plane) and, through the energy, to
+J1..J3 and B, against FP64 central differences (h = 1e-4) on the oracle.
+Then the unrolled gradient quench (differentiable in the couplings) against
+FP64 central differences of the same quench run on the oracle, and a fit of
+(J2, J3) to a target S(q) that recovers the couplings that made it.
+
+Tolerances: 2e-3 relative to the largest compared component (FP32 spins and
+transforms against FP64), as the other finite-difference tests; the unrolled
+quench (FP32 forward over several steps) 2e-2.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import pyro_cmc_b200 as pc
+from pyro_cmc_b200 import autograd as ag
+from pyro_cmc_b200 import ssf_fit
+
+pytestmark = pytest.mark.gpu
+
+C4 = dict(J1=1.0, J2=0.1, J3=-0.05, Delta=1.0, B=(0.2, 0.0, 0.0))
+P4 = [1.0, 0.1, -0.05, 0.2, 0.0, 0.0]
+
+
+def _unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _oracle_objective(L, p, Ss, w, target, lam):
+    """FP64: sum_r e_r + lam * sum_r sum_q w (S^zz_r - target)^2."""
+    tot = 0.0
+    for S in Ss:
+        o = oracle.System(L, J1=p[0], J2=p[1], J3=p[2], B=p[3:6])
+        o.set_spins(S)
+        tot += o.energy()
+        if lam:
+            Z = o.ssf(["zz"], mode=2)[0]
+            tot += lam * float((w * ((Z[:, 0] - target) ** 2 + Z[:, 1] ** 2)).sum())
+    return tot
+
+
+def test_config4_gradients_vs_central_differences():
+    L, R = 8, 2
+    rng = np.random.default_rng(4)
+    g = pc.pyrochlore_system(L, n_replicas=R, seed=1, **C4)
+    g.ssf_configure(["zz"], 0, [])
+    Q = rng.integers(0, L, size=3)
+    target = ssf_fit.zz_target(g, Q)
+    assert target.max() > 1e5  # the spiral's Bragg peak
+    for r in range(R):
+        g.set_spins(_unit(rng, g.N(r)), r)
+    w = rng.uniform(0, 1, L ** 3)
+    lam = 1.0 / float((w * target ** 2).sum())
+    Ss = [g.spins(r) for r in range(R)]
+    spins = ag.spins_tensor(g).clone().requires_grad_(True)
+    params = torch.tensor(P4, dtype=torch.float64, requires_grad=True)
+    wt = torch.as_tensor(w, device="cuda")
+    tt = torch.as_tensor(target, device="cuda")
+    obj = ag.energy(g, spins, params).sum() + lam * ssf_fit.weighted_zz_loss(ag.ssf(g, spins), wt, tt).sum()
+    obj.backward()
+    gs = ag.project_tangent(spins.grad, spins.detach())[:, :3].cpu().numpy()
+    gp = params.grad.numpy()
+    h = 1e-4
+    # couplings and field
+    for k in range(6):
+        dp = np.zeros(6)
+        dp[k] = h
+        fd = (_oracle_objective(L, np.array(P4) + dp, Ss, w, target, 0.0) -
+              _oracle_objective(L, np.array(P4) - dp, Ss, w, target, 0.0)) / (2 * h)
+        assert gp[k] == pytest.approx(fd, rel=2e-3, abs=2e-3 * max(1.0, abs(fd))), (k, gp[k], fd)
+    # spins: tangent-projected gradients at a few sites of each replica
+    got, ref = [], []
+    for r in range(R):
+        for i in rng.choice(g.N(r), size=6, replace=False):
+            fd = np.zeros(3)
+            for a in range(3):
+                Sp = [S.copy() for S in Ss]
+                Sm = [S.copy() for S in Ss]
+                Sp[r][i, a] += h
+                Sm[r][i, a] -= h
+                fd[a] = (_oracle_objective(L, P4, [Sp[r]], w, target, lam) -
+                         _oracle_objective(L, P4, [Sm[r]], w, target, lam)) / (2 * h)
+            s = Ss[r][i]
+            ref.append(fd - fd.dot(s) * s)
+            got.append(gs[r * g.N(0) + i])
+    got, ref = np.array(got), np.array(ref)
+    assert np.abs(got - ref).max() <= 2e-3 * np.abs(ref).max(), (np.abs(got - ref).max(), np.abs(ref).max())
+
+
+def _oracle_quench(L, p, S0, steps, lr):
+    o = oracle.System(L, J1=p[0], J2=p[1], J3=p[2], B=p[3:6])
+    S = S0.copy()
+    for _ in range(steps):
+        o.set_spins(S)
+        hB = o.local_fields() - np.asarray(p[3:6])
+        t = hB - (hB * S).sum(1, keepdims=True) * S
+        S = S - lr * t
+        S /= np.linalg.norm(S, axis=1, keepdims=True)
+    o.set_spins(S)
+    return o.ssf(["zz"], mode=2)[0]
+
+
+def test_unrolled_quench_coupling_gradient_vs_central_differences():
+    L, R, steps, lr = 3, 2, 6, 0.05
+    rng = np.random.default_rng(9)
+    g = pc.pyrochlore_system(L, n_replicas=R, seed=2, **C4)
+    g.ssf_configure(["zz"], 0, [])
+    S0 = [_unit(rng, g.N(r)) for r in range(R)]
+    for r in range(R):
+        g.set_spins(S0[r], r)
+    w = rng.uniform(0, 1, L ** 3)
+    target = ssf_fit.zz_target(g, rng.integers(0, L, size=3))
+    for r in range(R):
+        g.set_spins(S0[r], r)
+    spins0 = ag.spins_tensor(g).clone()
+    params = torch.tensor(P4, dtype=torch.float64, requires_grad=True)
+    S = ssf_fit.unrolled_quench(g, spins0, params, steps, lr)
+    loss = ssf_fit.weighted_zz_loss(ag.ssf(g, S), torch.as_tensor(w, device="cuda"),
+                                    torch.as_tensor(target, device="cuda")).sum()
+    loss.backward()
+    S32 = [spins0[r * g.N(0):(r + 1) * g.N(0), :3].cpu().numpy().astype(np.float64) for r in range(R)]
+
+    def f(p):
+        tot = 0.0
+        for r in range(R):
+            Z = _oracle_quench(L, p, S32[r], steps, lr)
+            tot += float((w * ((Z[:, 0] - target) ** 2 + Z[:, 1] ** 2)).sum())
+        return tot
+
+    h = 1e-4
+    fd = []
+    for k in range(6):
+        dp = np.zeros(6)
+        dp[k] = h
+        fd.append((f(np.array(P4) + dp) - f(np.array(P4) - dp)) / (2 * h))
+    fd = np.array(fd)
+    got = params.grad.numpy()
+    assert np.abs(got - fd).max() <= 2e-2 * np.abs(fd).max(), (got, fd)
+
+
+def test_fit_recovers_couplings_from_quenched_ssf():
+    """Target: S^zz(q) after a 20-step quench from fixed random starts with
+    J = (1, 0.1, -0.05), B = (0.2, 0, 0). Fit (J2, J3) from (0, 0) through the
+    unrolled quench; the fit lands within 0.01 of the true couplings."""
+    L, R, steps, lr = 4, 4, 20, 0.05
+    rng = np.random.default_rng(21)
+    g = pc.pyrochlore_system(L, n_replicas=R, seed=3, **C4)
+    g.ssf_configure(["zz"], 0, [])
+    for r in range(R):
+        g.set_spins(_unit(rng, g.N(r)), r)
+    spins0 = ag.spins_tensor(g).clone()
+    true = torch.tensor(P4, dtype=torch.float64)
+    with torch.no_grad():
+        S_t = ssf_fit.unrolled_quench(g, spins0, true, steps, lr)
+        target_r = ag.ssf(g, S_t)[:, 0, :, 0]  # per replica
+    w = torch.ones(L ** 3, dtype=torch.float64, device="cuda")
+    # one target per replica: broadcast through the loss
+    p, hist = ssf_fit.fit_couplings(g, spins0, target_r, w, [1.0, 0.0, 0.0, 0.2, 0.0, 0.0], free=(1, 2),
+                                    steps=steps, lr=lr, iters=80, step_size=0.01)
+    assert hist[-1] < 1e-2 * hist[0], hist[[0, -1]]
+    assert abs(p[1] - 0.1) < 0.01 and abs(p[2] + 0.05) < 0.01, p
