@@ -42,10 +42,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait for phase `parity`: false if it did not complete within
-// kMaxPolls polls (each poll is a hardware-timed try_wait).
-constexpr int kMaxPolls = 1 << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (int i = 0; i < kMaxPolls; ++i)
+// `polls` polls (each poll is a hardware-timed try_wait).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int polls) {
+    for (int i = 0; i < polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -174,10 +173,12 @@ __device__ __forceinline__ unsigned staged_tile(const PassArgs& a, const Tile ti
             sincosf(float(a.theta[i]), &sn, &cs);
         }
     }
-    if (!mbar_wait_bounded(bar, 0)) {
-        // the copies did not land: report, give them one more bounded wait, skip the update
+    if (!mbar_wait_bounded(bar, 0, a.wait_polls)) {
+        // the copies did not land: report, give them one more wait (at the
+        // full bound, so none is left writing into this CTA's shared memory
+        // after it exits), skip the update
         if (threadIdx.x == 0) atomicExch(a.err, 1);
-        mbar_wait_bounded(bar, 0);
+        mbar_wait_bounded(bar, 0, kStagedMaxPolls);
         return 0u;
     }
     if (!live) return 0u;
