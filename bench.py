@@ -592,26 +592,64 @@ def run_extras(pc, torch, np):
     e1.record(stream)
     torch.cuda.synchronize()
     a_ms = e0.elapsed_time(e1) / n_a
+    # the same anneal step for the K = 32 seeds its statistics need, batched
+    # as replicas of one system
+    K = 32
+    a2 = pc.pyrochlore_system(16, n_replicas=K, J1=1.0, J2=-0.1, J3=0.05, B=(0, 0, 0), seed=22,
+                              schedule=WL["schedule"])
+    a2.set_stream(stream.cuda_stream)
+    a2.random_spins(3)
+    a2.autotune()
+    a2.ssf_configure(["xx", "yy", "zz", "xy", "xz", "yz"], K)
+    slots = np.arange(K, dtype=np.int32)
+
+    def a2_step():
+        a2.sweep(0.5, 16, 1, count=False)
+        a2.ssf_sample(slots)
+
+    for _ in range(3):
+        a2_step()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(10):
+        a2_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    a2_ms = e0.elapsed_time(e1) / 10
+    del a2
+    out["plain_L16_32_seeds"] = {"value": K * 16 * 16 ** 3 * 16 / (a2_ms * 1e-3), "unit": UNIT,
+                                 "config": "the L=16 anneal step for 32 seeds batched as replicas of one system",
+                                 "ms_per_step": a2_ms}
     out["plain_L16"] = {"value": a.N() * 16 / (a_ms * 1e-3), "unit": UNIT,
                         "config": "anneal L=16 (65,536 spins), J=(1,-0.1,0.05), B=0, T=0.5; step = 16 sweeps + "
                                   "one S(q) sample (xx,yy,zz,xy,xz,yz)",
                         "ms_per_step": a_ms, "tile": list(atile)}
     del a
-    # gradient form: 256 x L=8 energy + S^zz(q) forward/backward
+    # gradient form (the gradient configuration): 256 x L=8 uniform random
+    # configurations, J = (1, 0.1, -0.05), B = (0.2, 0, 0); objective = energy
+    # (with its gradients in the spins, J1..J3 and B) + sum_q w(q) |S^zz(q) -
+    # S_target(q)|^2, w ~ U[0, 1], S_target = S^zz of the spiral_byhand state
+    # at a seeded random Q
     from pyro_cmc_b200 import autograd as ag
+    from pyro_cmc_b200 import ssf_fit
     B = 256
     g = pc.pyrochlore_system(8, n_replicas=B, J1=1.0, J2=0.1, J3=-0.05, B=(0.2, 0, 0), seed=3)
     g.set_stream(stream.cuda_stream)
     g.ssf_configure(["zz"], 0, [])
+    rng = np.random.default_rng(4)
+    Q = rng.integers(0, 8, size=3)
+    target = torch.as_tensor(ssf_fit.zz_target(g, Q), device="cuda")
     g.random_spins(11)
     spins = ag.spins_tensor(g).clone().requires_grad_(True)
-    w = torch.rand((B, 1, 512), device="cuda", dtype=torch.float64)
-    target = torch.zeros((B, 1, 512), device="cuda", dtype=torch.float64)
+    params = torch.tensor([1.0, 0.1, -0.05, 0.2, 0.0, 0.0], dtype=torch.float64, requires_grad=True)
+    w = torch.as_tensor(rng.uniform(0, 1, 512), device="cuda")
+    lam = 1.0 / float((w * target ** 2).sum())
 
     def fwd_bwd():
-        e = ag.energy(g, spins)
-        S = ag.ssf(g, spins)
-        loss = (w * (S[..., 0] - target) ** 2).sum() * 1e-8 + e.sum()
+        spins.grad = None
+        params.grad = None
+        e = ag.energy(g, spins, params)
+        loss = e.sum() + lam * ssf_fit.weighted_zz_loss(ag.ssf(g, spins), w, target).sum()
         loss.backward()
         return loss
 
@@ -621,8 +659,8 @@ def run_extras(pc, torch, np):
     e0.record(stream)
     for _ in range(5):
         with torch.no_grad():
-            ag.energy(g, spins)
-            ag.ssf(g, spins)
+            e = ag.energy(g, spins, params)
+            lam * ssf_fit.weighted_zz_loss(ag.ssf(g, spins), w, target).sum() + e.sum()
     e1.record(stream)
     torch.cuda.synchronize()
     fwd_ms = e0.elapsed_time(e1) / 5
@@ -632,8 +670,10 @@ def run_extras(pc, torch, np):
     e1.record(stream)
     torch.cuda.synchronize()
     fb_ms = e0.elapsed_time(e1) / 5
-    out["grad"] = {"value": B * g.N() / (fb_ms * 1e-3), "unit": "spins/s (energy + S^zz(q) forward and backward)",
-                   "config": "256 x L=8 (2,097,152 spins), J=(1,0.1,-0.05), B=(0.2,0,0)",
+    out["grad"] = {"value": B * g.N() / (fb_ms * 1e-3), "unit": "spins/s (energy + S^zz(q) loss, forward and backward)",
+                   "config": "256 x L=8 (2,097,152 spins), J=(1,0.1,-0.05), B=(0.2,0,0); loss = e + "
+                             "sum_q w(q)|S^zz(q) - S_target(q)|^2 / norm, w ~ U[0,1], S_target = S^zz of the "
+                             "spiral_byhand state at seeded random Q; gradients in the spins, J1..J3 and B",
                    "forward_ms": fwd_ms, "forward_backward_ms": fb_ms,
                    "backward_over_forward": (fb_ms - fwd_ms) / fwd_ms}
     del g

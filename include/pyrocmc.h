@@ -233,6 +233,15 @@ int pc_ssf_clear(pc_system* sys, int slot);
  * out[n_corr][n_k][2] (host). */
 int pc_ssf_current(pc_system* sys, int replica, double* out);
 
+/* save_ft_spin_state (src/MC.cpp:320-368): the raw per-sublattice DFT over
+ * cells of each spin component of one replica, WITHOUT the sublattice phase
+ * exp(-i q.r_mu) (which the reference also leaves to post-processing):
+ * out[3][16][n_k][2] (host; components x, y, z; sublattice sl = 4f + p;
+ * k flat as above; re, im), A^a_sl(K) = sum_cells exp(-2 pi i K.n / L) S^a.
+ * Computed on the device in FP32 (the transforms of the resolved S(q)),
+ * returned in FP64. Needs L to factor into two parts <= 8 (L <= 64). */
+int pc_spin_ft(pc_system* sys, int replica, double* out);
+
 /* -------------------------------------------------------- tempering / energy */
 
 /* Sets up batched parallel tempering over all replicas (replaces the MPI
@@ -361,6 +370,14 @@ int pc_last_kernel_times(pc_system* sys, double* metropolis_ms, double* overrela
  * current device; needs no pc_system. */
 int pc_lt_minimum(int L, double J1, double J2, double J3, double Delta, double* lambda_map, double* e_per_spin,
                   int64_t* k_star, double* eigvec);
+/* Bound of the first wait of the staged colour pass (load variant 3) on its
+ * bulk copies, in polls of a hardware-timed try_wait (default and maximum
+ * 2^22; < 0 restores the default). For tests of the timeout path: with 0
+ * every staged pass gives up at once, sets the device error flag, waits for
+ * its copies at the full bound (none is left in flight), skips its updates,
+ * and the call returns PC_ERR_TIMEOUT; the system stays usable. No
+ * counterpart in the reference (it has no device waits). */
+int pc_set_wait_limit(pc_system* sys, int polls);
 /* Enables per-kernel CUDA-event timing (off by default). */
 int pc_set_kernel_timing(pc_system* sys, int on);
 /* Launch overlap of consecutive colour passes (off by default; pc_autotune

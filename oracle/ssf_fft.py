@@ -35,6 +35,16 @@ def amplitudes(S: np.ndarray, L: int) -> np.ndarray:
     return B.reshape(3, L ** 3)
 
 
+def sublattice_ft(S: np.ndarray, L: int) -> np.ndarray:
+    """save_ft_spin_state's spin_ft (src/MC.cpp:320-368): per component a and
+    sublattice sl the 3-D DFT over cells (forward sign, unnormalised) of S^a
+    on that sublattice, without the sublattice phase. Returns complex
+    [3, 16, L^3], k flat in C order over (Kx, Ky, Kz)."""
+    S = np.asarray(S, dtype=np.float64).reshape(16, L, L, L, 3)  # [sl][cz][cy][cx][a]
+    F = np.fft.fftn(S, axes=(1, 2, 3))  # [sl][Kz][Ky][Kx][a]
+    return np.transpose(F, (4, 0, 3, 2, 1)).reshape(3, 16, L ** 3)
+
+
 def ssf(S: np.ndarray, L: int, corr) -> np.ndarray:
     """S^{ab}(k) = conj(B^a) B^b for each correlator name; [n_corr, L^3, 2]."""
     B = amplitudes(S, L)

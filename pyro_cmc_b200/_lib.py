@@ -82,6 +82,7 @@ _SIGNATURES = {
     "pc_energy_grad": (_I, [_P, _DP, _DP, _P, _DP, _DP]),
     "pc_energy_grad_field": (_I, [_P, _P, _DP, _DP, _P, _DP, _DP]),
     "pc_set_wait_limit": (_I, [_P, _I]),
+    "pc_spin_ft": (_I, [_P, _I, _DP]),
     "pc_ssf_forward": (_I, [_P, _P]),
     "pc_ssf_backward": (_I, [_P, _P, _P]),
     "pc_energy_noalloc": (_I, [_P, _I, _DP, _P, _P]),

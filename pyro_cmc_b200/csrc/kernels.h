@@ -53,7 +53,11 @@ struct PassArgs {
     PyroMats mats;
     int staged_rl;  // load variant 3: largest tile (rows x L sites); sizes the shared row blocks
     int* err;       // device error flag (set by a kernel whose bounded wait ran out)
+    int wait_polls; // load variant 3: polls of the first wait on the staged copies (kStagedMaxPolls)
 };
+// Bound of every wait of the staged pass on its bulk copies (polls of a
+// hardware-timed try_wait).
+constexpr int kStagedMaxPolls = 1 << 22;
 
 // pdl: launch with programmatic dependent launch (the kernel waits for the
 // previous kernel on the stream with griddepcontrol.wait before touching spins)
@@ -208,6 +212,12 @@ struct SsfOut {
     float2* amp;
 };
 void launch_ssf_z(const SsfGeom& g, const float2* G, const SsfOut& o, cudaStream_t st);
+// The per-sublattice transforms alone (after launch_ssf_xy with resolved = 1):
+// the z-DFT in place, leaving A[rep][3 * 16 (component, sublattice)][Kz][Ky][Kx]
+// (float2), the raw DFT over cells of each component on each sublattice.
+void launch_ssf_zdft_res(const SsfGeom& g, float2* A, cudaStream_t st);
+// Whether line lengths P, Q have the fixed-radix (resolved-capable) kernels.
+bool ssf_resolved_supported(int P, int Q);
 // Backward: Y^c(K) from upstream dS (val layout) and amplitudes; then adjoint
 // transform into grad_S (float4 per site, xyz components written).
 void launch_ssf_adjoint(const SsfGeom& g, const SsfOut& o, const double* dval, const float2* amp, float2* H,

@@ -751,21 +751,28 @@ __global__ void __launch_bounds__(256) ssf_z_kernel(const SsfGeom g, const float
     }
 }
 
+bool ssf_resolved_supported(int P, int Q) { return ssf_fast_path(P, Q); }
+
+void launch_ssf_zdft_res(const SsfGeom& g, float2* A, cudaStream_t st) {
+    const int L = g.L;
+    const int Cr = ssf_chunk_res(L);
+    const size_t smem = sizeof(float2) * (size_t(9) * L + 48 * (size_t(L) * (Cr + 1) + 1));
+    const int grid = g.n_rep * L * ((L + Cr - 1) / Cr);
+    switch (L) {
+        case 64: ssf_zdft_res_kernel<64><<<grid, 256, smem, st>>>(g, A); break;
+        case 32: ssf_zdft_res_kernel<32><<<grid, 256, smem, st>>>(g, A); break;
+        case 16: ssf_zdft_res_kernel<16><<<grid, 256, smem, st>>>(g, A); break;
+        case 8: ssf_zdft_res_kernel<8><<<grid, 256, smem, st>>>(g, A); break;
+        default: ssf_zdft_res_kernel<0><<<grid, 256, smem, st>>>(g, A);
+    }
+}
+
 void launch_ssf_z(const SsfGeom& g, const float2* G, const SsfOut& o, cudaStream_t st) {
     const int L = g.L, C = ssf_chunk(L);
     const int n_chunk = (L + C - 1) / C;
     if (ssf_fast_path(g.P, g.Q) && g.resolved) {
-        const int Cr = ssf_chunk_res(L);
-        const size_t smem = sizeof(float2) * (size_t(9) * L + 48 * (size_t(L) * (Cr + 1) + 1));
-        const int grid = g.n_rep * L * ((L + Cr - 1) / Cr);
         float2* A = const_cast<float2*>(G);
-        switch (L) {
-            case 64: ssf_zdft_res_kernel<64><<<grid, 256, smem, st>>>(g, A); break;
-            case 32: ssf_zdft_res_kernel<32><<<grid, 256, smem, st>>>(g, A); break;
-            case 16: ssf_zdft_res_kernel<16><<<grid, 256, smem, st>>>(g, A); break;
-            case 8: ssf_zdft_res_kernel<8><<<grid, 256, smem, st>>>(g, A); break;
-            default: ssf_zdft_res_kernel<0><<<grid, 256, smem, st>>>(g, A);
-        }
+        launch_ssf_zdft_res(g, A, st);
         ssf_accum_res_kernel<<<g.n_rep * L * L * L, 256, 0, st>>>(g, A, o);
         return;
     }

@@ -158,6 +158,7 @@ struct pc_system {
     DevBuf<unsigned long long> d_acc;
     DevBuf<int> d_err;  // set by a kernel whose bounded wait ran out
     int staged_rl = 0;  // load variant 3: largest row tile (R*L sites)
+    int wait_polls = pc::kStagedMaxPolls;  // load variant 3: bound of the first wait (pc_set_wait_limit)
     DevBuf<SlTable> d_tab_active, d_tab_full;
     std::vector<DevBuf<Tile>> d_colour_tiles;
     std::vector<int> n_colour_tiles;
@@ -651,6 +652,7 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.mats = s->mats;
     a.staged_rl = s->staged_rl;
     a.err = s->d_err.p;
+    a.wait_polls = s->wait_polls;
     return a;
 }
 
@@ -1785,6 +1787,46 @@ int pc_ssf_current(pc_system* sys, int replica, double* out) {
     return PC_OK;
 }
 
+int pc_spin_ft(pc_system* sys, int replica, double* out) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    rc = check_rep(sys, replica);
+    if (rc) return rc;
+    if (!out) return fail(PC_ERR_INVALID, "null output");
+    rc = ensure_groups(sys);
+    if (rc) return rc;
+    const int L = sys->L[size_t(replica)];
+    SsfGroup* grp = nullptr;
+    for (auto& g : sys->groups)
+        if (g.L == L) grp = &g;
+    if (!grp || !pc::ssf_resolved_supported(grp->P, grp->Q))
+        return fail(PC_ERR_UNSUPPORTED, "the per-sublattice transform needs L to factor into two parts <= 8");
+    DevBuf<int32_t> idx;
+    PC_CK(idx.alloc(1));
+    PC_CK(cudaMemcpy(idx.p, &replica, sizeof(int32_t), cudaMemcpyHostToDevice));
+    pc::SsfGeom geom{grp->L, grp->P, grp->Q, 1, idx.p, 1};
+    pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, grp->d_G.p, sys->stream);
+    PC_LAUNCH_CK();
+    pc::launch_ssf_zdft_res(geom, grp->d_G.p, sys->stream);
+    PC_LAUNCH_CK();
+    sys->launches += 2;
+    const size_t L3 = size_t(L) * L * L;
+    std::vector<float2> A(48 * L3);
+    PC_CK(cudaMemcpyAsync(A.data(), grp->d_G.p, sizeof(float2) * A.size(), cudaMemcpyDeviceToHost, sys->stream));
+    PC_CK(cudaStreamSynchronize(sys->stream));
+    // A[plane = 16 c + sl][Kz][Ky][Kx] -> out[c][sl][k = (Kx L + Ky) L + Kz][re, im]
+    for (size_t pl = 0; pl < 48; ++pl)
+        for (int kz = 0; kz < L; ++kz)
+            for (int ky = 0; ky < L; ++ky)
+                for (int kx = 0; kx < L; ++kx) {
+                    const float2 v = A[pl * L3 + (size_t(kz) * L + ky) * L + kx];
+                    double* o = out + (pl * L3 + (size_t(kx) * L + ky) * L + kz) * 2;
+                    o[0] = v.x;
+                    o[1] = v.y;
+                }
+    return PC_OK;
+}
+
 // ------------------------------------------------------------- tempering
 int pc_pt_configure(pc_system* sys, const double* T) {
     int rc = check_sys(sys);
@@ -2309,6 +2351,14 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     if (e_out) *e_out = *st_e;
     if (accepted) *accepted = *st_acc;
     return device_error_flag(sys, *st_flag);
+}
+
+int pc_set_wait_limit(pc_system* sys, int polls) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    sys->wait_polls = polls < 0 ? pc::kStagedMaxPolls : std::min(polls, pc::kStagedMaxPolls);
+    sys->drop_graphs();  // captured passes carry the old bound
+    return PC_OK;
 }
 
 int pc_set_kernel_timing(pc_system* sys, int on) {

@@ -356,6 +356,14 @@ class System:
         call("pc_ssf_current", self._h, replica, _dp(out))
         return out
 
+    def spin_ft(self, replica: int = 0):
+        """save_ft_spin_state's array: the per-sublattice DFT over cells of
+        each component, without sublattice phases, [3, 16, n_k, 2]
+        (pc_spin_ft)."""
+        out = np.empty((3, 16, self.Nc(replica), 2))
+        call("pc_spin_ft", self._h, replica, _dp(out))
+        return out
+
     def ssf_forward_device(self, out_ptr: int):
         call("pc_ssf_forward", self._h, C.c_void_p(out_ptr))
 

@@ -228,4 +228,17 @@ void save_spin_state(Lattice& lat, const std::filesystem::path& file_path) {
     f.close();
 }
 
+// save_ft_spin_state (src/MC.cpp:320-368): dataset "spin_ft" [3, n_sl, n_k, 2],
+// the per-sublattice DFT over cells of each spin component without the
+// sublattice phase, computed on the device (pc_spin_ft).
+void save_ft_spin_state(Lattice& lat, const std::filesystem::path& file_path) {
+    const uint64_t nk = uint64_t(lat.num_spins() / 16);
+    std::vector<double> ft(size_t(3 * 16 * nk * 2));
+    lat.to_device();
+    check(pc_spin_ft(lat.device(), 0, ft.data()));
+    OutFile f(file_path.string());
+    f.dataset_f64("spin_ft", {3, 16, nk, 2}, ft.data());
+    f.close();
+}
+
 }  // namespace CMC

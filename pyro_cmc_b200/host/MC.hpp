@@ -154,5 +154,8 @@ class OutFile;
 void write_geometry_group(OutFile& f, Lattice& sc, const char* group_name = "geometry");
 // .spins file (src/MC.cpp:371-406): spin_pos int32 [N,3], spin_orientation f64 [N,3]
 void save_spin_state(Lattice& lat, const std::filesystem::path& file_path);
+// .spins_ft file (src/MC.cpp:320-368): spin_ft f64 [3, 16, n_k, 2], the raw
+// per-sublattice DFT of each spin component (no sublattice phase)
+void save_ft_spin_state(Lattice& lat, const std::filesystem::path& file_path);
 
 }  // namespace CMC

@@ -180,3 +180,34 @@ def test_step_host_matches_the_same_calls(n_sweep, ssf_every):
         for x, y in zip(a.ssf_read(0), b.ssf_read(0)):
             np.testing.assert_array_equal(np.asarray(x), np.asarray(y))
         S_in = S_out
+
+
+@pytest.mark.parametrize("L", [2, 4, 8])
+def test_spin_ft_matches_oracle_sublattice_dft(L):
+    """pc_spin_ft (save_ft_spin_state's array, src/MC.cpp:320-368) against the
+    numpy restatement of the per-sublattice DFT (itself pinned on the
+    oracle's correlate); 1e-5 relative to the largest amplitude."""
+    from oracle import ssf_fft
+    g = pc.pyrochlore_system(L, J1=1.0, seed=1)
+    g.random_spins(L)
+    ft = g.spin_ft()
+    ref = ssf_fft.sublattice_ft(g.spins(), L)
+    assert ft.shape == (3, 16, L ** 3, 2)
+    scale = np.abs(ref).max()
+    assert np.abs(ft[..., 0] - ref.real).max() <= 1e-5 * scale
+    assert np.abs(ft[..., 1] - ref.imag).max() <= 1e-5 * scale
+
+
+def test_anneal_save_state_ft(tmp_path):
+    args = ["-o", tmp_path, "-s", 5, 4, "--J1", 1, "--T_sample", 0.5, "--n_steps", 4, "--n_sweep", 2,
+            "--n_burn_in", 2, "--n_sample", 2, "--init_uniform", "--save_state", "--save_state_ft"]
+    out = run("anneal", *args)
+    assert "Saving spin state FT" in out
+    from oracle import ssf_fft
+    with File(only(tmp_path, ".spins.npz")) as f:
+        S = f["/spin_orientation"][:]
+    with File(only(tmp_path, ".spins_ft.npz")) as f:
+        ft = f["/spin_ft"][:]
+    assert ft.shape == (3, 16, 64, 2)
+    ref = ssf_fft.sublattice_ft(S, 4)
+    assert np.abs(ft[..., 0] + 1j * ft[..., 1] - ref).max() <= 1e-5 * np.abs(ref).max()

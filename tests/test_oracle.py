@@ -322,3 +322,22 @@ def test_separable_ssf_equals_direct_sum(L):
     a = o.ssf(corr, mode=0)
     b = o.ssf(corr, mode=2)
     assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+
+
+@pytest.mark.parametrize("L", [1, 2, 3])
+def test_sublattice_ft_matches_oracle_correlate(L):
+    """oracle.ssf_fft.sublattice_ft (the spin_ft restatement) against the
+    oracle's own per-sublattice DFT: conj(A^a_mu) A^b_nu equals the resolved
+    correlator of the ssf_manager::sample restatement."""
+    from oracle import ssf_fft
+    o = oracle.System(L, J1=1.0, seed=2)
+    o.random_spins(11)
+    corr = ["xx", "yz", "zy"]
+    _, res = o.ssf(corr, mode=1, resolved=True)  # [corr][k][mu][nu][2]
+    A = ssf_fft.sublattice_ft(o.spins(), L)
+    ax = {"x": 0, "y": 1, "z": 2}
+    for c, name in enumerate(corr):
+        C = np.conj(A[ax[name[0]]])[:, None, :] * A[ax[name[1]]][None, :, :]  # [mu][nu][k]
+        C = np.transpose(C, (2, 0, 1))
+        assert np.abs(C.real - res[c, ..., 0]).max() <= 1e-10 * max(1.0, np.abs(res).max())
+        assert np.abs(C.imag - res[c, ..., 1]).max() <= 1e-10 * max(1.0, np.abs(res).max())
