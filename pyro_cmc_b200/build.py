@@ -72,8 +72,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 HOST = os.path.join(HERE, "host")
 BIN = os.path.join(HERE, "bin")
-HOST_LIB_SOURCES = ["MC.cpp", "managers.cpp", "h5out.cpp"]
-HOST_HEADERS = ["MC.hpp", "managers.hpp", "h5out.hpp", "cli_bits.hpp", "vec3.hpp"]
+HOST_LIB_SOURCES = ["MC.cpp", "managers.cpp", "h5out.cpp", "h5file.cpp"]
+HOST_HEADERS = ["MC.hpp", "managers.hpp", "h5out.hpp", "h5file.hpp", "cli_bits.hpp", "vec3.hpp"]
 DRIVERS = ["anneal", "fieldcool", "temper", "spiral_byhand", "ltgs"]
 
 

@@ -2,11 +2,12 @@
 // console lines and output tree of the reference's src/anneal.cpp.
 //
 // Differences from the reference, all deliberate:
-//  * the output is <name>.out.npz with the /ssf, /energy, /geometry tree
-//    (h5out.hpp), not HDF5;
+//  * the output <name>.out.h5 (/ssf, /energy, /geometry) is written by this
+//    package's own HDF5 writer (h5file.hpp); --npz writes the same tree as
+//    <name>.out.npz;
 //  * --seed is the Philox key itself, not an index into a seed table;
-//  * --save_state writes the spins (.spins.npz) and --save_state_ft the
-//    per-sublattice spin DFT (.spins_ft.npz) as the README documents (the
+//  * --save_state writes the spins (.spins.h5) and --save_state_ft the
+//    per-sublattice spin DFT (.spindft.h5) as the README documents (the
 //    reference swaps the two flags);
 //  * additions: --init_uniform (start uniform on S^2 instead of the
 //    default-constructed zero spins), --correlators (default: the reference's
@@ -24,10 +25,11 @@ using namespace CMC;
 
 int main(int argc, char* argv[]) {
     ArgParser prog("anneal");
+    prog.flag({"--npz"}, "Write the output as NumPy .npz archives instead of HDF5 (.h5)");
     prog.option({"--output_dir", "-o"}, "Path to output", "", true);
     prog.option({"--seed", "-s"}, "Seed of the RNG (Philox key)", "", true);
-    prog.flag({"--save_state"}, "Also write the final spin configuration to .spins.npz");
-    prog.flag({"--save_state_ft"}, "Also write the sublattice-resolved spin DFT to .spins_ft.npz");
+    prog.flag({"--save_state"}, "Also write the final spin configuration to .spins.h5 (.spins.npz with --npz)");
+    prog.flag({"--save_state_ft"}, "Also write the sublattice-resolved spin DFT to .spindft.h5 (.spindft.npz with --npz)");
     prog.flag({"--init_spiral"}, "Pre-initialise spins to a spiral with the wavevector given by --Q (requires --Q)");
     prog.flag({"--init_uniform"}, "Start from spins uniform on the sphere (device Philox) instead of zero");
     prog.option({"--T_hot"}, "Temperature  to begin annealing from");
@@ -51,6 +53,7 @@ int main(int argc, char* argv[]) {
         std::exit(1);
     }
     try {
+        const std::string ext = prog.boolean("--npz") ? ".npz" : ".h5";
         const std::filesystem::path outdir(prog.str("--output_dir"));
         if (!std::filesystem::exists(outdir)) throw std::runtime_error("Cannot open outdir");
         const uint64_t seed = uint64_t(prog.integer("--seed"));
@@ -89,7 +92,7 @@ int main(int argc, char* argv[]) {
             init_spiral_state(lat, Q_rounded, spiral_axis);
         }
         energy_manager e_manager;
-        const auto file_path = outdir / (name.str() + ".out.npz");
+        const auto file_path = outdir / (name.str() + ".out" + ext);
         OutFile file(file_path.string());
         ssf_manager ssfm(lat, prog.strs("--correlators"), file, "/ssf", T_sample, true);
         if (prog.boolean("--ssf_resolved")) ssfm.set_sublattice_resolved(true);
@@ -125,12 +128,12 @@ int main(int argc, char* argv[]) {
         file.close();
         std::cout << "Saved to \n" << file_path << std::endl;
         if (prog.boolean("--save_state")) {
-            const auto f = outdir / (name.str() + ".spins.npz");
+            const auto f = outdir / (name.str() + ".spins" + ext);
             std::printf("Saving spin state to %s\n", f.string().c_str());
             save_spin_state(lat, f);
         }
         if (prog.boolean("--save_state_ft")) {
-            const auto f = outdir / (name.str() + ".spins_ft.npz");
+            const auto f = outdir / (name.str() + ".spindft" + ext);
             std::printf("Saving spin state FT to %s\n", f.string().c_str());
             save_ft_spin_state(lat, f);
         }

@@ -14,9 +14,10 @@ using namespace CMC;
 
 int main(int argc, char* argv[]) {
     ArgParser prog("fieldcool");
+    prog.flag({"--npz"}, "Write the output as NumPy .npz archives instead of HDF5 (.h5)");
     prog.option({"--output_dir", "-o"}, "Path to output", "", true);
     prog.option({"--seed", "-s"}, "Seed of the RNG (Philox key)", "", true);
-    prog.flag({"--save_state"}, "Also write the final spin configuration to .spins.npz");
+    prog.flag({"--save_state"}, "Also write the final spin configuration to .spins.h5 (.spins.npz with --npz)");
     prog.flag({"--init_spiral"}, "Pre-initialise spins to a spiral with the wavevector given by --Q (requires --Q)");
     prog.flag({"--init_uniform"}, "Start from spins uniform on the sphere (device Philox) instead of zero");
     prog.option({"--T_hot"}, "Temperature  to begin annealing from");
@@ -35,6 +36,7 @@ int main(int argc, char* argv[]) {
         std::exit(1);
     }
     try {
+        const std::string ext = prog.boolean("--npz") ? ".npz" : ".h5";
         const std::filesystem::path outdir(prog.str("--output_dir"));
         if (!std::filesystem::exists(outdir)) throw std::runtime_error("Cannot open outdir");
         const uint64_t seed = uint64_t(prog.integer("--seed"));
@@ -85,7 +87,7 @@ int main(int argc, char* argv[]) {
             std::printf("[cold] Iter %4zu T=%.3e Acceptance rate: %.2f%%\n", i, T, accepted * 100.0 / N / double(n_sweep));
             ssfm.sample();
         }
-        const auto file_path = outdir / (name.str() + ".out.npz");
+        const auto file_path = outdir / (name.str() + ".out" + ext);
         OutFile file(file_path.string());
         ssfm.write_group(file, "/ssf");
         e_manager.write_group(file, "/energy");
@@ -93,7 +95,7 @@ int main(int argc, char* argv[]) {
         file.close();
         std::cout << "Saved to \n" << file_path << std::endl;
         if (prog.boolean("--save_state")) {
-            const auto f = outdir / (name.str() + ".spins.npz");
+            const auto f = outdir / (name.str() + ".spins" + ext);
             std::printf("Saving spin state to %s\n", f.string().c_str());
             save_spin_state(lat, f);
         }

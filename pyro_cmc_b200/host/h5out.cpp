@@ -1,4 +1,5 @@
-// h5out.cpp -- .npz writer (zip of .npy members, stored, Zip64 when large).
+// h5out.cpp -- HDF5 through H5File, or an .npz writer (zip of .npy members,
+// stored, Zip64 when large).
 #include "h5out.hpp"
 
 #include <cstdio>
@@ -65,9 +66,17 @@ std::string clean(const std::string& path) {
     return p;
 }
 
+bool ends_with(const std::string& s, const std::string& t) {
+    return s.size() >= t.size() && s.compare(s.size() - t.size(), t.size(), t) == 0;
+}
+
 }  // namespace
 
 OutFile::OutFile(const std::string& path) : path_(path) {
+    if (!ends_with(path, ".npz")) {
+        h5_.reset(new H5File(path));
+        return;
+    }
     fp_ = std::fopen(path.c_str(), "wb");
     if (!fp_) throw std::runtime_error("Failed to create output file: " + path);
 }
@@ -115,6 +124,7 @@ void OutFile::member(const std::string& name, const std::string& dtype, const st
 
 void OutFile::dataset(const std::string& path, const std::string& dtype, const std::vector<uint64_t>& shape,
                       const void* data, size_t itemsize) {
+    if (h5_) return h5_->dataset(path, dtype, shape, data);
     uint64_t n = 1;
     for (uint64_t s : shape) n *= s;
     member(clean(path) + ".npy", dtype, shape, data, size_t(n) * itemsize);
@@ -122,6 +132,7 @@ void OutFile::dataset(const std::string& path, const std::string& dtype, const s
 
 void OutFile::attribute(const std::string& group, const std::string& name, const std::string& dtype,
                         const std::vector<uint64_t>& shape, const void* data, size_t itemsize) {
+    if (h5_) return h5_->attribute(group, name, dtype, shape, data);
     uint64_t n = 1;
     for (uint64_t s : shape) n *= s;
     std::string g = clean(group);
@@ -129,6 +140,7 @@ void OutFile::attribute(const std::string& group, const std::string& name, const
 }
 
 void OutFile::dataset_strings(const std::string& path, const std::vector<std::string>& s) {
+    if (h5_) return h5_->strings(path, s);
     size_t w = 1;
     for (const auto& x : s) w = std::max(w, x.size());
     std::vector<char> buf(s.size() * w, 0);
@@ -136,8 +148,36 @@ void OutFile::dataset_strings(const std::string& path, const std::vector<std::st
     dataset(path, "|S" + std::to_string(w), {uint64_t(s.size())}, buf.data(), w);
 }
 
+size_t OutFile::reserve(const std::string& path, const std::string& dtype, const std::vector<uint64_t>& shape,
+                        size_t itemsize) {
+    if (h5_) return h5_->reserve(path, dtype, shape);
+    if (closed_) throw std::runtime_error("OutFile: write after close");
+    uint64_t n = 1;
+    for (uint64_t s : shape) n *= s;
+    pending_.push_back(Pending{path, dtype, shape, std::vector<unsigned char>(size_t(n) * itemsize, 0)});
+    return pending_.size() - 1;
+}
+
+void OutFile::write_slice(size_t handle, uint64_t off, const void* data, size_t nbytes) {
+    if (h5_) return h5_->write_at(handle, off, data, nbytes);
+    if (handle >= pending_.size()) throw std::invalid_argument("OutFile: bad handle");
+    auto& d = pending_[handle].data;
+    if (off + nbytes > d.size()) throw std::out_of_range("OutFile: slice beyond the reserved dataset");
+    std::memcpy(d.data() + off, data, nbytes);
+}
+
+void OutFile::commit() {
+    if (h5_) h5_->commit();
+}
+
 void OutFile::close() {
+    if (h5_) {
+        h5_->close();
+        return;
+    }
     if (closed_ || !fp_) return;
+    for (auto& p : pending_) member(clean(p.path) + ".npy", p.dtype, p.shape, p.data.data(), p.data.size());
+    pending_.clear();
     FILE* f = static_cast<FILE*>(fp_);
     std::vector<unsigned char> cd;
     for (const auto& e : entries_) {

@@ -3,7 +3,7 @@
 // same flags (provide_physical_args, --output_dir optional), the same printed
 // lines, and the output tree eigenvalue_map, k_star_idx, k_star_vec, E_min,
 // eigenvector [48, 2], /geometry/index_cell, /geometry/recip_vectors and the
-// root attribute k_dims, in <name>ltgs.out.npz.
+// root attribute k_dims, in <name>ltgs.out.h5 (<name>ltgs.out.npz with --npz).
 #include <cstdio>
 #include <filesystem>
 #include <iostream>
@@ -16,6 +16,7 @@ using namespace CMC;
 
 int main(int argc, char* argv[]) {
     ArgParser prog("ltgs");
+    prog.flag({"--npz"}, "Write the output as NumPy .npz archives instead of HDF5 (.h5)");
     prog.option({"--output_dir", "-o"}, "Path to output directory");
     provide_physical_args(prog);
     try {
@@ -25,6 +26,7 @@ int main(int argc, char* argv[]) {
         return 1;
     }
     try {
+        const std::string ext = prog.boolean("--npz") ? ".npz" : ".h5";
         std::filesystem::path outdir;
         if (prog.is_used("--output_dir")) {
             outdir = prog.str("--output_dir");
@@ -54,7 +56,7 @@ int main(int argc, char* argv[]) {
         std::printf("k*  idx = [%lld, %lld, %lld]\n", (long long)ks[0], (long long)ks[1], (long long)ks[2]);
         std::printf("k*  vec = [%.4f, %.4f, %.4f]  (rad / coord-unit)\n", kv[0], kv[1], kv[2]);
         if (!prog.is_used("--output_dir")) return 0;
-        const auto file_path = outdir / (name_LJ123(prog) + "ltgs.out.npz");
+        const auto file_path = outdir / (name_LJ123(prog) + "ltgs.out" + ext);
         OutFile f(file_path.string());
         f.dataset_f64("/eigenvalue_map", {uint64_t(Nk)}, lam.data());
         f.dataset_i64("/k_star_idx", {3}, ks);

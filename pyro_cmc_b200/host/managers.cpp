@@ -36,10 +36,11 @@ ssf_manager::ssf_manager(CMC::Lattice& sc, const std::vector<std::string>& corre
     configure(correlator_names);
 }
 
-ssf_manager::ssf_manager(CMC::Lattice& sc, const std::vector<std::string>& correlator_names, CMC::OutFile&,
+ssf_manager::ssf_manager(CMC::Lattice& sc, const std::vector<std::string>& correlator_names, CMC::OutFile& file,
                          const char* group_name, const std::vector<double>& T_sample, bool store_error_term)
     : ssf_manager(sc, correlator_names, 0, store_error_term) {
     streaming_ = true;
+    file_ = &file;
     group_ = group_name;
     T_sorted_ = T_sample;
     std::sort(T_sorted_.begin(), T_sorted_.end());
@@ -118,7 +119,21 @@ void ssf_manager::get_flat_buffer(size_t t_idx, std::vector<double>& corr_buf, s
     if (!store_error_term_) corr_sq_buf.clear();
 }
 
-// include/ssf_manager.hpp:413-465: store the current temperature in its slot
+// include/ssf_manager.hpp:375-405: static_corr[n_corr, n_T, n_k, 2] (or the
+// sublattice-resolved [n_corr, n_T, n_k, 16, 16, 2]) reserved in full, zeros
+// until a temperature is flushed into its slot.
+void ssf_manager::reserve_streamed() {
+    if (reserved_) return;
+    const uint64_t nc = get_n_corr(), nT = T_sorted_.size(), nk = uint64_t(n_kpoints_);
+    const std::vector<uint64_t> shape = ew_ == 512 ? std::vector<uint64_t>{nc, nT, nk, 16, 16, 2}
+                                                   : std::vector<uint64_t>{nc, nT, nk, 2};
+    h_sum_ = file_->reserve(group_ + "/static_corr", "<f8", shape, 8);
+    if (store_error_term_) h_sq_ = file_->reserve(group_ + "/static_corr_2", "<f8", shape, 8);
+    file_->commit();
+    reserved_ = true;
+}
+
+// include/ssf_manager.hpp:413-465: write the current temperature into its slot
 void ssf_manager::flush() {
     if (!streaming_) throw std::logic_error("flush() called on non-streaming ssf_manager");
     if (!have_current_) throw std::logic_error("flush() called with no accumulated data");
@@ -128,7 +143,14 @@ void ssf_manager::flush() {
     std::vector<double> s, q;
     get_flat_buffer(curr_idx, s, q);
     flushed_.erase(size_t(-1));
-    flushed_[size_t(it - T_sorted_.begin())] = {std::move(s), std::move(q)};
+    reserve_streamed();
+    const size_t slot = size_t(it - T_sorted_.begin()), nT = T_sorted_.size();
+    const size_t row = size_t(n_kpoints_) * ew_;  // doubles per (correlator, temperature)
+    for (size_t c = 0; c < get_n_corr(); ++c) {
+        const uint64_t off = uint64_t((c * nT + slot) * row) * 8;
+        file_->write_slice(h_sum_, off, s.data() + c * row, row * 8);
+        if (store_error_term_) file_->write_slice(h_sq_, off, q.data() + c * row, row * 8);
+    }
     have_current_ = false;
 }
 
@@ -144,7 +166,12 @@ void ssf_manager::write_group(CMC::OutFile& f, const char* group_name) {
     std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return T_list[a] < T_list[b]; });
     const size_t n_T_out = streaming_ ? T_sorted_.size() : n_T;
     const size_t ew = ew_;
-    std::vector<double> sum(nc * n_T_out * nk * ew, 0.0), sq(sum.size(), 0.0);
+    if (streaming_) {
+        // static_corr and static_corr_2 are already in the stream's file
+        if (&f != file_) throw std::invalid_argument("ssf_manager::write_group: streaming writes into its own file");
+        reserve_streamed();
+    }
+    std::vector<double> sum(streaming_ ? 0 : nc * n_T_out * nk * ew, 0.0), sq(sum.size(), 0.0);
     auto place = [&](size_t slot, const std::vector<double>& s, const std::vector<double>& q) {
         for (size_t c = 0; c < nc; ++c)
             for (size_t j = 0; j < nk * ew; ++j) {
@@ -152,18 +179,17 @@ void ssf_manager::write_group(CMC::OutFile& f, const char* group_name) {
                 if (!q.empty()) sq[(c * n_T_out + slot) * nk * ew + j] = q[c * nk * ew + j];
             }
     };
-    if (streaming_) {
-        for (const auto& kv : flushed_)
-            if (kv.first < n_T_out) place(kv.first, kv.second.first, kv.second.second);
-    } else if (!T_list.empty()) {
-        std::vector<double> s, q;
-        get_flat_buffer(curr_idx, s, q);
-        place(curr_idx, s, q);
+    if (!streaming_) {
+        if (!T_list.empty()) {
+            std::vector<double> s, q;
+            get_flat_buffer(curr_idx, s, q);
+            place(curr_idx, s, q);
+        }
+        const std::vector<uint64_t> shape = ew == 512 ? std::vector<uint64_t>{nc, n_T_out, nk, 16, 16, 2}
+                                                      : std::vector<uint64_t>{nc, n_T_out, nk, 2};
+        f.dataset_f64(g + "/static_corr", shape, sum.data());
+        if (store_error_term_) f.dataset_f64(g + "/static_corr_2", shape, sq.data());
     }
-    const std::vector<uint64_t> shape = ew == 512 ? std::vector<uint64_t>{nc, n_T_out, nk, 16, 16, 2}
-                                                  : std::vector<uint64_t>{nc, n_T_out, nk, 2};
-    f.dataset_f64(g + "/static_corr", shape, sum.data());
-    if (store_error_term_) f.dataset_f64(g + "/static_corr_2", shape, sq.data());
     std::vector<double> sT;
     std::vector<uint64_t> sN;
     for (size_t i : ord) {

@@ -91,7 +91,10 @@ public:
     ssf_manager(CMC::Lattice& sc, const std::vector<std::string>& correlator_names,
                 size_t n_temperatures_reserve = 0, bool store_error_term = true);
     // Streaming (anneal.cpp): one slot per T_sample value, sorted ascending;
-    // flush() stores the current temperature into its slot.
+    // flush() writes the current temperature into its slot of static_corr
+    // (and static_corr_2) in `file`, reserved at the first flush in the
+    // layout of the first call (include/ssf_manager.hpp:375-465), and keeps
+    // no copy; write_group(file) then adds the remaining datasets.
     ssf_manager(CMC::Lattice& sc, const std::vector<std::string>& correlator_names, CMC::OutFile& file,
                 const char* group_name, const std::vector<double>& T_sample, bool store_error_term = true);
 
@@ -128,13 +131,18 @@ private:
     std::vector<ipos_t> sl_positions_;
     bool store_error_term_;
     bool streaming_ = false;
+    CMC::OutFile* file_ = nullptr;
+    bool reserved_ = false;
+    size_t h_sum_ = 0, h_sq_ = 0;
     std::string group_;
     std::vector<double> T_sorted_;
-    // flushed temperatures (streaming) : slot -> (sum, sq)
+    // slot size_t(-1): sums carried over by point_at for the current
+    // temperature
     std::map<size_t, std::pair<std::vector<double>, std::vector<double>>> flushed_;
     bool have_current_ = false;
     size_t ew_ = 2;  // doubles per (correlator, k): 2, or 16*16*2 resolved
 
     void configure(const std::vector<std::string>& names);
+    void reserve_streamed();
     void on_new_temp() override;
 };

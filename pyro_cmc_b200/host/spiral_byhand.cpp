@@ -16,6 +16,7 @@ using namespace CMC;
 
 int main(int argc, char* argv[]) {
     ArgParser prog("spiral_byhand");
+    prog.flag({"--npz"}, "Write the output as NumPy .npz archives instead of HDF5 (.h5)");
     prog.option({"--output_dir", "-o"}, "Path to output", "", true);
     prog.positional("L", "Linear dimension of cubic supercell");
     prog.positional("Q", "Spiral wavevector index (3 integers)", 3);
@@ -29,6 +30,7 @@ int main(int argc, char* argv[]) {
         std::exit(1);
     }
     try {
+        const std::string ext = prog.boolean("--npz") ? ".npz" : ".h5";
         const std::filesystem::path outdir(prog.str("--output_dir"));
         if (!std::filesystem::exists(outdir)) throw std::runtime_error("Cannot open outdir");
         const int L = int(prog.integer("L"));
@@ -60,14 +62,14 @@ int main(int argc, char* argv[]) {
         ssfm.sample();
         e_manager.sample(total_E);
         std::cout << "Total E = " << total_E << std::endl;
-        const auto file_path = outdir / (name.str() + ".out.npz");
+        const auto file_path = outdir / (name.str() + ".out" + ext);
         OutFile file(file_path.string());
         ssfm.write_group(file, "/ssf");
         e_manager.write_group(file, "/energy");
         write_geometry_group(file, lat);
         file.close();
         std::cout << "Saved to \n" << file_path << std::endl;
-        const auto f = outdir / (name.str() + ".spins.npz");
+        const auto f = outdir / (name.str() + ".spins" + ext);
         std::printf("Saving spin state to %s\n", f.string().c_str());
         save_spin_state(lat, f);
     } catch (const std::exception& e) {

@@ -12,7 +12,7 @@
 //    [n_corr, n_T, n_k, 2] that ssf_manager produces, or with --ssf_resolved
 //    the sublattice-resolved layout [n_corr, n_T, n_k, 16, 16, 2] that the
 //    reference's write_ssf_group (temper.cpp:121-159) is written for;
-//  * output is <name>.out.npz; --seed is the Philox key.
+//  * output is <name>.out.h5 (<name>.out.npz with --npz); --seed is the Philox key.
 #include <algorithm>
 #include <cstdio>
 #include <filesystem>
@@ -27,6 +27,7 @@ using namespace CMC;
 
 int main(int argc, char* argv[]) {
     ArgParser prog("temper");
+    prog.flag({"--npz"}, "Write the output as NumPy .npz archives instead of HDF5 (.h5)");
     prog.option({"--output_dir", "-o"}, "Path to output", "", true);
     prog.option({"--seed", "-s"}, "Seed of the RNG (Philox key)", "", true);
     prog.option({"--n_replicas"}, "Number of replicas (rungs), one per temperature", "", true);
@@ -49,6 +50,7 @@ int main(int argc, char* argv[]) {
         std::exit(1);
     }
     try {
+        const std::string ext = prog.boolean("--npz") ? ".npz" : ".h5";
         const std::filesystem::path outdir(prog.str("--output_dir"));
         if (!std::filesystem::exists(outdir)) throw std::runtime_error("output_dir does not exist");
         const uint64_t seed = uint64_t(prog.integer("--seed"));
@@ -122,7 +124,7 @@ int main(int argc, char* argv[]) {
             eE2.push_back(E2[size_t(k)]);
             en.push_back(ne[size_t(k)]);
         }
-        const auto file_path = outdir / (name.str() + ".out.npz");
+        const auto file_path = outdir / (name.str() + ".out" + ext);
         OutFile file(file_path.string());
         const uint64_t nR = uint64_t(R);
         file.dataset_f64("/energy/T_list", {nR}, eT.data());
@@ -177,7 +179,7 @@ int main(int argc, char* argv[]) {
             auto& spins = proto.get_objects<HeisenbergSpin>();
             for (size_t i = 0; i < spins.size(); ++i)
                 for (int a = 0; a < 3; ++a) spins[i].S[a] = S[3 * i + size_t(a)];
-            const auto f = outdir / (name.str() + ".spins.npz");
+            const auto f = outdir / (name.str() + ".spins" + ext);
             std::printf("[temper] Saving spin state of coldest replica (T=%.3e) to %s\n", T_grid.back(),
                         f.string().c_str());
             save_spin_state(proto, f);

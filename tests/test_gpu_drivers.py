@@ -35,7 +35,7 @@ def test_anneal_driver_output_and_determinism(tmp_path):
             "--correlators", "xx", "yy", "zz", "xy", "xz", "yz", "yx", "zx", "zy", "--save_state"]
     out = run("anneal", *args)
     assert "[anneal] Iter" in out and "Saved to" in out
-    path = only(tmp_path, ".out.npz")
+    path = only(tmp_path, ".out.h5")
     T_grid, S_idx = generate_T_profile(10.0, 0.5, [1.0, 0.5], 10)
     with File(path) as f:
         np.testing.assert_array_equal(f["/energy/T_list"], T_grid)
@@ -50,7 +50,7 @@ def test_anneal_driver_output_and_determinism(tmp_path):
         assert int(f["/ssf"].attrs["n_spins"]) == 128 and list(f["/ssf"].attrs["k_dims"]) == [2, 2, 2]
         assert (f["/geometry/index_cell"] == 16 * np.eye(3)).all()
         assert f["/ssf/sl_positions"].shape == (16, 3)
-    with File(only(tmp_path, ".spins.npz")) as f:
+    with File(only(tmp_path, ".spins.h5")) as f:
         assert f["/spin_orientation"].shape == (128, 3) and f["/spin_pos"].dtype == np.int32
         assert np.allclose(np.linalg.norm(f["/spin_orientation"], axis=1), 1.0, atol=1e-5)
     # the same run through the Python protocol: identical calls, identical chain
@@ -63,10 +63,10 @@ def test_spiral_byhand_driver(tmp_path):
     out = run("spiral_byhand", "-o", tmp_path, 4, 1, 2, 0)
     E = float(out.split("Total E = ")[1].split()[0])
     o = oracle.System(4, J1=-1.0, j1_mode=1)
-    with File(only(tmp_path, ".spins.npz")) as f:
+    with File(only(tmp_path, ".spins.h5")) as f:
         o.set_spins(f["/spin_orientation"][:].astype(np.float32).astype(np.float64))
     assert E == pytest.approx(o.energy(), abs=1e-4)
-    with File(only(tmp_path, ".out.npz")) as f:
+    with File(only(tmp_path, ".out.h5")) as f:
         sc = f["/ssf/static_corr"][:]
         tot = sc[1, 0, :, 0] + sc[2, 0, :, 0]
         N = 16 * 64
@@ -78,7 +78,7 @@ def test_temper_driver(tmp_path):
               "--T_hot", 2.0, "--T_sample", 0.5, "--n_sweep", 4, "--n_burn_in", 8, "--n_sample", 20, "--init_uniform",
               "--save_state")
     assert "per-pair swap acceptance" in out
-    with File(only(tmp_path, ".out.npz")) as f:
+    with File(only(tmp_path, ".out.h5")) as f:
         T = f["/energy/T_list"][:]
         assert len(T) == 6 and (np.diff(T) > 0).all()
         assert (f["/energy/n_samples"][:] == 20).all()
@@ -92,7 +92,7 @@ def test_fieldcool_driver(tmp_path):
     out = run("fieldcool", "-o", tmp_path, "-s", 3, 2, "--J1", 1, "-B", 0, 0, 0.5, "--T_cold", 0.2, "--n_steps", 8,
               "--n_sweep", 4, "--n_burn_in", 4, "--n_sample", 3, "--init_uniform")
     assert "Releasing field" in out
-    with File(only(tmp_path, ".out.npz")) as f:
+    with File(only(tmp_path, ".out.h5")) as f:
         assert len(f["/energy/T_list"]) == 8
         assert list(f["/ssf/n_samples"]) == [3]
         assert f["/ssf/static_corr"].shape == (3, 1, 8, 2)
@@ -110,7 +110,7 @@ def test_resolved_ssf_from_the_drivers(tmp_path):
         d = tmp_path / tag
         d.mkdir()
         run("anneal", "-o", d, *base, *extra)
-        with File(only(d, ".out.npz")) as f:
+        with File(only(d, ".out.h5")) as f:
             outs[tag] = f["/ssf/static_corr"][:]
     c, r = outs["c"], outs["r"]
     assert c.shape == (2, 1, 8, 2) and r.shape == (2, 1, 8, 16, 16, 2)
@@ -125,7 +125,7 @@ def test_resolved_ssf_from_the_drivers(tmp_path):
     d.mkdir()
     run("temper", "-o", d, "-s", 3, "--n_replicas", 4, 2, "--J1", 1, "--T_sample", 0.3, "--n_sweep", 2,
         "--n_burn_in", 2, "--n_sample", 3, "--init_uniform", "--ssf_resolved")
-    with File(only(d, ".out.npz")) as f:
+    with File(only(d, ".out.h5")) as f:
         assert f["/ssf/static_corr"].shape == (3, 1, 8, 16, 16, 2)
         assert (f["/ssf/static_corr_2"][..., 0] >= 0).all()
 
@@ -137,7 +137,7 @@ def test_ltgs_driver(tmp_path):
     out = run("ltgs", "-o", tmp_path, 3, "--J1", 1, "--J2", 0.1, "--J3", -0.05, "--Delta", 0.5)
     assert "LT minimum:" in out and "k*  idx" in out and "Saved to" in out
     e_ref, k_ref = olt.lt_minimum(3, 1.0, 0.1, -0.05, 0.5)
-    with File(only(tmp_path, "ltgs.out.npz")) as f:
+    with File(only(tmp_path, "ltgs.out.h5")) as f:
         assert abs(float(f["/E_min"]) - e_ref) <= 1e-9
         lam = f["/eigenvalue_map"][:]
         assert lam.shape == (27,) and abs(lam.min() - 2 * e_ref) <= 1e-9
@@ -204,10 +204,35 @@ def test_anneal_save_state_ft(tmp_path):
     out = run("anneal", *args)
     assert "Saving spin state FT" in out
     from oracle import ssf_fft
-    with File(only(tmp_path, ".spins.npz")) as f:
+    with File(only(tmp_path, ".spins.h5")) as f:
         S = f["/spin_orientation"][:]
-    with File(only(tmp_path, ".spins_ft.npz")) as f:
+    with File(only(tmp_path, ".spindft.h5")) as f:
         ft = f["/spin_ft"][:]
     assert ft.shape == (3, 16, 64, 2)
     ref = ssf_fft.sublattice_ft(S, 4)
     assert np.abs(ft[..., 0] + 1j * ft[..., 1] - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_anneal_npz_container_holds_the_same_tree(tmp_path):
+    """--npz writes the tree of the HDF5 output as an .npz archive: same
+    datasets, shapes, values and attributes for the same seed."""
+    args = ["-s", 11, 2, "--J1", 1, "--J2", 0.05, "--T_sample", 1.0, 0.5, "--n_steps", 6, "--n_sweep", 2,
+            "--n_burn_in", 2, "--n_sample", 2, "--init_uniform", "--save_state"]
+    (tmp_path / "h").mkdir()
+    (tmp_path / "z").mkdir()
+    run("anneal", "-o", tmp_path / "h", *args)
+    run("anneal", "-o", tmp_path / "z", *args, "--npz")
+    with File(only(tmp_path / "h", ".out.h5")) as a, File(only(tmp_path / "z", ".out.npz")) as b:
+        for g in ("energy", "ssf", "geometry"):
+            assert set(a[g].keys()) == set(b[g].keys()), g
+            for k in a[g].keys():
+                x, y = a[g + "/" + k][:], b[g + "/" + k][:]
+                if x.dtype == object:
+                    assert [s.decode() for s in x] == [s.decode() for s in y]
+                else:
+                    assert x.dtype == y.dtype and x.shape == y.shape, (g, k)
+                    np.testing.assert_array_equal(x, y)
+        for k in ("n_spins", "k_dims"):
+            np.testing.assert_array_equal(a["ssf"].attrs[k], b["ssf"].attrs[k])
+    with File(only(tmp_path / "h", ".spins.h5")) as a, File(only(tmp_path / "z", ".spins.npz")) as b:
+        np.testing.assert_array_equal(a["/spin_orientation"][:], b["/spin_orientation"][:])

@@ -88,7 +88,7 @@ def test_anneal_driver_lifted_matches_python_protocol(tmp_path):
     r = subprocess.run([os.path.join(build.BIN, "anneal"), *map(str, args)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr + r.stdout
     assert "(lifted Metropolis)" in r.stdout
-    files = [f for f in os.listdir(tmp_path) if f.endswith(".out.npz")]
+    files = [f for f in os.listdir(tmp_path) if f.endswith(".out.h5")]
     from pyro_cmc_b200.h5compat import File
     with File(os.path.join(tmp_path, files[0])) as f:
         E = f["/energy/E"][:]
