@@ -552,6 +552,18 @@ def run_extras(pc, torch, np):
     n_tot = sum(16 * L ** 3 for L in Ls)
     batched = n_tot * rounds * 10 / (ms * 1e-3)
     att, acc = b.pt_exchange_stats()
+    # the same rounds in one persistent cooperative launch per stretch of
+    # sweeps between S(q) samples (pc_set_pt_persistent)
+    b.set_pt_persistent(True)
+    b.pt_run(2, 10, 16)
+    torch.cuda.synchronize()
+    l0 = b.launch_count()
+    e0.record(stream)
+    b.pt_run(rounds, 10, 16)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_p = e0.elapsed_time(e1)
+    launches_p = b.launch_count() - l0
     del b
     # plain single small replica (L=8), the comparison point for batching
     p1 = pc.pyrochlore_system(8, J1=1.0, J2=0.0, J3=0.02, B=(0, 0, 0.1), seed=9, schedule=WL["schedule"])
@@ -569,6 +581,8 @@ def run_extras(pc, torch, np):
                       "config": "parallel tempering, 128 replicas (L 8/12/16/24 x 32 T geometric in [0.02, 2]), "
                                 "J=(1,0,0.02), B=(0,0,0.1), exchange every 10 sweeps, S(q) xx/yy/zz every 16 sweeps",
                       "ms_per_10_sweeps": ms / rounds, "tile": list(btile), "exchange_accept": float(acc.sum()) / max(1.0, float(att.sum())),
+                      "persistent": {"value": n_tot * rounds * 10 / (ms_p * 1e-3), "ms_per_10_sweeps": ms_p / rounds,
+                                     "kernel_launches_per_round": launches_p / rounds},
                       "plain_single_L8": plain_small, "batched_over_plain_L8": batched / plain_small}
     # plain single replica of the L=16 anneal: one sampling step = 16 sweeps +
     # one S(q) sample of the anneal's six correlators

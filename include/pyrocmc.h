@@ -259,6 +259,19 @@ int pc_pt_configure(pc_system* sys, const double* T);
  * rounds, (1,2),.. on odd, src/temper.cpp:437-473). The schedule is captured
  * as a CUDA graph and replayed. */
 int pc_pt_run(pc_system* sys, int n_rounds, int n_sweep, int ssf_every);
+/* Tempering rounds in one persistent cooperative launch (off by default): with
+ * 1, pc_pt_run runs all its rounds -- every colour pass of every replica, the
+ * energies and the exchanges -- in one kernel launch with grid barriers
+ * between the phases (with S(q) samples: one launch per stretch of sweeps
+ * between samples). Same site updates, draws and exchange rule as the
+ * per-pass graph: the same chain, up to the rounding of the energy sums (one
+ * thread per site here, one per cubic cell there), which the exchange
+ * decisions see. PC_ERR_UNSUPPORTED for systems it does not cover
+ * (non-pyrochlore couplings, lifted moves, reflection overrelaxation, the
+ * staged row tiles, block sizes outside 32..256). No counterpart in the
+ * reference (an execution strategy of src/temper.cpp:418-474). */
+int pc_set_pt_persistent(pc_system* sys, int on);
+int pc_get_pt_persistent(pc_system* sys, int* on);
 /* Zeroes the energy accumulators and exchange statistics (after burn-in);
  * the replica-to-slot assignment and the spins are kept. */
 int pc_pt_reset_stats(pc_system* sys);
@@ -372,11 +385,14 @@ int pc_lt_minimum(int L, double J1, double J2, double J3, double Delta, double* 
                   int64_t* k_star, double* eigvec);
 /* Bound of the first wait of the staged colour pass (load variant 3) on its
  * bulk copies, in polls of a hardware-timed try_wait (default and maximum
- * 2^22; < 0 restores the default). For tests of the timeout path: with 0
- * every staged pass gives up at once, sets the device error flag, waits for
- * its copies at the full bound (none is left in flight), skips its updates,
- * and the call returns PC_ERR_TIMEOUT; the system stays usable. No
- * counterpart in the reference (it has no device waits). */
+ * 2^22; < 0 restores the default), and of every grid-barrier wait of the
+ * persistent tempering kernel, in polls of ~64 ns (default and maximum 2^24).
+ * For tests of the timeout paths: with 0 every staged pass gives up at once,
+ * sets the device error flag, waits for its copies at the full bound (none is
+ * left in flight), skips its updates, and the call returns PC_ERR_TIMEOUT; a
+ * persistent tempering launch gives up at its first barrier and every block
+ * leaves (the round is left unfinished), PC_ERR_TIMEOUT. The system stays
+ * usable. No counterpart in the reference (it has no device waits). */
 int pc_set_wait_limit(pc_system* sys, int polls);
 /* Enables per-kernel CUDA-event timing (off by default). */
 int pc_set_kernel_timing(pc_system* sys, int on);

@@ -97,6 +97,8 @@ _SIGNATURES = {
     "pc_set_launch_overlap": (_I, [_P, _I]),
     "pc_set_cluster_sweeps": (_I, [_P, _I]),
     "pc_get_cluster_sweeps": (_I, [_P, _IP]),
+    "pc_set_pt_persistent": (_I, [_P, _I]),
+    "pc_get_pt_persistent": (_I, [_P, _IP]),
 }
 
 

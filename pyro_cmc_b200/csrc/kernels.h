@@ -29,6 +29,10 @@ enum PassMode {
 // j I with j != 0 (kVarIso), or when that holds for every group but the J2
 // group, whose matrix is 0 everywhere (kVarIsoNoJ2: J2 = 0).
 constexpr int kVarIso = 5, kVarIsoNoJ2 = 6;
+// Or'ed into a load variant (0, kVarIso, kVarIsoNoJ2): spins, own spin and
+// temperature are read with L2-coherent loads, for a kernel that writes them
+// in an earlier phase of the same launch (the persistent tempering kernel).
+constexpr int kVarCoherent = 0x100;
 struct PassArgs {
     float4* spins;
     const ReplicaDev* reps;
@@ -243,6 +247,40 @@ struct PtArgs {
     int n_slots;
 };
 void launch_pt_exchange(const PtArgs& a, cudaStream_t st);
+
+// Tempering rounds of a batch of replicas in one persistent cooperative launch
+// (pt_persistent.cu): per round, n_sweep sweeps (every colour pass of every
+// replica; a grid barrier between passes), then, with `exchange`, the energy
+// of every replica, its per-replica sum and the exchange round, each phase
+// behind a grid barrier. The barrier's waits are bounded: when one runs out
+// the kernel sets *err = kErrGridBarrier and every block leaves.
+constexpr int kErrGridBarrier = 2;
+struct PersistArgs {
+    PassArgs pass;  // pass arguments (tiles, n_tiles, sweep_offset, or_pass unused)
+    const Tile* colour_tiles[16];
+    int n_colour_tiles[16];
+    int n_colours;
+    int fused;  // 1: one fused Metropolis + rotation pass per colour; 0: Metropolis passes, then rotation passes
+    int n_rounds, n_sweep;
+    int exchange;       // 1: energy + exchange after each round's sweeps
+    uint64_t* sweep;    // device sweep counter: read at entry, advanced by n_rounds * n_sweep at exit
+    // energy (one thread per site, bonds to higher sublattices, each bond once)
+    const Tile* e_tiles;
+    const int32_t* e_order;
+    int n_e_tiles;
+    double* partial;  // [n_e_tiles][4]
+    const int32_t* tile_begin;
+    const int32_t* tile_end;
+    double* e;    // per replica energy per cell
+    double* mag;  // per replica sum of S
+    int R;
+    PtArgs pt;
+    unsigned int* bar;  // [2]: arrivals, generation (zero before the first launch)
+    int max_polls;      // bound of each barrier wait (polls of ~64 ns)
+};
+// Blocks that fit on the device at once for this block size (0: unsupported).
+int pt_persistent_capacity(int iso, int fused, int threads);
+int launch_pt_persistent(const PersistArgs& a, int iso, int grid, int threads, cudaStream_t st);
 
 // Seed merge of S(q) accumulators and spiral-plane invariants (merge.cu).
 struct MergeArgs {

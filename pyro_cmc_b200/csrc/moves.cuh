@@ -318,28 +318,31 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
 //   kVarIso, kVarIsoNoJ2: VAR 0 for systems whose group matrices are all j I
 //          (or all but a zero J2 group), chosen by the host in place of VAR 0:
 //          the same bits, fewer instructions, no per-group branches.
-template <int SL, int VAR>
+template <int SL, int VAR_>
 __device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const PassArgs& a, const ReplicaDev& rep,
                                              const Coords& c, float4 (&v)[kStructNb], int phase) {
+    constexpr int VAR = VAR_ & ~kVarCoherent;
+    constexpr bool NC = (VAR_ & kVarCoherent) == 0;
+    static_assert(NC || VAR == 0 || VAR == kVarIso || VAR == kVarIsoNoJ2, "coherent loads: variants 0 and iso");
     constexpr int kJ3 = grp_begin(SL, 4);
     float3 h = make_float3(0.f, 0.f, 0.f);
     if constexpr (VAR == 0) {
         if (phase == 1) {
-            add_group<SL, 0>(h, S, rep.Nc, c, a.mats);
-            add_group<SL, 1>(h, S, rep.Nc, c, a.mats);
-            add_group<SL, 2>(h, S, rep.Nc, c, a.mats);
-            add_group<SL, 3>(h, S, rep.Nc, c, a.mats);
-            add_group<SL, 4>(h, S, rep.Nc, c, a.mats);
-            add_group<SL, 5>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 0, NC>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 1, NC>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 2, NC>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 3, NC>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 4, NC>(h, S, rep.Nc, c, a.mats);
+            add_group<SL, 5, NC>(h, S, rep.Nc, c, a.mats);
         }
     } else if constexpr (VAR == kVarIso || VAR == kVarIsoNoJ2) {
         if (phase == 1) {
-            add_group_iso<SL, 0>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 1>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 2>(h, S, rep.Nc, c, a.mats);
-            if constexpr (VAR == kVarIso) add_group_iso<SL, 3>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 4>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 5>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 0, NC>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 1, NC>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 2, NC>(h, S, rep.Nc, c, a.mats);
+            if constexpr (VAR == kVarIso) add_group_iso<SL, 3, NC>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 4, NC>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 5, NC>(h, S, rep.Nc, c, a.mats);
         }
     } else if constexpr (VAR == 1) {
         if (phase == 0)
@@ -365,14 +368,15 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
     float4 v[kStructNb];
     site_field<SL, VAR>(S, a, rep, c, v, 0);  // issue loads (VAR 1, 2)
     const size_t i = size_t(SL) * rep.Nc + cell;
-    const float4 s0 = S[i];
+    constexpr bool kCoherent = (VAR & kVarCoherent) != 0;
+    const float4 s0 = kCoherent ? __ldcg(S + i) : S[i];
     constexpr bool kMet = MODE == kMetropolis || MODE == kFusedRotate || MODE == kFusedReflect;
     constexpr bool kRot = MODE == kOverrelaxRotate || MODE == kFusedRotate;
     // draws first: they do not depend on the local field, so they overlap the loads
     uint4 w = make_uint4(0, 0, 0, 0);
     float sigma = 0.f, invT = 0.f;
     if (kMet) {
-        const double T = a.T_rep[r];
+        const double T = kCoherent ? __ldcg(a.T_rep + r) : a.T_rep[r];
         sigma = sqrtf(float(T) * a.inv_T_ref);
         invT = float(1.0 / T);
         w = site_draw_rk(a.rkeys, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));

@@ -36,19 +36,33 @@ __device__ __forceinline__ int pick(const int (&v)[3]) {
         return v[1];
 }
 
-template <int SL, int E>
+// NC: the spins are read-only for the whole kernel (a colour pass reads other
+// sublattices than it writes), so loads may use the non-coherent read-only
+// path (__ldg). A kernel that also writes the spins it gathers in a later
+// phase (the persistent tempering kernel: colour passes separated by grid
+// barriers) loads with NC = false: L2-coherent loads (__ldcg) that never hit
+// a stale L1 line.
+template <bool NC>
+__device__ __forceinline__ float4 load_spin(const float4* p) {
+    if constexpr (NC)
+        return __ldg(p);
+    else
+        return __ldcg(p);
+}
+
+template <int SL, int E, bool NC = true>
 __device__ __forceinline__ float4 load_nb(const float4* __restrict__ S, int Nc, const Coords& c) {
     constexpr int s2 = nb_sl(SL, E), dx = nb_dx(SL, E), dy = nb_dy(SL, E), dz = nb_dz(SL, E);
     const uint32_t off = uint32_t(s2) * (uint32_t(Nc) << 4) + uint32_t(pick<dx>(c.x)) + uint32_t(pick<dy>(c.y)) +
                          uint32_t(pick<dz>(c.z));
-    return __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(S) + off));
+    return load_spin<NC>(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(S) + off));
 }
 
-template <int SL, int G, int... K>
+template <int SL, int G, bool NC, int... K>
 __device__ __forceinline__ float3 group_sum(const float4* __restrict__ S, int Nc, const Coords& c,
                                             std::integer_sequence<int, K...>) {
     constexpr int B = grp_begin(SL, G);
-    const float4 v[sizeof...(K)] = {load_nb<SL, B + K>(S, Nc, c)...};
+    const float4 v[sizeof...(K)] = {load_nb<SL, B + K, NC>(S, Nc, c)...};
     float3 t = make_float3(0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < int(sizeof...(K)); ++k) {
@@ -59,11 +73,11 @@ __device__ __forceinline__ float3 group_sum(const float4* __restrict__ S, int Nc
     return t;
 }
 
-template <int SL, int G>
+template <int SL, int G, bool NC = true>
 __device__ __forceinline__ void add_group(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                           const PyroMats& mats) {
     if (mats.active[SL] & (1u << G)) {
-        const float3 t = group_sum<SL, G>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
+        const float3 t = group_sum<SL, G, NC>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
         const float* J = mats.M[SL][G];
         h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
         h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
@@ -77,10 +91,10 @@ __device__ __forceinline__ void add_group(float3& h, const float4* __restrict__ 
 // no test of the group's activity. add_group gives the same bits on such a
 // matrix: its two zero terms add exact zeros to the rounded j t, and the sum
 // is added to h unfused, as here.
-template <int SL, int G>
+template <int SL, int G, bool NC = true>
 __device__ __forceinline__ void add_group_iso(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                               const PyroMats& mats) {
-    const float3 t = group_sum<SL, G>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
+    const float3 t = group_sum<SL, G, NC>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
     const float j = mats.M[SL][G][0];
     h.x = __fadd_rn(h.x, __fmul_rn(j, t.x));
     h.y = __fadd_rn(h.y, __fmul_rn(j, t.y));
@@ -152,10 +166,10 @@ __device__ __forceinline__ void field_groups(float3& h, const float4 (&v)[kStruc
 // neighbours on higher sublattices, h+_i = sum_G M_G sum_{e in G, s2 > SL} S_e.
 // Since the matrix seen from the other end is the transpose, the energy
 // 0.5 sum_i S_i.h_i equals sum_i S_i.h+_i: half the neighbour loads.
-template <int SL, int E>
+template <int SL, int E, bool NC = true>
 __device__ __forceinline__ void add_upper(float3& t, const float4* __restrict__ S, int Nc, const Coords& c) {
     if constexpr (nb_sl(SL, E) > SL) {
-        const float4 v = load_nb<SL, E>(S, Nc, c);
+        const float4 v = load_nb<SL, E, NC>(S, Nc, c);
         t.x += v.x;
         t.y += v.y;
         t.z += v.z;
@@ -169,14 +183,14 @@ __host__ __device__ constexpr bool group_has_upper(int sl, int g) {
 // ISO 1: every group matrix is j I with j != 0; ISO 2: so but the J2 group
 // (group 3), which is 0 and skipped (as add_group_iso: no activity test,
 // three multiplies and three unfused adds per group, the same bits).
-template <int SL, int G, int ISO, int... K>
+template <int SL, int G, int ISO, bool NC, int... K>
 __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                                 const PyroMats& mats, std::integer_sequence<int, K...>) {
     if constexpr (group_has_upper(SL, G) && !(ISO == 2 && G == 3)) {
         if (ISO || (mats.active[SL] & (1u << G))) {
             constexpr int B = grp_begin(SL, G);
             float3 t = make_float3(0.f, 0.f, 0.f);
-            (add_upper<SL, B + K>(t, S, Nc, c), ...);
+            (add_upper<SL, B + K, NC>(t, S, Nc, c), ...);
             const float* J = mats.M[SL][G];
             if constexpr (ISO) {
                 h.x = __fadd_rn(h.x, __fmul_rn(J[0], t.x));
@@ -190,22 +204,22 @@ __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restr
         }
     }
 }
-template <int SL, int G, int ISO>
+template <int SL, int G, int ISO, bool NC>
 __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                                 const PyroMats& mats) {
-    add_group_upper<SL, G, ISO>(h, S, Nc, c, mats, std::make_integer_sequence<int, grp_size(SL, G)>{});
+    add_group_upper<SL, G, ISO, NC>(h, S, Nc, c, mats, std::make_integer_sequence<int, grp_size(SL, G)>{});
 }
-template <int SL, int ISO = 0>
+template <int SL, int ISO = 0, bool NC = true>
 __device__ __forceinline__ float3 struct_field_upper(const float4* __restrict__ S, const PyroMats& mats, int cell,
                                                      int L, int Nc, uint64_t divL) {
     const Coords c = cell_coords(cell, L, divL);
     float3 h = make_float3(0.f, 0.f, 0.f);
-    add_group_upper<SL, 0, ISO>(h, S, Nc, c, mats);
-    add_group_upper<SL, 1, ISO>(h, S, Nc, c, mats);
-    add_group_upper<SL, 2, ISO>(h, S, Nc, c, mats);
-    add_group_upper<SL, 3, ISO>(h, S, Nc, c, mats);
-    add_group_upper<SL, 4, ISO>(h, S, Nc, c, mats);
-    add_group_upper<SL, 5, ISO>(h, S, Nc, c, mats);
+    add_group_upper<SL, 0, ISO, NC>(h, S, Nc, c, mats);
+    add_group_upper<SL, 1, ISO, NC>(h, S, Nc, c, mats);
+    add_group_upper<SL, 2, ISO, NC>(h, S, Nc, c, mats);
+    add_group_upper<SL, 3, ISO, NC>(h, S, Nc, c, mats);
+    add_group_upper<SL, 4, ISO, NC>(h, S, Nc, c, mats);
+    add_group_upper<SL, 5, ISO, NC>(h, S, Nc, c, mats);
     return h;
 }
 

@@ -119,6 +119,11 @@ namespace pc {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace pc
 
+// Bound of each grid-barrier wait of the persistent tempering kernel, in
+// polls of ~64 ns (about a second; a colour pass of the largest batches takes
+// well under a millisecond).
+constexpr int kBarrierMaxPolls = 1 << 24;
+
 struct pc_system {
     int device = 0;
     int sms = 148;
@@ -229,6 +234,11 @@ struct pc_system {
     DevBuf<uint64_t> d_round;
     std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> pt_graphs;  // (n_sweep, phase)
     uint64_t pt_sweeps_done = 0;
+    // rounds in one persistent cooperative launch (pt_persistent.cu)
+    bool pt_persistent = false;
+    DevBuf<unsigned int> d_bar;                 // grid barrier: arrivals, generation
+    std::map<std::array<int, 3>, int> persist_cap;  // (iso, fused, threads) -> resident blocks
+    int barrier_polls = kBarrierMaxPolls;       // bound of each grid-barrier wait (pc_set_wait_limit)
 
     // pinned host staging for the small per-call transfers (upstream scalars,
     // energies, gradient sums, the device error flag): one synchronisation per
@@ -298,6 +308,7 @@ struct pc_system {
             g.d_amp.release();
         }
         d_slot_of_rep.release();
+        d_bar.release();
         d_ladder_begin.release();
         d_rep_of_slot.release();
         d_pt_slot_of_rep.release();
@@ -1376,6 +1387,9 @@ int pc_set_sweep_counter(pc_system* sys, int replica, uint64_t sweep) {
 int device_error_flag(pc_system* s, int flag) {
     if (!flag) return PC_OK;
     PC_CK(cudaMemsetAsync(s->d_err.p, 0, sizeof(int), s->stream));
+    if (flag == pc::kErrGridBarrier)
+        return fail(PC_ERR_TIMEOUT, "the persistent tempering kernel stopped waiting at a grid barrier (bounded wait "
+                                    "ran out); the round was left unfinished");
     return fail(PC_ERR_TIMEOUT, "a colour pass stopped waiting for its staged neighbour rows (bounded wait ran out); "
                                 "the updates of that pass were skipped");
 }
@@ -1881,6 +1895,27 @@ int pc_pt_configure(pc_system* sys, const double* T) {
 }
 
 namespace {
+pc::PtArgs pt_args(pc_system* s) {
+    pc::PtArgs a;
+    a.n_ladders = s->n_ladders;
+    a.ladder_begin = s->d_ladder_begin.p;
+    a.T_slot = s->d_T_slot.p;
+    a.rep_of_slot = s->d_rep_of_slot.p;
+    a.slot_of_rep = s->d_pt_slot_of_rep.p;
+    a.T_rep = s->d_T.p;
+    a.e_rep = s->d_e.p;
+    a.reps = s->d_reps.p;
+    a.E_sum = s->d_E_sum.p;
+    a.E2_sum = s->d_E2_sum.p;
+    a.n_e = s->d_n_e.p;
+    a.attempts = s->d_att.p;
+    a.accepts = s->d_accn.p;
+    a.round = s->d_round.p;
+    a.seed = s->seed;
+    a.n_slots = int(s->T_slot.size());
+    return a;
+}
+
 int enqueue_pt_round(pc_system* s, int n_sweep, int ssf_every, uint64_t sweep_phase) {
     for (int i = 0; i < n_sweep; ++i) {
         int rc = enqueue_sweep(s, uint64_t(i), 1, false);
@@ -1899,27 +1934,109 @@ int enqueue_pt_round(pc_system* s, int n_sweep, int ssf_every, uint64_t sweep_ph
     s->launches++;
     int rc = enqueue_energy(s);
     if (rc) return rc;
-    pc::PtArgs a;
-    a.n_ladders = s->n_ladders;
-    a.ladder_begin = s->d_ladder_begin.p;
-    a.T_slot = s->d_T_slot.p;
-    a.rep_of_slot = s->d_rep_of_slot.p;
-    a.slot_of_rep = s->d_pt_slot_of_rep.p;
-    a.T_rep = s->d_T.p;
-    a.e_rep = s->d_e.p;
-    a.reps = s->d_reps.p;
-    a.E_sum = s->d_E_sum.p;
-    a.E2_sum = s->d_E2_sum.p;
-    a.n_e = s->d_n_e.p;
-    a.attempts = s->d_att.p;
-    a.accepts = s->d_accn.p;
-    a.round = s->d_round.p;
-    a.seed = s->seed;
-    a.n_slots = int(s->T_slot.size());
-    pc::launch_pt_exchange(a, s->stream);
+    pc::launch_pt_exchange(pt_args(s), s->stream);
     PC_LAUNCH_CK();
     s->launches++;
     return PC_OK;
+}
+
+// Why the rounds of this system cannot run in the persistent kernel (nullptr:
+// they can): it covers the structured couplings with standard Metropolis
+// moves, rotation overrelaxation, the fused or reference-order schedule and
+// the per-site neighbour loads (not the staged rows).
+const char* pt_persistent_unsupported(pc_system* s) {
+    if (!s->structured) return "the persistent tempering kernel needs the pyrochlore couplings";
+    if (s->update != 0) return "the persistent tempering kernel runs standard Metropolis moves";
+    if (s->or_mode != 0) return "the persistent tempering kernel runs rotation overrelaxation";
+    if (s->schedule > 1) return "the persistent tempering kernel runs the fused or reference-order schedule";
+    if (use_staged(s)) return "the persistent tempering kernel does not run the staged row tiles";
+    if (s->threads < 32 || s->threads > 256 || s->threads % 32) return "the persistent tempering kernel needs 32..256 threads";
+    return nullptr;
+}
+
+// One persistent launch: n_rounds rounds of n_sweep sweeps, each followed by
+// the energies and the exchange when `exchange`.
+int launch_persistent(pc_system* s, int n_rounds, int n_sweep, int exchange) {
+    const int fused = s->schedule == 1 ? 1 : 0;
+    const std::array<int, 3> key = {s->iso_kind, fused, s->threads};
+    auto it = s->persist_cap.find(key);
+    if (it == s->persist_cap.end())
+        it = s->persist_cap.emplace(key, pc::pt_persistent_capacity(s->iso_kind, fused, s->threads)).first;
+    if (it->second <= 0) return fail(PC_ERR_UNSUPPORTED, "no cooperative launch of the persistent kernel fits");
+    int most = s->R;
+    for (int c = 0; c < s->n_colours; ++c) most = std::max(most, s->n_colour_tiles[size_t(c)]);
+    const int grid = std::max(1, std::min(it->second, most));
+    pc::PersistArgs p;
+    std::memset(&p, 0, sizeof(p));
+    p.pass = pass_args(s, 0, 0, 0);
+    for (int c = 0; c < s->n_colours; ++c) {
+        p.colour_tiles[c] = s->d_colour_tiles[size_t(c)].p;
+        p.n_colour_tiles[c] = s->n_colour_tiles[size_t(c)];
+    }
+    p.n_colours = s->n_colours;
+    p.fused = fused;
+    p.n_rounds = n_rounds;
+    p.n_sweep = n_sweep;
+    p.exchange = exchange;
+    p.sweep = s->d_sweep.p;
+    p.e_tiles = s->d_all_tiles.p;
+    p.e_order = s->d_all_order.p;
+    p.n_e_tiles = s->n_all_tiles;
+    p.partial = s->d_partial.p;
+    p.tile_begin = s->d_tile_begin.p;
+    p.tile_end = s->d_tile_end.p;
+    p.e = s->d_e.p;
+    p.mag = s->d_mag.p;
+    p.R = s->R;
+    p.pt = pt_args(s);
+    p.bar = s->d_bar.p;
+    p.max_polls = s->barrier_polls;
+    PC_CK(cudaMemsetAsync(s->d_bar.p, 0, 2 * sizeof(unsigned int), s->stream));
+    const int e = pc::launch_pt_persistent(p, s->iso_kind, grid, s->threads, s->stream);
+    if (e != 0) return fail(PC_ERR_CUDA, std::string("persistent launch: ") + cudaGetErrorString(cudaError_t(e)));
+    s->launches++;
+    return PC_OK;
+}
+
+// pc_pt_run on the persistent kernel. Without S(q) samples, all rounds are one
+// launch. With samples, a round is split at the sweeps after which S(q) is
+// sampled (the S(q) kernels run between the launches), and its energies and
+// exchange come last, after a sample that follows the round's last sweep, as
+// in the per-pass schedule.
+int run_pt_persistent(pc_system* s, int n_rounds, int n_sweep, int ssf_every) {
+    if (!s->d_bar.p) PC_CK(s->d_bar.alloc(2));
+    PC_CK(cudaMemsetAsync(s->d_err.p, 0, sizeof(int), s->stream));
+    if (ssf_every <= 0) {
+        int rc = n_rounds > 0 ? launch_persistent(s, n_rounds, n_sweep, 1) : PC_OK;
+        if (rc) return rc;
+        s->pt_sweeps_done += uint64_t(n_rounds) * uint64_t(n_sweep);
+        s->host_sweep += uint64_t(n_rounds) * uint64_t(n_sweep);
+        return device_error(s);
+    }
+    for (int round = 0; round < n_rounds; ++round) {
+        const uint64_t phase = s->pt_sweeps_done % uint64_t(ssf_every);
+        int start = 0;
+        for (int i = 0; i < n_sweep; ++i) {
+            if ((phase + uint64_t(i) + 1) % uint64_t(ssf_every) != 0) continue;
+            const bool last = i + 1 == n_sweep;
+            int rc = launch_persistent(s, 1, i + 1 - start, 0);
+            if (rc) return rc;
+            pc::SsfOut o = ssf_out_base(s);
+            o.acc_sum = s->d_ssf_sum.p;
+            o.acc_sq = s->d_ssf_sq.p;
+            o.slot_of_rep = s->d_pt_slot_of_rep.p;
+            rc = enqueue_ssf(s, o, false);
+            if (rc) return rc;
+            for (auto& n : s->ssf_n) n++;
+            start = i + 1;
+            if (last) break;
+        }
+        int rc = launch_persistent(s, 1, n_sweep - start, 1);
+        if (rc) return rc;
+        s->pt_sweeps_done += uint64_t(n_sweep);
+        s->host_sweep += uint64_t(n_sweep);
+    }
+    return device_error(s);
 }
 }  // namespace
 
@@ -1939,6 +2056,10 @@ int pc_pt_run(pc_system* sys, int n_rounds, int n_sweep, int ssf_every) {
         }
     }
     PC_CK(cudaMemsetAsync(sys->d_acc.p, 0, sizeof(unsigned long long) * size_t(sys->R), sys->stream));
+    if (sys->pt_persistent) {
+        if (const char* why = pt_persistent_unsupported(sys)) return fail(PC_ERR_UNSUPPORTED, why);
+        return run_pt_persistent(sys, n_rounds, n_sweep, ssf_every);
+    }
     const uint64_t period = ssf_every > 0 ? uint64_t(ssf_every) : 1;
     for (int round = 0; round < n_rounds; ++round) {
         const uint64_t phase = sys->pt_sweeps_done % period;
@@ -2357,7 +2478,28 @@ int pc_set_wait_limit(pc_system* sys, int polls) {
     int rc = check_sys(sys, false);
     if (rc) return rc;
     sys->wait_polls = polls < 0 ? pc::kStagedMaxPolls : std::min(polls, pc::kStagedMaxPolls);
+    sys->barrier_polls = polls < 0 ? kBarrierMaxPolls : std::min(polls, kBarrierMaxPolls);
     sys->drop_graphs();  // captured passes carry the old bound
+    return PC_OK;
+}
+
+int pc_set_pt_persistent(pc_system* sys, int on) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (on) {
+        rc = check_sys(sys);
+        if (rc) return rc;
+        if (const char* why = pt_persistent_unsupported(sys)) return fail(PC_ERR_UNSUPPORTED, why);
+    }
+    sys->pt_persistent = on != 0;
+    return PC_OK;
+}
+
+int pc_get_pt_persistent(pc_system* sys, int* on) {
+    int rc = check_sys(sys, false);
+    if (rc) return rc;
+    if (!on) return fail(PC_ERR_INVALID, "null output");
+    *on = sys->pt_persistent ? 1 : 0;
     return PC_OK;
 }
 

@@ -187,6 +187,18 @@ class System:
         call("pc_get_cluster_sweeps", self._h, C.byref(v))
         return bool(v.value)
 
+    def set_pt_persistent(self, on: bool):
+        """Tempering rounds (pt_run) in one persistent cooperative launch: all
+        colour passes of all replicas, the energies and the exchanges, with
+        grid barriers between the phases; raises PyroCMCError (code 4,
+        unsupported) where the system does not qualify."""
+        call("pc_set_pt_persistent", self._h, int(bool(on)))
+
+    def pt_persistent(self) -> bool:
+        v = C.c_int()
+        call("pc_get_pt_persistent", self._h, C.byref(v))
+        return bool(v.value)
+
     def set_kernel_path(self, force_generic: bool):
         """Force the generic bond-table kernels (True) or allow the structured
         pyrochlore kernels (False, default)."""
