@@ -320,9 +320,27 @@ def run_profile_batched(args):
     b.random_spins(5)
     b.pt_configure(T)
     b.ssf_configure(["xx", "yy", "zz"], len(Ls), sorted(Ls))
+    if args.persistent:
+        b.set_pt_persistent(True)
     b.pt_run(4, 10, 16)
     torch.cuda.synchronize()
-    print(f"profile batched: 128 replicas, tile={args.tile}, launches={b.launch_count()}", flush=True)
+    print(f"profile batched: 128 replicas, tile={args.tile}, persistent={args.persistent}, "
+          f"launches={b.launch_count()}", flush=True)
+
+
+def run_profile_energy(args):
+    """Three energy evaluations of the L = 64 field-cool lattice (uniform
+    random spins), for ncu captures of the per-cell energy kernel."""
+    import torch
+
+    import pyro_cmc_b200 as pc
+    torch.cuda.set_device(0)
+    s = pc.pyrochlore_system(WL["L"], J1=WL["J1"], J2=WL["J2"], J3=WL["J3"], B=WL["B"], seed=1)
+    s.random_spins(1)
+    for _ in range(3):
+        s.energy()
+    torch.cuda.synchronize()
+    print(f"profile energy: L={WL['L']}, launches={s.launch_count()}", flush=True)
 
 
 def cpu_baseline_one_core():
@@ -348,6 +366,10 @@ def main():
                          "captures (prints a launch summary, no JSON line)")
     ap.add_argument("--profile-batched", action="store_true",
                     help="4 tempering rounds of the batched form with a fixed tile, for ncu captures (no JSON line)")
+    ap.add_argument("--persistent", action="store_true",
+                    help="with --profile-batched: the rounds in one persistent launch")
+    ap.add_argument("--profile-energy", action="store_true",
+                    help="three energy evaluations of the L = 64 lattice, for ncu captures (no JSON line)")
     ap.add_argument("--profile-grad", action="store_true",
                     help="one warm-up and one forward + backward of the gradient form, for ncu captures (no JSON line)")
     ap.add_argument("--tile", type=int, nargs=3, default=[128, 7, 0], metavar=("THREADS", "CTAS", "VARIANT"),
@@ -370,6 +392,9 @@ def main():
         return
     if args.profile_batched:
         run_profile_batched(args)
+        return
+    if args.profile_energy:
+        run_profile_energy(args)
         return
 
     import numpy as np

@@ -50,6 +50,18 @@ __device__ __forceinline__ float4 load_spin(const float4* p) {
         return __ldcg(p);
 }
 
+// h += J t for a general 3x3 group matrix J (row-major), with every rounding
+// fixed: row a adds fma(J[3a+2], t.z, fma(J[3a+1], t.y, J[3a] t.x)) to h. Left
+// to the compiler, the contraction of the plain expression into FMAs may differ
+// between the kernels that inline it, and the chains of the per-pass,
+// persistent, staged and cluster-resident sweeps would part at the first
+// decision the last bit changes.
+__device__ __forceinline__ void add_matvec(float3& h, const float* J, const float3& t) {
+    h.x = __fadd_rn(h.x, fmaf(J[2], t.z, fmaf(J[1], t.y, __fmul_rn(J[0], t.x))));
+    h.y = __fadd_rn(h.y, fmaf(J[5], t.z, fmaf(J[4], t.y, __fmul_rn(J[3], t.x))));
+    h.z = __fadd_rn(h.z, fmaf(J[8], t.z, fmaf(J[7], t.y, __fmul_rn(J[6], t.x))));
+}
+
 template <int SL, int E, bool NC = true>
 __device__ __forceinline__ float4 load_nb(const float4* __restrict__ S, int Nc, const Coords& c) {
     constexpr int s2 = nb_sl(SL, E), dx = nb_dx(SL, E), dy = nb_dy(SL, E), dz = nb_dz(SL, E);
@@ -79,9 +91,7 @@ __device__ __forceinline__ void add_group(float3& h, const float4* __restrict__ 
     if (mats.active[SL] & (1u << G)) {
         const float3 t = group_sum<SL, G, NC>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
         const float* J = mats.M[SL][G];
-        h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
-        h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
-        h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+        add_matvec(h, J, t);
     }
 }
 
@@ -148,9 +158,7 @@ __device__ __forceinline__ void add_group_v(float3& h, const float4 (&v)[kStruct
         t.z += v[k].z;
     }
     const float* J = mats.M[SL][G];
-    h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
-    h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
-    h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+    add_matvec(h, J, t);
 }
 
 // h += sum of the group matrices times the group sums, groups [G0, G1)
@@ -197,9 +205,7 @@ __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restr
                 h.y = __fadd_rn(h.y, __fmul_rn(J[0], t.y));
                 h.z = __fadd_rn(h.z, __fmul_rn(J[0], t.z));
             } else {
-                h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
-                h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
-                h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+                add_matvec(h, J, t);
             }
         }
     }

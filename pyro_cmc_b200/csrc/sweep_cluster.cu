@@ -57,9 +57,7 @@ __device__ __forceinline__ void cl_add_group(float3& h, const float4 (&v)[kStruc
             t.z += v[k].z;
         }
         const float* J = mats.M[SL][G];
-        h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
-        h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
-        h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+        add_matvec(h, J, t);
     }
 }
 

@@ -106,9 +106,7 @@ __device__ __forceinline__ void row_add_group(float3& h, const float4* rows, con
     if (mats.active[SL] & (1u << G)) {
         const float3 t = row_group_sum<SL, G>(rows, q, std::make_integer_sequence<int, grp_size(SL, G)>{});
         const float* J = mats.M[SL][G];
-        h.x += J[0] * t.x + J[1] * t.y + J[2] * t.z;
-        h.y += J[3] * t.x + J[4] * t.y + J[5] * t.z;
-        h.z += J[6] * t.x + J[7] * t.y + J[8] * t.z;
+        add_matvec(h, J, t);
     }
 }
 template <int SL>
