@@ -40,6 +40,15 @@ __device__ __forceinline__ void uniform_angle(uint32_t w, float* s, float* c) {
     __sincosf(6.2831853f * (u24(w) - 0.5f), s, c);
 }
 
+// Dot product and the products of the moves with every rounding fixed: an FMA
+// chain in a fixed order. Left to the compiler, the contraction of the plain
+// expressions into FMAs may differ between the kernels that inline a move
+// (per-pass, persistent, staged, cluster-resident), and their chains would
+// part at the first decision that the last bit changes.
+__device__ __forceinline__ float dot3_rn(float ax, float ay, float az, float bx, float by, float bz) {
+    return fmaf(az, bz, fmaf(ay, by, __fmul_rn(ax, bx)));
+}
+
 // h = sum over shells J_k * sum of neighbour spins (MC_runner::local_field,
 // src/MC.cpp:87-96).
 __device__ __forceinline__ float3 local_field(const float4* __restrict__ S, const SlTable& tb, int cx, int cy, int cz,
@@ -76,25 +85,29 @@ __device__ __forceinline__ float3 local_field(const float4* __restrict__ S, cons
 // false (spin unchanged) for a zero field or a zero spin.
 template <bool REFLECT>
 __device__ __forceinline__ bool overrelax_spin(float4 s0, float3 h, float sn, float cs, float4& out) {
-    const float n2 = h.x * h.x + h.y * h.y + h.z * h.z;
+    const float n2 = dot3_rn(h.x, h.y, h.z, h.x, h.y, h.z);
     // a zero local field leaves the spin as it is; so does a zero spin (the
     // reference's default-constructed state, which rotation keeps at zero)
-    if (!(n2 > 1e-30f) || !(s0.x * s0.x + s0.y * s0.y + s0.z * s0.z > 0.f)) return false;
-    const float av = h.x * s0.x + h.y * s0.y + h.z * s0.z;
+    if (!(n2 > 1e-30f) || !(dot3_rn(s0.x, s0.y, s0.z, s0.x, s0.y, s0.z) > 0.f)) return false;
+    const float av = dot3_rn(h.x, h.y, h.z, s0.x, s0.y, s0.z);
     float nx, ny, nz;
     if (REFLECT) {
         const float f = 2.f * av / (n2 + 1e-10f);
-        nx = -s0.x + f * h.x;
-        ny = -s0.y + f * h.y;
-        nz = -s0.z + f * h.z;
+        nx = fmaf(f, h.x, -s0.x);
+        ny = fmaf(f, h.y, -s0.y);
+        nz = fmaf(f, h.z, -s0.z);
     } else {
+        // cs s + f h + g (h x s)
         const float f = (1.f - cs) * av / n2;
         const float g = sn * rsqrtf(n2);
-        nx = cs * s0.x + f * h.x + g * (h.y * s0.z - h.z * s0.y);
-        ny = cs * s0.y + f * h.y + g * (h.z * s0.x - h.x * s0.z);
-        nz = cs * s0.z + f * h.z + g * (h.x * s0.y - h.y * s0.x);
+        const float cx = fmaf(h.y, s0.z, -__fmul_rn(h.z, s0.y));
+        const float cy = fmaf(h.z, s0.x, -__fmul_rn(h.x, s0.z));
+        const float cz = fmaf(h.x, s0.y, -__fmul_rn(h.y, s0.x));
+        nx = fmaf(g, cx, fmaf(f, h.x, __fmul_rn(cs, s0.x)));
+        ny = fmaf(g, cy, fmaf(f, h.y, __fmul_rn(cs, s0.y)));
+        nz = fmaf(g, cz, fmaf(f, h.z, __fmul_rn(cs, s0.z)));
     }
-    const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+    const float inv = rsqrtf(dot3_rn(nx, ny, nz, nx, ny, nz));
     out = make_float4(nx * inv, ny * inv, nz * inv, s0.w);  // w: the lifting direction, kept
     return true;
 }
@@ -113,14 +126,14 @@ __device__ __forceinline__ bool metropolis_spin(const PassArgs& a, float4 s0, fl
     float s_a, c_a, s_b, c_b;
     uniform_angle(w.y, &s_a, &c_a);
     uniform_angle(w.w, &s_b, &c_b);
-    float nx = s0.x + sigma * (r0 * c_a);
-    float ny = s0.y + sigma * (r0 * s_a);
-    float nz = s0.z + sigma * (r1 * c_b);
-    const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+    float nx = fmaf(sigma, __fmul_rn(r0, c_a), s0.x);
+    float ny = fmaf(sigma, __fmul_rn(r0, s_a), s0.y);
+    float nz = fmaf(sigma, __fmul_rn(r1, c_b), s0.z);
+    const float inv = rsqrtf(dot3_rn(nx, ny, nz, nx, ny, nz));
     nx *= inv;
     ny *= inv;
     nz *= inv;
-    const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
+    const float dE = dot3_rn(nx - s0.x, ny - s0.y, nz - s0.z, h.x, h.y, h.z);
     if (dE < 0.f || u24_lowbytes(w) < __expf(-dE * invT)) {
         out = make_float4(nx, ny, nz, s0.w);
         return true;
@@ -397,10 +410,10 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
         float s_a, c_a, s_b, c_b;
         uniform_angle(w.y, &s_a, &c_a);
         uniform_angle(w.w, &s_b, &c_b);
-        nx = s0.x + sigma * (r0 * c_a);
-        ny = s0.y + sigma * (r0 * s_a);
-        nz = s0.z + sigma * (r1 * c_b);
-        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+        nx = fmaf(sigma, __fmul_rn(r0, c_a), s0.x);
+        ny = fmaf(sigma, __fmul_rn(r0, s_a), s0.y);
+        nz = fmaf(sigma, __fmul_rn(r1, c_b), s0.z);
+        const float inv = rsqrtf(dot3_rn(nx, ny, nz, nx, ny, nz));
         nx *= inv;
         ny *= inv;
         nz *= inv;
@@ -418,7 +431,7 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
     }
     bool acc = false;
     if (kMet) {
-        const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
+        const float dE = dot3_rn(nx - s0.x, ny - s0.y, nz - s0.z, h.x, h.y, h.z);
         if (dE < 0.f || u < __expf(-dE * invT)) {
             s1 = make_float4(nx, ny, nz, w_after<MODE>(s0.w));
             acc = true;

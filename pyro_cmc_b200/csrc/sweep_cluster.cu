@@ -99,10 +99,10 @@ __device__ __forceinline__ Proposal cl_prepare(const ClusterArgs& a, const float
         float s_a, c_a, s_b, c_b;
         uniform_angle(w.y, &s_a, &c_a);
         uniform_angle(w.w, &s_b, &c_b);
-        float nx = s0.x + sigma * (r0 * c_a);
-        float ny = s0.y + sigma * (r0 * s_a);
-        float nz = s0.z + sigma * (r1 * c_b);
-        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+        float nx = fmaf(sigma, __fmul_rn(r0, c_a), s0.x);
+        float ny = fmaf(sigma, __fmul_rn(r0, s_a), s0.y);
+        float nz = fmaf(sigma, __fmul_rn(r1, c_b), s0.z);
+        const float inv = rsqrtf(dot3_rn(nx, ny, nz, nx, ny, nz));
         p.nx = nx * inv;
         p.ny = ny * inv;
         p.nz = nz * inv;
@@ -135,7 +135,7 @@ __device__ __forceinline__ bool cl_finish(const ClusterArgs& a, float4* own, int
     s1.w = w_after<MODE>(s0.w);
     bool acc = false;
     if (kMet) {
-        const float dE = (p.nx - s0.x) * h.x + (p.ny - s0.y) * h.y + (p.nz - s0.z) * h.z;
+        const float dE = dot3_rn(p.nx - s0.x, p.ny - s0.y, p.nz - s0.z, h.x, h.y, h.z);
         if (dE < 0.f || p.u < __expf(-dE * p.invT)) {
             s1 = make_float4(p.nx, p.ny, p.nz, w_after<MODE>(s0.w));
             acc = true;

@@ -153,10 +153,10 @@ __device__ __forceinline__ unsigned staged_tile(const PassArgs& a, const Tile ti
         float s_a, c_a, s_b, c_b;
         uniform_angle(w.y, &s_a, &c_a);
         uniform_angle(w.w, &s_b, &c_b);
-        nx = s0.x + sigma * (r0 * c_a);
-        ny = s0.y + sigma * (r0 * s_a);
-        nz = s0.z + sigma * (r1 * c_b);
-        const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
+        nx = fmaf(sigma, __fmul_rn(r0, c_a), s0.x);
+        ny = fmaf(sigma, __fmul_rn(r0, s_a), s0.y);
+        nz = fmaf(sigma, __fmul_rn(r1, c_b), s0.z);
+        const float inv = rsqrtf(dot3_rn(nx, ny, nz, nx, ny, nz));
         nx *= inv;
         ny *= inv;
         nz *= inv;
@@ -201,7 +201,7 @@ __device__ __forceinline__ unsigned staged_tile(const PassArgs& a, const Tile ti
     float4 s1 = s0;
     s1.w = w_after<MODE>(s0.w);
     if (kMet) {
-        const float dE = (nx - s0.x) * h.x + (ny - s0.y) * h.y + (nz - s0.z) * h.z;
+        const float dE = dot3_rn(nx - s0.x, ny - s0.y, nz - s0.z, h.x, h.y, h.z);
         if (dE < 0.f || u < __expf(-dE * invT)) {
             s1 = make_float4(nx, ny, nz, w_after<MODE>(s0.w));
             acc = true;
