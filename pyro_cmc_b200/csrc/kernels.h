@@ -30,8 +30,9 @@ enum PassMode {
 // group, whose matrix is 0 everywhere (kVarIsoNoJ2: J2 = 0).
 constexpr int kVarIso = 5, kVarIsoNoJ2 = 6;
 // Or'ed into a load variant (0, kVarIso, kVarIsoNoJ2): spins, own spin and
-// temperature are read with L2-coherent loads, for a kernel that writes them
-// in an earlier phase of the same launch (the persistent tempering kernel).
+// temperature are read with ordinary weak loads instead of the read-only path,
+// for a kernel that writes them in an earlier phase of the same launch (the
+// persistent tempering kernel, whose grid barrier orders the phases).
 constexpr int kVarCoherent = 0x100;
 struct PassArgs {
     float4* spins;
@@ -255,6 +256,10 @@ void launch_pt_exchange(const PtArgs& a, cudaStream_t st);
 // behind a grid barrier. The barrier's waits are bounded: when one runs out
 // the kernel sets *err = kErrGridBarrier and every block leaves.
 constexpr int kErrGridBarrier = 2;
+// Grid barrier state: [0] top arrivals, [1] generation, then kBarrierGroups
+// sub-counters, kBarrierStride words apart (one 128-byte line each).
+constexpr int kBarrierGroups = 32, kBarrierStride = 32;
+constexpr int kBarrierWords = kBarrierStride * (1 + kBarrierGroups);
 struct PersistArgs {
     PassArgs pass;  // pass arguments (tiles, n_tiles, sweep_offset, or_pass unused)
     const Tile* colour_tiles[16];
@@ -275,7 +280,7 @@ struct PersistArgs {
     double* mag;  // per replica sum of S
     int R;
     PtArgs pt;
-    unsigned int* bar;  // [2]: arrivals, generation (zero before the first launch)
+    unsigned int* bar;  // [kBarrierWords], zero before the launch
     int max_polls;      // bound of each barrier wait (polls of ~64 ns)
 };
 // Blocks that fit on the device at once for this block size (0: unsupported).

@@ -382,14 +382,14 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
     site_field<SL, VAR>(S, a, rep, c, v, 0);  // issue loads (VAR 1, 2)
     const size_t i = size_t(SL) * rep.Nc + cell;
     constexpr bool kCoherent = (VAR & kVarCoherent) != 0;
-    const float4 s0 = kCoherent ? __ldcg(S + i) : S[i];
+    const float4 s0 = kCoherent ? __ldca(S + i) : S[i];
     constexpr bool kMet = MODE == kMetropolis || MODE == kFusedRotate || MODE == kFusedReflect;
     constexpr bool kRot = MODE == kOverrelaxRotate || MODE == kFusedRotate;
     // draws first: they do not depend on the local field, so they overlap the loads
     uint4 w = make_uint4(0, 0, 0, 0);
     float sigma = 0.f, invT = 0.f;
     if (kMet) {
-        const double T = kCoherent ? __ldcg(a.T_rep + r) : a.T_rep[r];
+        const double T = kCoherent ? __ldca(a.T_rep + r) : a.T_rep[r];
         sigma = sqrtf(float(T) * a.inv_T_ref);
         invT = float(1.0 / T);
         w = site_draw_rk(a.rkeys, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));

@@ -10,7 +10,8 @@
 // sequence of updates as with one launch per colour pass. Phases are separated
 // by a grid barrier (arrive on a counter, wait on a generation word). Spins,
 // temperatures and energies written in an earlier phase of the launch are read
-// with L2-coherent loads (kVarCoherent), never through the read-only path.
+// with ordinary loads ordered by the barrier's fences (kVarCoherent), never
+// through the read-only path.
 //
 // The energy phase counts every bond once from its lower-sublattice end (one
 // thread per site, struct_field_upper) into per-tile FP64 partials, the next
@@ -35,6 +36,12 @@ namespace pc {
 
 namespace {
 
+// Two-level arrival: block b arrives on sub-counter b % kBarrierGroups (each
+// on its own 128-byte line), the last arrival of a group arrives on the top
+// counter, and the last of those bumps the generation that every block waits
+// on. Arrivals on one address are serialised at its L2 slice; spread over the
+// groups, a barrier of ~1000 blocks costs about two atomic round trips instead
+// of ~1000 serialised atomics.
 __device__ __forceinline__ bool grid_barrier(const PersistArgs& p) {
     __shared__ int s_ok;
     __syncthreads();
@@ -43,13 +50,23 @@ __device__ __forceinline__ bool grid_barrier(const PersistArgs& p) {
         volatile int* err = p.pass.err;
         const unsigned int g = *gen;  // before arriving: the generation cannot move until this block arrives
         __threadfence();              // this block's writes before the arrival
-        const unsigned int arrived = atomicAdd(p.bar, 1u);
+        const unsigned int grp = blockIdx.x % kBarrierGroups;
+        const unsigned int n_grp = (gridDim.x - grp + kBarrierGroups - 1) / kBarrierGroups;
+        const unsigned int n_top = gridDim.x < kBarrierGroups ? gridDim.x : kBarrierGroups;
+        unsigned int* sub = p.bar + kBarrierStride * (1 + grp);
         int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(p.bar, 0u);
+        bool waiter = true;
+        if (atomicAdd(sub, 1u) == n_grp - 1) {
+            atomicExch(sub, 0u);
             __threadfence();
-            atomicAdd(p.bar + 1, 1u);
-        } else {
+            if (atomicAdd(p.bar, 1u) == n_top - 1) {
+                atomicExch(p.bar, 0u);
+                __threadfence();
+                atomicAdd(p.bar + 1, 1u);
+                waiter = false;
+            }
+        }
+        if (waiter) {
             int polls = 0;
             while (*gen == g) {
                 if (*err != 0) {

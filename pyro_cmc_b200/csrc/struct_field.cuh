@@ -40,14 +40,16 @@ __device__ __forceinline__ int pick(const int (&v)[3]) {
 // sublattices than it writes), so loads may use the non-coherent read-only
 // path (__ldg). A kernel that also writes the spins it gathers in a later
 // phase (the persistent tempering kernel: colour passes separated by grid
-// barriers) loads with NC = false: L2-coherent loads (__ldcg) that never hit
-// a stale L1 line.
+// barriers) loads with NC = false: ordinary weak loads (ld.global.ca), which
+// keep the L1 hits of neighbouring threads inside a phase; the grid barrier's
+// gpu-scope fences order them after the other blocks' writes of the earlier
+// phases (PTX memory model: fence, flag, fence message passing).
 template <bool NC>
 __device__ __forceinline__ float4 load_spin(const float4* p) {
     if constexpr (NC)
         return __ldg(p);
     else
-        return __ldcg(p);
+        return __ldca(p);
 }
 
 // h += J t for a general 3x3 group matrix J (row-major), with every rounding

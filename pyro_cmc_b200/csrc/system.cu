@@ -236,7 +236,7 @@ struct pc_system {
     uint64_t pt_sweeps_done = 0;
     // rounds in one persistent cooperative launch (pt_persistent.cu)
     bool pt_persistent = false;
-    DevBuf<unsigned int> d_bar;                 // grid barrier: arrivals, generation
+    DevBuf<unsigned int> d_bar;                 // grid barrier state (pc::kBarrierWords)
     std::map<std::array<int, 3>, int> persist_cap;  // (iso, fused, threads) -> resident blocks
     int barrier_polls = kBarrierMaxPolls;       // bound of each grid-barrier wait (pc_set_wait_limit)
 
@@ -1963,9 +1963,13 @@ int launch_persistent(pc_system* s, int n_rounds, int n_sweep, int exchange) {
     if (it == s->persist_cap.end())
         it = s->persist_cap.emplace(key, pc::pt_persistent_capacity(s->iso_kind, fused, s->threads)).first;
     if (it->second <= 0) return fail(PC_ERR_UNSUPPORTED, "no cooperative launch of the persistent kernel fits");
-    int most = s->R;
+    // as few blocks as give every block the same number of tiles of the largest
+    // colour class: each pass ends at a barrier, so the block with the most
+    // tiles sets its length
+    int most = 1;
     for (int c = 0; c < s->n_colours; ++c) most = std::max(most, s->n_colour_tiles[size_t(c)]);
-    const int grid = std::max(1, std::min(it->second, most));
+    const int per_block = (most + it->second - 1) / it->second;
+    const int grid = std::max(1, (most + per_block - 1) / per_block);
     pc::PersistArgs p;
     std::memset(&p, 0, sizeof(p));
     p.pass = pass_args(s, 0, 0, 0);
@@ -1991,7 +1995,7 @@ int launch_persistent(pc_system* s, int n_rounds, int n_sweep, int exchange) {
     p.pt = pt_args(s);
     p.bar = s->d_bar.p;
     p.max_polls = s->barrier_polls;
-    PC_CK(cudaMemsetAsync(s->d_bar.p, 0, 2 * sizeof(unsigned int), s->stream));
+    PC_CK(cudaMemsetAsync(s->d_bar.p, 0, pc::kBarrierWords * sizeof(unsigned int), s->stream));
     const int e = pc::launch_pt_persistent(p, s->iso_kind, grid, s->threads, s->stream);
     if (e != 0) return fail(PC_ERR_CUDA, std::string("persistent launch: ") + cudaGetErrorString(cudaError_t(e)));
     s->launches++;
@@ -2004,7 +2008,7 @@ int launch_persistent(pc_system* s, int n_rounds, int n_sweep, int exchange) {
 // exchange come last, after a sample that follows the round's last sweep, as
 // in the per-pass schedule.
 int run_pt_persistent(pc_system* s, int n_rounds, int n_sweep, int ssf_every) {
-    if (!s->d_bar.p) PC_CK(s->d_bar.alloc(2));
+    if (!s->d_bar.p) PC_CK(s->d_bar.alloc(pc::kBarrierWords));
     PC_CK(cudaMemsetAsync(s->d_err.p, 0, sizeof(int), s->stream));
     if (ssf_every <= 0) {
         int rc = n_rounds > 0 ? launch_persistent(s, n_rounds, n_sweep, 1) : PC_OK;

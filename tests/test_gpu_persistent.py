@@ -135,3 +135,24 @@ def test_persistent_rounds_refused_where_not_covered():
     with pytest.raises(pc.PyroCMCError) as ei:
         s.set_pt_persistent(True)
     assert ei.value.code == _lib.ERR_UNSUPPORTED
+
+
+def test_persistent_rounds_at_the_batched_workload():
+    """The batched tempering form at full size (128 replicas, L = 8, 12, 16,
+    24 with 32 temperatures each, J = (1, 0, 0.02), B = (0, 0, 0.1), the fused
+    schedule), 3 rounds of 10 sweeps with S(q) every 16: ~1000 resident blocks
+    gather neighbours that other blocks wrote one barrier earlier. Spins,
+    slots, exchange statistics and S(q) accumulators identical to the per-pass
+    graphs."""
+    Ls = [8] * 32 + [12] * 32 + [16] * 32 + [24] * 32
+    T = np.concatenate([np.geomspace(2.0, 0.02, 32)] * 4)
+    c = dict(J1=1.0, J2=0.0, J3=0.02, B=(0.0, 0.0, 0.1))
+    a, b = _pair(Ls, T, c, 1, 7)
+    for s in (a, b):
+        s.ssf_configure(["xx", "yy", "zz"], len(Ls), sorted(Ls))
+        s.pt_run(3, 10, 16)
+    _same_chain(a, b, len(Ls))
+    for slot in (0, 40, 70, 127):
+        L = sorted(Ls)[slot]
+        for x, y in zip(a.ssf_read(slot, L), b.ssf_read(slot, L)):
+            np.testing.assert_array_equal(np.asarray(x), np.asarray(y))
