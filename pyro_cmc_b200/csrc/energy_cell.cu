@@ -177,7 +177,11 @@ __device__ __forceinline__ void target_batch(float (&acc)[kAcc], const float3 (&
      ...);
 }
 
-constexpr int kTargetBatch = 8;
+// Targets loaded together per batch. With 4 (and 5 resident blocks of 128:
+// 96 registers, a few spilled to L1) the L = 64 energy takes 28 us against 33
+// with 8 targets and 3 blocks (168 registers, no spills): more warps in flight
+// hide more of the gather latency than the spills cost (same sums either way).
+constexpr int kTargetBatch = 4;
 
 template <int T0, int ISO>
 __device__ __forceinline__ void remote_bonds(float (&acc)[kAcc], const float3 (&own)[16], const char* base,
@@ -198,7 +202,7 @@ __device__ __forceinline__ void load_own(float3 (&own)[16], const char* base, ui
 }
 
 template <int ISO>
-__global__ void __launch_bounds__(kEnergyCellThreads, 3) energy_cell_kernel(const __grid_constant__ EnergyCellArgs a) {
+__global__ void __launch_bounds__(kEnergyCellThreads, 5) energy_cell_kernel(const __grid_constant__ EnergyCellArgs a) {
     __shared__ double red[4 * 32];
     const int4 tile = a.tiles[blockIdx.x];  // (replica, first cell, cells, -)
     const ReplicaDev rep = a.reps[tile.x];

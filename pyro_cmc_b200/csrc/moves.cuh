@@ -505,7 +505,12 @@ __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant_
 // The colour passes gather 30 neighbours per site through L1 and use almost no
 // shared memory: ask for the largest L1 (smallest shared-memory carveout), once
 // per kernel and device, whatever kernels with large shared memory (the S(q)
-// stages) ran before.
+// stages) ran before. With the 8 KB configuration this leaves 7 resident
+// blocks of 128 threads (every block holds 1 KB of shared memory for the
+// system) where 64 registers would allow 8; a larger carveout that admits the
+// 8th block (the driver chose 164 KB for a 7 % request) measured slower at
+// L = 64 (10.73 against 10.50 us per pass): the L1 it takes costs more than
+// the extra warps give.
 inline void prefer_l1(const void* fn) {
     static std::mutex mu;
     static std::set<std::pair<int, const void*>> done;
