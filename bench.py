@@ -91,31 +91,8 @@ def measured_peaks():
 # capture of the same kernel (bench.py --profile-case, a cold-L2 launch):
 # DRAM bytes read + written, and L2 -> SM bytes. A profiler figure, reported
 # with its source; the timed loop itself runs with the lattice L2-resident.
-PROFILED_PASS = {"dram_bytes": 68572672.0, "l2_to_sm_bytes": 95.7e6,
+PROFILED_PASS = {"dram_bytes": 68572672.0, "l2_to_sm_bytes": 95.7e6, "lts_throughput_pct": 27.8,
                  "source": "ncu --set full of struct_pass_kernel, bench.py --profile-case (profiles/colour_pass_L64.md)"}
-
-
-def l2_copy_bandwidth(torch, stream):
-    """Device copy of a 32 MiB buffer into another (both resident in the
-    126 MB L2), best of 20, in GB/s counting read + write bytes: the L2
-    bandwidth the colour pass's neighbour gathers are measured against."""
-    n = 32 << 20
-    a = torch.empty(n, dtype=torch.uint8, device="cuda")
-    b = torch.empty_like(a)
-    a.fill_(1)
-    for _ in range(5):
-        b.copy_(a)
-    best = None
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for _ in range(20):
-        e0.record(stream)
-        for _ in range(10):
-            b.copy_(a)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / 10
-        best = ms if best is None else min(best, ms)
-    return 2 * n / (best * 1e-3) / 1e9
 
 
 class ClockSampler:
@@ -510,7 +487,6 @@ def main():
     peak, peak_kind = measured_peaks()
     alg_bytes = 32.0 * s.Nc()  # one colour pass: one sublattice, float4 read + write per site
     achieved = alg_bytes / (t_pass * 1e-3) / 1e9 if t_pass > 0 else None
-    l2_gbs = l2_copy_bandwidth(torch, stream)
     l2_bytes = PROFILED_PASS["l2_to_sm_bytes"]
     gather_bytes = 32 * 16.0 * s.Nc()  # per site: own float4 read + write and 30 neighbour float4 loads
     roofline = {"bound": "hbm", "kernel": "struct_pass_kernel (fused Metropolis + overrelaxation colour pass)",
@@ -520,15 +496,17 @@ def main():
                 "traffic": PROFILED_PASS["dram_bytes"], "traffic_source": "profile: " + PROFILED_PASS["source"],
                 "alg_bytes_per_launch": alg_bytes, "launch_ms": t_pass, "launch_ms_isolated": t_met_isolated,
                 "l2": {"l2_to_sm_bytes_per_launch": l2_bytes, "source": "profile: " + PROFILED_PASS["source"],
-                       "gather_request_bytes_per_launch": gather_bytes, "l2_copy_gbs_measured": l2_gbs,
-                       "frac_l2": (l2_bytes / (t_pass * 1e-3) / 1e9) / l2_gbs if t_pass > 0 else None},
+                       "gather_request_bytes_per_launch": gather_bytes,
+                       "l2_to_sm_gbs": l2_bytes / (t_pass * 1e-3) / 1e9 if t_pass > 0 else None,
+                       "lts_throughput_pct_of_peak": PROFILED_PASS["lts_throughput_pct"]},
                 "note": "achieved = 32 B x Nc sites per launch / mean launch duration: CUDA events around the "
                         "graph-launched sweeps of the timed steps over their colour-pass launches (inter-kernel "
                         "gaps included); launch_ms_isolated: events around single launches outside graphs. "
                         "frac_survey_64B counts 64 B per spin-update (Metropolis + overrelaxation read + write, "
                         "the survey's accounting) for the same launch. The lattice (67 MB) stays in L2 during "
-                        "the timed loop; the neighbour gathers are L2 -> SM traffic (l2), measured against a "
-                        "device copy of a 32 MiB L2-resident buffer timed in this run"}
+                        "the timed loop; the neighbour gathers are L2 -> SM traffic (l2): the profiled bytes per launch "
+                        "over this run's launch time, and the L2 throughput ncu reports for the launch as a share "
+                        "of the L2's own peak"}
 
     extras = {}
     if not args.no_extras and rank == 0:
