@@ -157,3 +157,33 @@ def test_anneal_cli_errors():
     r = subprocess.run([exe, "-o", "/tmp", "-s", "1", "4", "--J1", "1", "--J3", "0.1", "--Q", "0.5",
                         "--T_sample", "0.1", "--dry_run"], capture_output=True, text=True)
     assert r.returncode == 1 and "mutually exclusive" in r.stderr
+
+
+def test_hdf5_edge_cases_and_corruption(tmp_path):
+    """Empty and scalar datasets, an attribute on a dataset, implicit nested
+    groups and a dataset added after a commit read back; a flipped byte in an
+    object header is caught by its lookup3 checksum."""
+    import subprocess
+
+    from pyro_cmc_b200.h5compat import File
+
+    exe = _compile(tmp_path, "h5_edges")
+    out = tmp_path / "e.h5"
+    subprocess.run([str(exe), str(out)], check=True)
+    with File(str(out)) as f:
+        assert list(f["/a/b/c/empty"]) == []
+        np.testing.assert_array_equal(f["/a/b/vec"][:], [1.5, -2.0, 3.25, 0.0])
+        assert float(f["/scalar"]) == 42.0 and f["/scalar"].shape == ()
+        assert f["/a/none"].shape == (0,)
+        np.testing.assert_array_equal(f["/a/b/c/late"][:], [-1, 1])
+        assert set(f["/a/b"].keys()) == {"c", "vec"} and set(f["/a/b/c"].keys()) == {"empty", "late"}
+        assert int(f._attrs("a/b/vec")["k"]) == 7
+    raw = bytearray(out.read_bytes())
+    i = raw.rfind(b"OHDR")
+    raw[i + 12] ^= 0xFF
+    bad = tmp_path / "bad.h5"
+    bad.write_bytes(bytes(raw))
+    with pytest.raises(ValueError, match="checksum"):
+        with File(str(bad)) as f:
+            f["/a/b/c/late"][:]
+
