@@ -236,3 +236,48 @@ def test_anneal_npz_container_holds_the_same_tree(tmp_path):
             np.testing.assert_array_equal(a["ssf"].attrs[k], b["ssf"].attrs[k])
     with File(only(tmp_path / "h", ".spins.h5")) as a, File(only(tmp_path / "z", ".spins.npz")) as b:
         np.testing.assert_array_equal(a["/spin_orientation"][:], b["/spin_orientation"][:])
+
+
+def test_anneal_file_holds_finished_temperatures_while_running(tmp_path):
+    """The reference pre-allocates /ssf/static_corr and writes each sample
+    temperature's slice when its sampling ends (include/ssf_manager.hpp:375-465),
+    so an interrupted run leaves a readable file with the temperatures finished
+    so far. The driver is paused (SIGSTOP: its host thread stops, kernels
+    already queued finish) when it starts sampling the second temperature; the
+    file on disk then holds the first temperature's slice and zeros in the
+    others, and no /ssf/T_list yet. After SIGCONT the run completes normally."""
+    import signal
+
+    build.build()
+    exe = os.path.join(build.BIN, "anneal")
+    args = ["-o", tmp_path, "-s", 3, 4, "--J1", 1, "--J2", -0.1, "--T_sample", 1.0, 0.5, 0.2, "--n_steps", 30,
+            "--n_sweep", 4, "--n_burn_in", 4, "--n_sample", 4, "--init_uniform"]
+    p = subprocess.Popen(["stdbuf", "-oL", exe, *map(str, args)], stdout=subprocess.PIPE, text=True)
+    seen = 0
+    stopped = False
+    try:
+        for line in p.stdout:
+            if line.startswith("Sampling at T"):
+                seen += 1
+                if seen == 2:
+                    os.kill(p.pid, signal.SIGSTOP)
+                    stopped = True
+                    break
+        assert stopped
+        with File(only(tmp_path, ".out.h5")) as f:
+            sc = f["/ssf/static_corr"][:]
+            assert "/ssf/T_list" not in f
+        assert sc.shape == (6, 3, 64, 2)
+        # T_sample sorted ascending: slot 2 is T = 1.0, sampled first
+        assert np.abs(sc[:, 2]).max() > 0
+        assert np.abs(sc[:, :2]).max() == 0
+    finally:
+        if stopped:
+            os.kill(p.pid, signal.SIGCONT)
+        p.stdout.read()
+        p.wait(timeout=300)
+    assert p.returncode == 0
+    with File(only(tmp_path, ".out.h5")) as f:
+        sc = f["/ssf/static_corr"][:]
+        np.testing.assert_array_equal(f["/ssf/T_list"][:], [0.2, 0.5, 1.0])
+    assert (np.abs(sc).reshape(6, 3, -1).max(axis=2) > 0).all()
