@@ -14,20 +14,24 @@ step starts with a cold L2.
 
   value   device-timed steps, spins resident in HBM (CUDA events on the
           system's stream, max over ranks)
-  e2e     the same steps through the host-buffer C-ABI call pc_step_host:
-          pinned-host spins in, spins and energy out, copies inside the timing
-  roofline  the Metropolis colour-pass kernel: 32 B (float4 read + write) per
-          updated site against the measured HBM copy bandwidth
-  cpu_baseline  the oracle (FP64 restatement of the reference sweep) on one
-          host core, on a bounded sample of the same lattice
+  e2e     the same steps through the host-buffer C-ABI call pc_step_host3:
+          pinned-host spins (x, y, z float32) in, spins and energy out, copies
+          inside the timing; the float4 call pc_step_host beside it
+  roofline  the fused colour-pass kernel: 32 B (float4 read + write) per
+          updated site against the measured HBM copy bandwidth, with the
+          survey's 64 B per spin-update and the L2 side beside it
+  cpu_baseline  the reference's own src/MC.cpp sweep compiled unchanged
+          (oracle/_ref; the oracle's FP64 restatement where it was not built)
+          on one host core, on a bounded sample of the same lattice
 Also reported: the batched parallel-tempering form (128 replicas, L in
-{8,12,16,24} x 32 T) and the gradient form (256 x L=8 energy + S(q)
-forward/backward).
+{8,12,16,24} x 32 T; per-pass graphs and one persistent launch), the L=16
+anneal step for one and for 32 seeds, and the gradient form (256 x L=8
+energy + S^zz(q) loss, forward and backward with coupling gradients).
 
 --gpus N runs N independent replicas of the workload, one per GPU (the path
 has no exchange across GPUs): scaling "weak", value = all ranks' updates / the
-slowest rank's time. --impl reference runs the CPU reference arm (the oracle
-on all host cores) on rank 0 only.
+slowest rank's time. --impl reference runs the CPU reference arm (the same
+compiled reference code on all host threads) on rank 0 only.
 """
 from __future__ import annotations
 
@@ -465,24 +469,32 @@ def main():
     t_met_isolated, _ = s.kernel_times()
     s.set_kernel_timing(False)
 
-    # end to end through host buffers
-    S4_in = torch.empty((N, 4), dtype=torch.float32, pin_memory=True).numpy()
-    S4_out = torch.empty((N, 4), dtype=torch.float32, pin_memory=True).numpy()
-    S4_in[:] = s.spins_f4()
-    for _ in range(args.warmup):
-        s.step_host(S4_in, S4_out, T, WL["n_sweep"], WL["ssf_every"], 0)
-    barrier()
-    e2e_s = 0.0
-    for _ in range(args.steps):
-        flush_buf.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        s.step_host(S4_in, S4_out, T, WL["n_sweep"], WL["ssf_every"], 0)  # returns after the D2H copy
-        e2e_s += time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s / args.steps, dist)
-    e2e = {"value": world * N * WL["n_sweep"] / e2e_s, "unit": UNIT, "h2d_bytes_per_step": N * 16,
-           "d2h_bytes_per_step": N * 16 + 8, "ms_per_step": e2e_s * 1e3,
-           "call": "pc_step_host (pinned host spins in/out)"}
+    # end to end through host buffers: the packed (x, y, z) call, and the
+    # float4 call beside it
+    def time_e2e(step, cols):
+        S_in = torch.empty((N, cols), dtype=torch.float32, pin_memory=True).numpy()
+        S_out = torch.empty((N, cols), dtype=torch.float32, pin_memory=True).numpy()
+        S_in[:] = s.spins_f4()[:, :cols]
+        for _ in range(args.warmup):
+            step(S_in, S_out, T, WL["n_sweep"], WL["ssf_every"], 0)
+        barrier()
+        tot = 0.0
+        for _ in range(args.steps):
+            flush_buf.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            step(S_in, S_out, T, WL["n_sweep"], WL["ssf_every"], 0)  # returns after the D2H copy
+            tot += time.perf_counter() - t0
+        return max_over_ranks(tot / args.steps, dist)
+
+    e2e_s = time_e2e(s.step_host3, 3)
+    e2e4_s = time_e2e(s.step_host, 4)
+    e2e = {"value": world * N * WL["n_sweep"] / e2e_s, "unit": UNIT, "h2d_bytes_per_step": N * 12,
+           "d2h_bytes_per_step": N * 12 + 8, "ms_per_step": e2e_s * 1e3,
+           "call": "pc_step_host3 (pinned host spins as x, y, z float32 in and out)",
+           "float4": {"value": world * N * WL["n_sweep"] / e2e4_s, "ms_per_step": e2e4_s * 1e3,
+                      "h2d_bytes_per_step": N * 16, "d2h_bytes_per_step": N * 16 + 8,
+                      "call": "pc_step_host (pinned host spins as float4 in and out)"}}
 
     peak, peak_kind = measured_peaks()
     alg_bytes = 32.0 * s.Nc()  # one colour pass: one sublattice, float4 read + write per site

@@ -368,6 +368,14 @@ int pc_set_tile(pc_system* sys, int threads, int ctas_per_sm);
  * to S4_out and the energy per cell to *e_out. */
 int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, int n_sweep, int ssf_every,
                  int ssf_slot, double* e_out, uint64_t* accepted);
+/* The same step with host spins as N x 3 floats (x, y, z per site, the three
+ * components of the reference's HeisenbergSpin::S, include/MC.hpp:55): 12
+ * bytes a spin cross the bus instead of 16. The spins are unpacked and packed
+ * on the device; the lifting directions of lifted Metropolis (the fourth
+ * float4 component) stay on the device. Same chain and results as
+ * pc_step_host given the same spins. */
+int pc_step_host3(pc_system* sys, const float* S3_in, float* S3_out, double T, int n_sweep, int ssf_every,
+                  int ssf_slot, double* e_out, uint64_t* accepted);
 /* CUDA events around the last pc_sweep call's kernels: average duration in
  * milliseconds of the Metropolis and overrelaxation colour-pass kernels. */
 int pc_last_kernel_times(pc_system* sys, double* metropolis_ms, double* overrelax_ms);

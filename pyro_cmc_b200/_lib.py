@@ -92,6 +92,7 @@ _SIGNATURES = {
     "pc_get_tile": (_I, [_P, _IP, _IP]),
     "pc_set_tile": (_I, [_P, _I, _I]),
     "pc_step_host": (_I, [_P, _FP, _FP, _D, _I, _I, _I, _DP, _U64P]),
+    "pc_step_host3": (_I, [_P, _FP, _FP, _D, _I, _I, _I, _DP, _U64P]),
     "pc_last_kernel_times": (_I, [_P, _DP, _DP]),
     "pc_set_kernel_timing": (_I, [_P, _I]),
     "pc_set_launch_overlap": (_I, [_P, _I]),

@@ -9,7 +9,8 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpyrocmc.so")
 SOURCES = ["system.cu", "sweep.cu", "sweep_lifted.cu", "sweep_staged.cu", "sweep_cluster.cu", "grad.cu", "ssf.cu",
-           "pt.cu", "pt_persistent.cu", "noalloc.cu", "lt.cu", "merge.cu", "energy_cell.cu"]
+           "pt.cu", "pt_persistent.cu", "noalloc.cu", "lt.cu", "merge.cu", "energy_cell.cu",
+           "hostio.cu"]
 HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh", "struct_field.cuh", "moves.cuh", "dft.cuh", "pt.cuh"]
 
 NVCC_FLAGS = [

@@ -249,6 +249,11 @@ struct PtArgs {
 };
 void launch_pt_exchange(const PtArgs& a, cudaStream_t st);
 
+// Packed host spins (hostio.cu): (x, y, z) x n <-> the first three float4
+// components; unpacking keeps each spin's fourth component.
+void launch_spins_from_xyz(float4* spins, const float* xyz, int64_t n, cudaStream_t st);
+void launch_spins_to_xyz(float* xyz, const float4* spins, int64_t n, cudaStream_t st);
+
 // Tempering rounds of a batch of replicas in one persistent cooperative launch
 // (pt_persistent.cu): per round, n_sweep sweeps (every colour pass of every
 // replica; a grid barrier between passes), then, with `exchange`, the energy

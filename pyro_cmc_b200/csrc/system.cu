@@ -162,6 +162,7 @@ struct pc_system {
     DevBuf<uint64_t> d_sweep;
     DevBuf<unsigned long long> d_acc;
     DevBuf<int> d_err;  // set by a kernel whose bounded wait ran out
+    DevBuf<float> d_stage3;  // pc_step_host3: replica 0's spins as packed (x, y, z)
     int staged_rl = 0;  // load variant 3: largest row tile (R*L sites)
     int wait_polls = pc::kStagedMaxPolls;  // load variant 3: bound of the first wait (pc_set_wait_limit)
     DevBuf<SlTable> d_tab_active, d_tab_full;
@@ -277,6 +278,7 @@ struct pc_system {
         d_sweep.release();
         d_acc.release();
         d_err.release();
+        d_stage3.release();
         d_tab_active.release();
         d_tab_full.release();
         for (auto& t : d_colour_tiles) t.release();
@@ -2172,7 +2174,6 @@ int pc_energy_grad_field(pc_system* sys, const void* field_dev, const double* g,
 namespace {
 int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double* e_per_cell, void* grad_S_dev,
                    double* grad_J, double* grad_B) {
-    int rc = PC_OK;
     const int ns = int(sys->specs.size());
     // the structured kernel forms the coupling products only when they are asked for
     const bool structured = sys->grad_struct && sys->threads <= 256;
@@ -2238,7 +2239,6 @@ int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double*
         if (grad_J)
             for (int k = 0; k < 9 * ns; ++k) grad_J[size_t(r) * 9 * size_t(ns) + size_t(k)] = gr * o[4 + k] / nc;
     }
-    (void)rc;
     return PC_OK;
 }
 }  // namespace
@@ -2395,8 +2395,12 @@ int pc_autotune(pc_system* sys) {
 }
 
 // --------------------------------------------------------------- bench API
-int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, int n_sweep, int ssf_every,
-                 int ssf_slot, double* e_out, uint64_t* accepted) {
+namespace {
+// The host-buffer step of pc_step_host (float4 spins, packed = false) and
+// pc_step_host3 (packed (x, y, z) spins, unpacked and packed on the device in
+// a staging buffer).
+int step_host(pc_system* sys, const float* S_in, float* S_out, bool packed, double T, int n_sweep, int ssf_every,
+              int ssf_slot, double* e_out, uint64_t* accepted) {
     int rc = check_sys(sys);
     if (rc) return rc;
     if (!(T > 0)) return fail(PC_ERR_INVALID, "temperature must be positive");
@@ -2404,7 +2408,10 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     const bool do_ssf = ssf_slot >= 0 && ssf_every > 0;
     if (do_ssf && (!sys->ssf_ready || ssf_slot >= sys->n_slots || sys->L_of_slot[size_t(ssf_slot)] != sys->L[0]))
         return fail(PC_ERR_STATE, "ssf slot not configured for replica 0");
-    const size_t bytes = sizeof(float4) * size_t(sys->N(0));
+    const int64_t n0 = sys->N(0);
+    const size_t bytes = (packed ? 3 * sizeof(float) : sizeof(float4)) * size_t(n0);
+    if (packed && sys->d_stage3.n < size_t(3 * n0)) PC_CK(sys->d_stage3.alloc(size_t(3 * n0)));
+    void* dev_io = packed ? static_cast<void*>(sys->d_stage3.p) : static_cast<void*>(sys->d_spins.p);
     if (!sys->copy_stream) {
         PC_CK(cudaStreamCreateWithFlags(&sys->copy_stream, cudaStreamNonBlocking));
         PC_CK(cudaEventCreateWithFlags(&sys->ev_swept, cudaEventDisableTiming));
@@ -2415,7 +2422,12 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     double* st_e = st_T + R;
     uint64_t* st_acc = reinterpret_cast<uint64_t*>(st_e + 1);
     int* st_flag = reinterpret_cast<int*>(st_acc + 1);
-    PC_CK(cudaMemcpyAsync(sys->d_spins.p, S4_in, bytes, cudaMemcpyHostToDevice, sys->stream));
+    PC_CK(cudaMemcpyAsync(dev_io, S_in, bytes, cudaMemcpyHostToDevice, sys->stream));
+    if (packed) {
+        pc::launch_spins_from_xyz(sys->d_spins.p, sys->d_stage3.p, n0, sys->stream);
+        PC_LAUNCH_CK();
+        sys->launches++;
+    }
     for (size_t r = 0; r < R; ++r) st_T[r] = T;
     PC_CK(cudaMemcpyAsync(sys->d_T.p, st_T, sizeof(double) * R, cudaMemcpyHostToDevice, sys->stream));
     PC_CK(cudaMemsetAsync(sys->d_acc.p, 0, sizeof(unsigned long long) * size_t(sys->R), sys->stream));
@@ -2431,7 +2443,7 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     int done = 0;
     bool copying = false;
     // once the result copy is enqueued, every return (error paths included)
-    // waits for it: the caller may reuse or free S4_out as soon as we return
+    // waits for it: the caller may reuse or free S_out as soon as we return
     struct CopyWait {
         const bool& active;
         cudaStream_t s;
@@ -2447,9 +2459,14 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
             done += chunk;
         }
         if (done == n_sweep && !copying) {  // spins final: copy them out while S(q) and the energy run
+            if (packed) {
+                pc::launch_spins_to_xyz(sys->d_stage3.p, sys->d_spins.p, n0, sys->stream);
+                PC_LAUNCH_CK();
+                sys->launches++;
+            }
             PC_CK(cudaEventRecord(sys->ev_swept, sys->stream));
             PC_CK(cudaStreamWaitEvent(sys->copy_stream, sys->ev_swept, 0));
-            PC_CK(cudaMemcpyAsync(S4_out, sys->d_spins.p, bytes, cudaMemcpyDeviceToHost, sys->copy_stream));
+            PC_CK(cudaMemcpyAsync(S_out, dev_io, bytes, cudaMemcpyDeviceToHost, sys->copy_stream));
             copying = true;
         }
         if (do_ssf && chunk == ssf_every) {
@@ -2476,6 +2493,17 @@ int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, in
     if (e_out) *e_out = *st_e;
     if (accepted) *accepted = *st_acc;
     return device_error_flag(sys, *st_flag);
+}
+}  // namespace
+
+int pc_step_host(pc_system* sys, const float* S4_in, float* S4_out, double T, int n_sweep, int ssf_every,
+                 int ssf_slot, double* e_out, uint64_t* accepted) {
+    return step_host(sys, S4_in, S4_out, false, T, n_sweep, ssf_every, ssf_slot, e_out, accepted);
+}
+
+int pc_step_host3(pc_system* sys, const float* S3_in, float* S3_out, double T, int n_sweep, int ssf_every,
+                  int ssf_slot, double* e_out, uint64_t* accepted) {
+    return step_host(sys, S3_in, S3_out, true, T, n_sweep, ssf_every, ssf_slot, e_out, accepted);
 }
 
 int pc_set_wait_limit(pc_system* sys, int polls) {

@@ -487,6 +487,19 @@ class System:
              int(n_sweep), int(ssf_every), int(ssf_slot), C.byref(e), C.byref(acc))
         return e.value, acc.value
 
+    def step_host3(self, S3_in, S3_out, T: float, n_sweep: int, ssf_every: int = 0, ssf_slot: int = -1):
+        """step_host with packed host spins (pc_step_host3): float32 [N, 3]
+        numpy arrays (pinned for full speed), 12 bytes a spin over the bus;
+        the lifting directions stay on the device."""
+        for a in (S3_in, S3_out):
+            if a.dtype != np.float32 or a.shape != (self.N(0), 3) or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError("step_host3 takes C-contiguous float32 [N, 3] arrays")
+        e = C.c_double(0)
+        acc = C.c_uint64(0)
+        call("pc_step_host3", self._h, S3_in.ctypes.data_as(_FP), S3_out.ctypes.data_as(_FP), float(T),
+             int(n_sweep), int(ssf_every), int(ssf_slot), C.byref(e), C.byref(acc))
+        return e.value, acc.value
+
 
 def pyrochlore_system(L, J1=1.0, J2=0.0, J3=0.0, Delta=1.0, B=(0.0, 0.0, 0.0), T_ref=1.0, seed=0,
                       n_replicas=None, split_J1=True, overrelax_mode=0, colouring=0, generic=False,

@@ -281,3 +281,35 @@ def test_anneal_file_holds_finished_temperatures_while_running(tmp_path):
         sc = f["/ssf/static_corr"][:]
         np.testing.assert_array_equal(f["/ssf/T_list"][:], [0.2, 0.5, 1.0])
     assert (np.abs(sc).reshape(6, 3, -1).max(axis=2) > 0).all()
+
+
+@pytest.mark.parametrize("update", [0, 1])
+def test_step_host3_matches_step_host(update):
+    """pc_step_host3 (packed x, y, z host spins, unpacked and packed on the
+    device) against pc_step_host on the same spins: the same spins out, energy,
+    accepted moves and S(q) sums, over three consecutive steps. With lifted
+    Metropolis (update 1) the lifting directions stay on the device: the float4
+    path is fed its own output, directions included, and the chains agree."""
+    L, T = 8, 0.7
+    kw = dict(J1=1.0, J2=0.1, J3=0.05, B=(0.0, 0.0, 0.5), seed=37, schedule=1, update=update)
+    a = pc.pyrochlore_system(L, **kw)
+    b = pc.pyrochlore_system(L, **kw)
+    for s in (a, b):
+        s.ssf_configure(["xx", "zz", "xy"], 1)
+    a.random_spins(4)
+    S4 = np.ascontiguousarray(a.spins_f4())
+    b.set_spins_f4(S4)
+    S3 = np.ascontiguousarray(S4[:, :3])
+    for _ in range(3):
+        S3_out = np.zeros_like(S3)
+        S4_out = np.zeros_like(S4)
+        e3, acc3 = a.step_host3(S3, S3_out, T, 20, 8, 0)
+        e4, acc4 = b.step_host(S4, S4_out, T, 20, 8, 0)
+        np.testing.assert_array_equal(S3_out, S4_out[:, :3])
+        assert e3 == e4 and acc3 == acc4
+        S3, S4 = S3_out, S4_out
+    for x, y in zip(a.ssf_read(0), b.ssf_read(0)):
+        np.testing.assert_array_equal(np.asarray(x), np.asarray(y))
+    np.testing.assert_array_equal(a.spins_f4(), b.spins_f4())
+    with pytest.raises(ValueError):
+        a.step_host3(np.zeros((a.N(0), 4), np.float32), S3, T, 1)
