@@ -7,7 +7,7 @@ Deterministic (one configuration, no randomness in the comparison):
   configuration's couplings (1e-5 relative to the quantity's scale); one
   overrelaxation pass with given angles at L = 12, 16, 24, 64 (FP32 bound of
   the small-L test: 99.5 % of components within 1e-5, all within 2e-4); one
-  sweep site by site against the oracle's Philox mirror at L = 12, 16, 64 (at
+  sweep site by site against the oracle's Philox mirror at L = 12, 16, 24, 64 (at
   these sizes a handful of the 10^4..10^6 accept decisions sit within FP32
   rounding of their threshold and may flip, so: accepted counts within 1e-5 of
   the proposals, 99.9 % of spins within 1e-4).
@@ -123,7 +123,7 @@ def test_overrelax_pass_with_given_angles_at_config_sizes(L, c):
 
 
 @pytest.mark.parametrize("schedule", [0, 1])
-@pytest.mark.parametrize("L,c,T", [(12, CONFIG3, 0.3), (16, CONFIG2, 0.5), (64, CONFIG5, 0.5)])
+@pytest.mark.parametrize("L,c,T", [(12, CONFIG3, 0.3), (16, CONFIG2, 0.5), (24, CONFIG3, 0.05), (64, CONFIG5, 0.5)])
 def test_sweep_follows_oracle_mirror_at_config_sizes(L, c, T, schedule):
     seed = 4321
     g, o = _pair(L, c, seed=seed, schedule=schedule)
