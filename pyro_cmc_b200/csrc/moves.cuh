@@ -92,13 +92,13 @@ __device__ __forceinline__ bool overrelax_spin(float4 s0, float3 h, float sn, fl
     const float av = dot3_rn(h.x, h.y, h.z, s0.x, s0.y, s0.z);
     float nx, ny, nz;
     if (REFLECT) {
-        const float f = 2.f * av / (n2 + 1e-10f);
+        const float f = __fdividef(2.f * av, n2 + 1e-10f);
         nx = fmaf(f, h.x, -s0.x);
         ny = fmaf(f, h.y, -s0.y);
         nz = fmaf(f, h.z, -s0.z);
     } else {
         // cs s + f h + g (h x s)
-        const float f = (1.f - cs) * av / n2;
+        const float f = __fdividef((1.f - cs) * av, n2);
         const float g = sn * rsqrtf(n2);
         const float cx = fmaf(h.y, s0.z, -__fmul_rn(h.z, s0.y));
         const float cy = fmaf(h.z, s0.x, -__fmul_rn(h.x, s0.z));

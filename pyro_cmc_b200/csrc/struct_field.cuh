@@ -53,15 +53,16 @@ __device__ __forceinline__ float4 load_spin(const float4* p) {
 }
 
 // h += J t for a general 3x3 group matrix J (row-major), with every rounding
-// fixed: row a adds fma(J[3a+2], t.z, fma(J[3a+1], t.y, J[3a] t.x)) to h. Left
-// to the compiler, the contraction of the plain expression into FMAs may differ
-// between the kernels that inline it, and the chains of the per-pass,
+// fixed: h_a = fma(J[3a+2], t.z, fma(J[3a+1], t.y, fma(J[3a], t.x, h_a))).
+// Left to the compiler, the contraction of the plain expression into FMAs may
+// differ between the kernels that inline it, and the chains of the per-pass,
 // persistent, staged and cluster-resident sweeps would part at the first
-// decision the last bit changes.
+// decision the last bit changes. For J = j I the two outer terms add exact
+// zeros, so the result is fma(j, t_a, h_a): the bits of add_group_iso.
 __device__ __forceinline__ void add_matvec(float3& h, const float* J, const float3& t) {
-    h.x = __fadd_rn(h.x, fmaf(J[2], t.z, fmaf(J[1], t.y, __fmul_rn(J[0], t.x))));
-    h.y = __fadd_rn(h.y, fmaf(J[5], t.z, fmaf(J[4], t.y, __fmul_rn(J[3], t.x))));
-    h.z = __fadd_rn(h.z, fmaf(J[8], t.z, fmaf(J[7], t.y, __fmul_rn(J[6], t.x))));
+    h.x = fmaf(J[2], t.z, fmaf(J[1], t.y, fmaf(J[0], t.x, h.x)));
+    h.y = fmaf(J[5], t.z, fmaf(J[4], t.y, fmaf(J[3], t.x, h.y)));
+    h.z = fmaf(J[8], t.z, fmaf(J[7], t.y, fmaf(J[6], t.x, h.z)));
 }
 
 template <int SL, int E, bool NC = true>
@@ -99,18 +100,17 @@ __device__ __forceinline__ void add_group(float3& h, const float4* __restrict__ 
 
 // add_group for a group whose matrix is j I, j != 0 (every group of a system
 // with nonzero isotropic couplings: J2, J3, and J1 with Delta = 1): three
-// multiplies and three adds instead of nine multiply-adds and three adds, and
-// no test of the group's activity. add_group gives the same bits on such a
-// matrix: its two zero terms add exact zeros to the rounded j t, and the sum
-// is added to h unfused, as here.
+// multiply-adds instead of nine, and no test of the group's activity.
+// add_group gives the same bits on such a matrix (add_matvec: its two zero
+// terms add exact zeros to fma(j, t, h)).
 template <int SL, int G, bool NC = true>
 __device__ __forceinline__ void add_group_iso(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                               const PyroMats& mats) {
     const float3 t = group_sum<SL, G, NC>(S, Nc, c, std::make_integer_sequence<int, grp_size(SL, G)>{});
     const float j = mats.M[SL][G][0];
-    h.x = __fadd_rn(h.x, __fmul_rn(j, t.x));
-    h.y = __fadd_rn(h.y, __fmul_rn(j, t.y));
-    h.z = __fadd_rn(h.z, __fmul_rn(j, t.z));
+    h.x = fmaf(j, t.x, h.x);
+    h.y = fmaf(j, t.y, h.y);
+    h.z = fmaf(j, t.z, h.z);
 }
 
 __device__ __forceinline__ Coords cell_coords(int cell, int L, uint64_t divL) {
@@ -192,7 +192,7 @@ __host__ __device__ constexpr bool group_has_upper(int sl, int g) {
 }
 // ISO 1: every group matrix is j I with j != 0; ISO 2: so but the J2 group
 // (group 3), which is 0 and skipped (as add_group_iso: no activity test,
-// three multiplies and three unfused adds per group, the same bits).
+// three multiply-adds per group, the same bits).
 template <int SL, int G, int ISO, bool NC, int... K>
 __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restrict__ S, int Nc, const Coords& c,
                                                 const PyroMats& mats, std::integer_sequence<int, K...>) {
@@ -203,9 +203,9 @@ __device__ __forceinline__ void add_group_upper(float3& h, const float4* __restr
             (add_upper<SL, B + K, NC>(t, S, Nc, c), ...);
             const float* J = mats.M[SL][G];
             if constexpr (ISO) {
-                h.x = __fadd_rn(h.x, __fmul_rn(J[0], t.x));
-                h.y = __fadd_rn(h.y, __fmul_rn(J[0], t.y));
-                h.z = __fadd_rn(h.z, __fmul_rn(J[0], t.z));
+                h.x = fmaf(J[0], t.x, h.x);
+                h.y = fmaf(J[0], t.y, h.y);
+                h.z = fmaf(J[0], t.z, h.z);
             } else {
                 add_matvec(h, J, t);
             }
