@@ -34,10 +34,18 @@ constexpr int kVarIso = 5, kVarIsoNoJ2 = 6;
 // for a kernel that writes them in an earlier phase of the same launch (the
 // persistent tempering kernel, whose grid barrier orders the phases).
 constexpr int kVarCoherent = 0x100;
+// The per-replica constants of a Metropolis proposal at temperature T: the
+// kick width sqrt(T / T_ref) and 1 / T, rounded as the moves use them. Formed
+// once per replica whenever the temperatures change, not per site.
+__host__ __device__ inline float2 proposal_consts(double T, float inv_T_ref) {
+    return make_float2(sqrtf(float(T) * inv_T_ref), float(1.0 / T));
+}
+
 struct PassArgs {
     float4* spins;
     const ReplicaDev* reps;
     const double* T_rep;         // per-replica temperature (device)
+    const float2* Tq;            // per replica (sqrt(T / T_ref), 1 / T): proposal_consts of T_rep (device)
     const uint64_t* sweep_base;  // device sweep counter
     uint64_t sweep_offset;       // added to *sweep_base
     uint64_t seed;
@@ -236,6 +244,8 @@ struct PtArgs {
     int32_t* rep_of_slot;
     int32_t* slot_of_rep;
     double* T_rep;           // updated: T_rep[r] = T_slot[slot_of_rep[r]]
+    float2* Tq;              // updated with T_rep: proposal_consts(T_rep[r], inv_T_ref)
+    float inv_T_ref;
     const double* e_rep;     // energy per cell of each replica
     const ReplicaDev* reps;  // for Nc
     double* E_sum;           // per slot
@@ -248,6 +258,8 @@ struct PtArgs {
     int n_slots;
 };
 void launch_pt_exchange(const PtArgs& a, cudaStream_t st);
+// Tq[r] = proposal_consts(T[r], inv_T_ref) for r < R (sweep.cu).
+void launch_refresh_tq(const double* T, float2* q, int R, float inv_T_ref, cudaStream_t st);
 
 // Packed host spins (hostio.cu): (x, y, z) x n <-> the first three float4
 // components; unpacking keeps each spin's fourth component.

@@ -389,9 +389,9 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
     uint4 w = make_uint4(0, 0, 0, 0);
     float sigma = 0.f, invT = 0.f;
     if (kMet) {
-        const double T = kCoherent ? __ldca(a.T_rep + r) : a.T_rep[r];
-        sigma = sqrtf(float(T) * a.inv_T_ref);
-        invT = float(1.0 / T);
+        const float2 q = kCoherent ? __ldca(a.Tq + r) : a.Tq[r];
+        sigma = q.x;
+        invT = q.y;
         w = site_draw_rk(a.rkeys, uint32_t(r), sweep, kDrawMetropolis, uint32_t(i));
     }
     float sn = 0.f, cs = 1.f;

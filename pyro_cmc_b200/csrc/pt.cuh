@@ -53,6 +53,8 @@ __device__ __forceinline__ void pt_exchange_block(const PtArgs& a) {
                 a.slot_of_rep[rb] = s;
                 a.T_rep[ra] = Tb;
                 a.T_rep[rb] = Ta;
+                a.Tq[ra] = proposal_consts(Tb, a.inv_T_ref);
+                a.Tq[rb] = proposal_consts(Ta, a.inv_T_ref);
             }
         }
     }

@@ -366,6 +366,13 @@ void launch_random_spins(float4* spins, const ReplicaDev* reps, const Tile* tile
 }
 
 __global__ void advance_counter_kernel(uint64_t* c, uint64_t n) { *c += n; }
+
+__global__ void refresh_tq_kernel(const double* T, float2* q, int R, float inv_T_ref) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) q[r] = proposal_consts(T[r], inv_T_ref);
+}
+void launch_refresh_tq(const double* T, float2* q, int R, float inv_T_ref, cudaStream_t st) {
+    refresh_tq_kernel<<<(R + 255) / 256, 256, 0, st>>>(T, q, R, inv_T_ref);
+}
 void launch_advance_counter(uint64_t* counter, uint64_t n, cudaStream_t st) {
     advance_counter_kernel<<<1, 1, 0, st>>>(counter, n);
 }

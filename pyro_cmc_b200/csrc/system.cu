@@ -159,6 +159,7 @@ struct pc_system {
     DevBuf<ReplicaDev> d_reps;
     DevBuf<float4> d_spins;
     DevBuf<double> d_T;
+    DevBuf<float2> d_Tq;  // proposal_consts of d_T, refreshed before each batch of sweeps
     DevBuf<uint64_t> d_sweep;
     DevBuf<unsigned long long> d_acc;
     DevBuf<int> d_err;  // set by a kernel whose bounded wait ran out
@@ -275,6 +276,7 @@ struct pc_system {
         d_reps.release();
         d_spins.release();
         d_T.release();
+        d_Tq.release();
         d_sweep.release();
         d_acc.release();
         d_err.release();
@@ -645,6 +647,7 @@ pc::PassArgs pass_args(pc_system* s, int colour, uint64_t sweep_offset, int or_p
     a.spins = s->d_spins.p;
     a.reps = s->d_reps.p;
     a.T_rep = s->d_T.p;
+    a.Tq = s->d_Tq.p;
     a.sweep_base = s->d_sweep.p;
     a.sweep_offset = sweep_offset;
     a.seed = s->seed;
@@ -808,7 +811,20 @@ int launch_cluster(pc_system* s, int n_sweeps, int n_or) {
     return PC_OK;
 }
 
+// d_Tq from d_T (every writer of the temperatures but the exchange round,
+// which updates both, comes before a batch of sweeps)
+int refresh_tq(pc_system* s) {
+    pc::launch_refresh_tq(s->d_T.p, s->d_Tq.p, s->R, float(1.0 / s->T_ref), s->stream);
+    PC_LAUNCH_CK();
+    s->launches++;
+    return PC_OK;
+}
+
 int run_sweeps(pc_system* s, int n_sweeps, int n_or) {
+    if (n_sweeps > 0) {
+        const int rc = refresh_tq(s);
+        if (rc) return rc;
+    }
     if (s->cluster_sweep && !s->timing && n_sweeps > 0 && cluster_eligible(s, n_or)) {
         const int rc = launch_cluster(s, n_sweeps, n_or);
         if (rc) return rc;
@@ -975,6 +991,7 @@ int pc_create(int n_replicas, const int32_t* L, uint64_t seed, pc_system** out) 
     if (e == cudaSuccess) e = s->d_spins.alloc(size_t(s->N_tot));
     if (e == cudaSuccess) e = cudaMemset(s->d_spins.p, 0, sizeof(float4) * size_t(s->N_tot));
     if (e == cudaSuccess) e = s->d_T.alloc(size_t(n_replicas));
+    if (e == cudaSuccess) e = s->d_Tq.alloc(size_t(n_replicas));
     if (e == cudaSuccess) e = s->d_sweep.alloc(1);
     if (e == cudaSuccess) e = cudaMemset(s->d_sweep.p, 0, sizeof(uint64_t));
     if (e == cudaSuccess) e = s->d_acc.alloc(size_t(n_replicas));
@@ -1905,6 +1922,8 @@ pc::PtArgs pt_args(pc_system* s) {
     a.rep_of_slot = s->d_rep_of_slot.p;
     a.slot_of_rep = s->d_pt_slot_of_rep.p;
     a.T_rep = s->d_T.p;
+    a.Tq = s->d_Tq.p;
+    a.inv_T_ref = float(1.0 / s->T_ref);
     a.e_rep = s->d_e.p;
     a.reps = s->d_reps.p;
     a.E_sum = s->d_E_sum.p;
@@ -2062,6 +2081,8 @@ int pc_pt_run(pc_system* sys, int n_rounds, int n_sweep, int ssf_every) {
         }
     }
     PC_CK(cudaMemsetAsync(sys->d_acc.p, 0, sizeof(unsigned long long) * size_t(sys->R), sys->stream));
+    rc = refresh_tq(sys);
+    if (rc) return rc;
     if (sys->pt_persistent) {
         if (const char* why = pt_persistent_unsupported(sys)) return fail(PC_ERR_UNSUPPORTED, why);
         return run_pt_persistent(sys, n_rounds, n_sweep, ssf_every);
