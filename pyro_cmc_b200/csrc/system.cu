@@ -81,11 +81,17 @@ template <typename T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    // on failure the buffer stays empty (p null, n 0): a later size check
+    // allocates again instead of trusting a size that was never allocated
     cudaError_t alloc(size_t count) {
         release();
-        n = count;
         if (count == 0) return cudaSuccess;
-        return cudaMalloc(&p, count * sizeof(T));
+        const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess)
+            n = count;
+        else
+            p = nullptr;
+        return e;
     }
     void release() {
         if (p) cudaFree(p);

@@ -113,9 +113,15 @@ class _H5:
         size = int.from_bytes(m[p:p + w], "little")
         p += w
         blocks = [(a, p, p + size)]
+        seen = set()
         out = []
         while blocks:
             start, p, end = blocks.pop(0)
+            if start in seen:
+                raise ValueError(f"object header at {addr}: continuation blocks form a cycle")
+            seen.add(start)
+            if end + 4 > len(m):
+                raise ValueError(f"object header at {addr}: runs past the end of the file")
             (ck,) = struct.unpack_from("<I", m, end)
             if lookup3(m[start:end]) != ck:
                 raise ValueError(f"object header at {start - self._base}: checksum mismatch")
