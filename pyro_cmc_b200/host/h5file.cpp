@@ -295,11 +295,14 @@ void H5File::strings(const std::string& path, const std::vector<std::string>& s)
     put8(g, 0);
     put64(g, size);
     g.insert(g.end(), objs.begin(), objs.end());
-    // object 0: the free space, its size counting its own 16-byte header
+    // object 0: the free space from its own 16-byte header to the end of the
+    // collection, header included (a reader steps from the header's start to
+    // the collection's end by this size)
+    const uint64_t free_bytes = size - g.size();
     put16(g, 0);
     put16(g, 0);
     put32(g, 0);
-    put64(g, size - g.size());
+    put64(g, free_bytes);
     g.resize(size, 0);
     const uint64_t gaddr = append(g);
     Bytes el;

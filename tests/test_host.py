@@ -121,6 +121,11 @@ def test_hdf5_bytes_follow_the_published_format(tmp_path):
         assert raw[gcol:gcol + 8] == b"GCOL" + bytes([1, 0, 0, 0])
         assert struct.unpack_from("<Q", raw, gcol + 8)[0] == 4096
         assert h5._heap(gcol) == {1: b"xx", 2: b"yz", 3: b"z"}
+        # the free-space object (index 0) spans from its header to the end of the
+        # collection, header included: 16 + 3 objects of 16 + 8 bytes before it
+        free = gcol + 16 + 3 * 24
+        idx, _ref, _r, fsize = struct.unpack_from("<HHIQ", raw, free)
+        assert idx == 0 and fsize == 4096 - (free - gcol)
     finally:
         h5.close()
 
