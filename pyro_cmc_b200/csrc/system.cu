@@ -2318,6 +2318,10 @@ int pc_autotune(pc_system* sys) {
     uint64_t sweep0 = 0;
     PC_CK(cudaMemcpyAsync(&sweep0, sys->d_sweep.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, sys->stream));
     PC_CK(cudaStreamSynchronize(sys->stream));
+    // the timing runs sweep at T = 1; the temperatures (a tempering ladder's
+    // current assignment included) are put back afterwards, like the spins
+    std::vector<double> T_saved(size_t(sys->R));
+    PC_CK(cudaMemcpy(T_saved.data(), sys->d_T.p, sizeof(double) * T_saved.size(), cudaMemcpyDeviceToHost));
     std::vector<double> T(size_t(sys->R), 1.0);
     PC_CK(cudaMemcpy(sys->d_T.p, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
     // candidates: neighbour-load variant x threads per CTA x resident CTAs per
@@ -2416,6 +2420,7 @@ int pc_autotune(pc_system* sys) {
     PC_CK(cudaMemcpyAsync(sys->d_spins.p, saved.p, bytes, cudaMemcpyDeviceToDevice, sys->stream));
     PC_CK(cudaMemcpyAsync(sys->d_sweep.p, &sweep0, sizeof(uint64_t), cudaMemcpyHostToDevice, sys->stream));
     PC_CK(cudaStreamSynchronize(sys->stream));
+    PC_CK(cudaMemcpy(sys->d_T.p, T_saved.data(), sizeof(double) * T_saved.size(), cudaMemcpyHostToDevice));
     sys->host_sweep = sweep0;
     saved.release();
     return PC_OK;

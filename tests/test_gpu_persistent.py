@@ -156,3 +156,23 @@ def test_persistent_rounds_at_the_batched_workload():
         L = sorted(Ls)[slot]
         for x, y in zip(a.ssf_read(slot, L), b.ssf_read(slot, L)):
             np.testing.assert_array_equal(np.asarray(x), np.asarray(y))
+
+
+def test_autotune_after_configure_keeps_the_ladder():
+    """pc_autotune times its candidates at T = 1 on the system itself; it puts
+    back the spins, the sweep counter and the temperatures (the ladder's
+    current assignment), so a tempering run autotuned after pc_pt_configure
+    is the chain of the same run without autotuning (the chain does not
+    depend on the tile the autotuner picks)."""
+    c = CASES[0]
+    runs = []
+    for tune in (False, True):
+        s = pc.pyrochlore_system(LS, seed=21, schedule=1, **c)
+        s.random_spins(21)
+        s.pt_configure(TS)
+        s.pt_run(1, 2)
+        if tune:
+            s.autotune()
+        s.pt_run(3, 2)
+        runs.append(s)
+    _same_chain(runs[0], runs[1], len(LS))
