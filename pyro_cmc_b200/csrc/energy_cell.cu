@@ -17,10 +17,14 @@
 // gathers its neighbours on higher sublattices. Consecutive threads take
 // consecutive cells along x, so every load of a warp is a 512-byte row segment.
 //
-// Bond energies accumulate in FP32 (four sums per cell, as the per-site
-// local field of the other kernels is FP32), the field and magnetisation
-// terms and everything above the cell in FP64; per-CTA FP64 partials are summed per replica
-// in fixed order by energy_finalize_kernel (deterministic).
+// Bond energies accumulate in FP32 (as the per-site local field of the other
+// kernels is FP32): four sums per cell, each bond's S_i.S_j times its j; or,
+// when every group's j is the same on all 16 sublattices (`uniform`: the
+// pyrochlore J1-J2-J3 model with isotropic couplings), one sum of bare
+// S_i.S_j per group (three multiply-adds a bond), multiplied by the group's j
+// once per cell. The Zeeman and magnetisation terms use the cell's summed
+// spin; everything above the cell is FP64, and per-CTA FP64 partials are
+// summed per replica in fixed order by energy_finalize_kernel (deterministic).
 #include <cuda_runtime.h>
 
 #include <utility>
@@ -124,38 +128,43 @@ __host__ __device__ constexpr int cb_tb(int t) { return kCB.tb[t]; }
 __host__ __device__ constexpr int cb_rsl(int k) { return kCB.rsl[k]; }
 __host__ __device__ constexpr int cb_rg(int k) { return kCB.rg[k]; }
 
-// Bond energies accumulate in kAcc FP32 sums per cell (site sl into sum
-// sl % kAcc): fewer live registers than one sum per site.
-constexpr int kAcc = 4;
+// Bond energies accumulate in kAcc FP32 sums per cell: site sl into sum
+// sl % 4 (fewer live registers than one sum per site), or group G into sum G
+// (UNI).
+constexpr int kAcc = kGroups;
+static_assert(kAcc >= 4, "per-site sums use four accumulators");
 
-// acc += S_SL . M[SL][G] n  (ISO: M = j I; ISO 2: the J2 group is zero and skipped)
-template <int SL, int G, int ISO>
+// acc += S_SL . M[SL][G] n  (ISO: M = j I; ISO 2: the J2 group is zero and
+// skipped); UNI: acc[G] += S_SL . n, the group's j applied per cell
+template <int SL, int G, int ISO, bool UNI>
 __device__ __forceinline__ void bond_term(float (&acc)[kAcc], const float3 (&own)[16], const float3& n,
                                           const PyroMats& mats) {
     if constexpr (ISO == 2 && G == 3) {
         return;
+    } else if constexpr (UNI) {
+        acc[G] = fmaf(own[SL].z, n.z, fmaf(own[SL].y, n.y, fmaf(own[SL].x, n.x, acc[G])));
     } else if constexpr (ISO != 0) {
         const float d = own[SL].x * n.x + own[SL].y * n.y + own[SL].z * n.z;
-        acc[SL % kAcc] = fmaf(mats.M[SL][G][0], d, acc[SL % kAcc]);
+        acc[SL % 4] = fmaf(mats.M[SL][G][0], d, acc[SL % 4]);
     } else {
         const float* J = mats.M[SL][G];
         const float tx = J[0] * n.x + J[1] * n.y + J[2] * n.z;
         const float ty = J[3] * n.x + J[4] * n.y + J[5] * n.z;
         const float tz = J[6] * n.x + J[7] * n.y + J[8] * n.z;
-        acc[SL % kAcc] += own[SL].x * tx + own[SL].y * ty + own[SL].z * tz;
+        acc[SL % 4] += own[SL].x * tx + own[SL].y * ty + own[SL].z * tz;
     }
 }
 
-template <int ISO, int... K>
+template <int ISO, bool UNI, int... K>
 __device__ __forceinline__ void intra_bonds(float (&acc)[kAcc], const float3 (&own)[16], const PyroMats& mats,
                                             std::integer_sequence<int, K...>) {
-    (bond_term<cb_isl(K), cb_ig(K), ISO>(acc, own, own[cb_is2(K)], mats), ...);
+    (bond_term<cb_isl(K), cb_ig(K), ISO, UNI>(acc, own, own[cb_is2(K)], mats), ...);
 }
 
-template <int T, int ISO, int... K>
+template <int T, int ISO, bool UNI, int... K>
 __device__ __forceinline__ void target_bonds(float (&acc)[kAcc], const float3 (&own)[16], const float3& n,
                                              const PyroMats& mats, std::integer_sequence<int, K...>) {
-    (bond_term<cb_rsl(cb_tb(T) + K), cb_rg(cb_tb(T) + K), ISO>(acc, own, n, mats), ...);
+    (bond_term<cb_rsl(cb_tb(T) + K), cb_rg(cb_tb(T) + K), ISO, UNI>(acc, own, n, mats), ...);
 }
 
 template <int T>
@@ -167,12 +176,12 @@ __device__ __forceinline__ float3 load_target(const char* base, uint32_t sl_byte
 }
 
 // Targets [T0, T0 + sizeof...(K)) loaded together (one round trip), then their bonds.
-template <int T0, int ISO, int... K>
+template <int T0, int ISO, bool UNI, int... K>
 __device__ __forceinline__ void target_batch(float (&acc)[kAcc], const float3 (&own)[16], const char* base,
                                              uint32_t sl_bytes, const Coords& c, const PyroMats& mats,
                                              std::integer_sequence<int, K...>) {
     const float3 n[sizeof...(K)] = {load_target<T0 + K>(base, sl_bytes, c)...};
-    (target_bonds<T0 + K, ISO>(acc, own, n[K], mats,
+    (target_bonds<T0 + K, ISO, UNI>(acc, own, n[K], mats,
                                std::make_integer_sequence<int, cb_tb(T0 + K + 1) - cb_tb(T0 + K)>{}),
      ...);
 }
@@ -183,13 +192,13 @@ __device__ __forceinline__ void target_batch(float (&acc)[kAcc], const float3 (&
 // hide more of the gather latency than the spills cost (same sums either way).
 constexpr int kTargetBatch = 4;
 
-template <int T0, int ISO>
+template <int T0, int ISO, bool UNI>
 __device__ __forceinline__ void remote_bonds(float (&acc)[kAcc], const float3 (&own)[16], const char* base,
                                              uint32_t sl_bytes, const Coords& c, const PyroMats& mats) {
     if constexpr (T0 < cb_n_tgt()) {
         constexpr int n = (cb_n_tgt() - T0) < kTargetBatch ? (cb_n_tgt() - T0) : kTargetBatch;
-        target_batch<T0, ISO>(acc, own, base, sl_bytes, c, mats, std::make_integer_sequence<int, n>{});
-        remote_bonds<T0 + n, ISO>(acc, own, base, sl_bytes, c, mats);
+        target_batch<T0, ISO, UNI>(acc, own, base, sl_bytes, c, mats, std::make_integer_sequence<int, n>{});
+        remote_bonds<T0 + n, ISO, UNI>(acc, own, base, sl_bytes, c, mats);
     }
 }
 
@@ -201,7 +210,7 @@ __device__ __forceinline__ void load_own(float3 (&own)[16], const char* base, ui
     ((own[SL] = make_float3(v[SL].x, v[SL].y, v[SL].z)), ...);
 }
 
-template <int ISO>
+template <int ISO, bool UNI>
 __global__ void __launch_bounds__(kEnergyCellThreads, 5) energy_cell_kernel(const __grid_constant__ EnergyCellArgs a) {
     __shared__ double red[4 * 32];
     const int4 tile = a.tiles[blockIdx.x];  // (replica, first cell, cells, -)
@@ -217,17 +226,21 @@ __global__ void __launch_bounds__(kEnergyCellThreads, 5) energy_cell_kernel(cons
         float acc[kAcc];
 #pragma unroll
         for (int k = 0; k < kAcc; ++k) acc[k] = 0.f;
-        intra_bonds<ISO>(acc, own, a.mats, std::make_integer_sequence<int, cb_n_intra()>{});
-        remote_bonds<0, ISO>(acc, own, base, sl_bytes, c, a.mats);
+        intra_bonds<ISO, UNI>(acc, own, a.mats, std::make_integer_sequence<int, cb_n_intra()>{});
+        remote_bonds<0, ISO, UNI>(acc, own, base, sl_bytes, c, a.mats);
 #pragma unroll
-        for (int k = 0; k < kAcc; ++k) v[0] += double(acc[k]);
+        for (int k = 0; k < (UNI ? kAcc : 4); ++k) v[0] += UNI ? double(a.mats.M[0][k][0]) * double(acc[k]) : double(acc[k]);
+        float3 m = own[0];
 #pragma unroll
-        for (int sl = 0; sl < 16; ++sl) {
-            v[0] -= double(own[sl].x * a.B[0] + own[sl].y * a.B[1] + own[sl].z * a.B[2]);
-            v[1] += double(own[sl].x);
-            v[2] += double(own[sl].y);
-            v[3] += double(own[sl].z);
+        for (int sl = 1; sl < 16; ++sl) {
+            m.x += own[sl].x;
+            m.y += own[sl].y;
+            m.z += own[sl].z;
         }
+        v[0] -= double(fmaf(m.z, a.B[2], fmaf(m.y, a.B[1], m.x * a.B[0])));
+        v[1] = double(m.x);
+        v[2] = double(m.y);
+        v[3] = double(m.z);
     }
     // block-wide FP64 sum: warp shuffles, then one warp over the warp sums
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -251,12 +264,17 @@ __global__ void __launch_bounds__(kEnergyCellThreads, 5) energy_cell_kernel(cons
 
 void launch_energy_cells(const EnergyCellArgs& a, cudaStream_t st) {
     if (a.n_tiles <= 0) return;
-    if (a.iso == 1)
-        energy_cell_kernel<1><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+    const bool uni = a.uniform != 0;
+    if (a.iso == 1 && uni)
+        energy_cell_kernel<1, true><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+    else if (a.iso == 2 && uni)
+        energy_cell_kernel<2, true><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+    else if (a.iso == 1)
+        energy_cell_kernel<1, false><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
     else if (a.iso == 2)
-        energy_cell_kernel<2><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+        energy_cell_kernel<2, false><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
     else
-        energy_cell_kernel<0><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
+        energy_cell_kernel<0, false><<<a.n_tiles, kEnergyCellThreads, 0, st>>>(a);
 }
 
 }  // namespace pc

@@ -142,6 +142,7 @@ struct EnergyCellArgs {
     float B[3];
     double* partial;
     int iso;  // as EnergyArgs::iso
+    int uniform;  // iso != 0 and every group's j the same on all 16 sublattices: per-group bond sums
     PyroMats mats;
 };
 void launch_energy_cells(const EnergyCellArgs& a, cudaStream_t st);

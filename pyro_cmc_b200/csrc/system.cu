@@ -195,6 +195,7 @@ struct pc_system {
     // work items of up to kGradK tiles of one (replica, sublattice)
     bool grad_struct = false;
     int iso_kind = 0;  // 1: every group matrix j I, j != 0; 2: so but a zero J2 group (isotropic variants)
+    bool iso_uniform = false;  // iso_kind != 0 and each group's j the same on every sublattice
     uint32_t spec_mask[16][pc::kGroups][2] = {};
     DevBuf<int4> d_grad_items;
     int n_grad_items = 0;
@@ -489,6 +490,10 @@ void build_struct(pc_system* s) {
     for (int g = 0; g < pc::kGroups; ++g)
         if (g != 3) others = others && iso_nz[g];
     s->iso_kind = !s->structured ? 0 : (others && iso_nz[3]) ? 1 : (others && zero[3]) ? 2 : 0;
+    s->iso_uniform = s->iso_kind != 0;
+    for (int sl = 1; sl < 16; ++sl)
+        for (int g = 0; g < pc::kGroups; ++g)
+            if (s->mats.M[sl][g][0] != s->mats.M[0][g][0]) s->iso_uniform = false;
 }
 
 // Colour classes from the active bonds: sublattices joined by a nonzero bond
@@ -872,6 +877,7 @@ int enqueue_energy(pc_system* s) {
         for (int i = 0; i < 3; ++i) c.B[i] = float(s->B[i]);
         c.partial = s->d_cell_partial.p;
         c.iso = s->iso_kind;
+        c.uniform = s->iso_uniform ? 1 : 0;
         c.mats = s->mats;
         pc::launch_energy_cells(c, s->stream);
         PC_LAUNCH_CK();

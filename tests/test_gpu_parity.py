@@ -87,6 +87,40 @@ def test_energy_and_local_field(L, ci, generic):
         assert err <= REL, (name, err)
 
 
+@pytest.mark.parametrize("L", [1, 2, 4])
+@pytest.mark.parametrize("J2", [-0.1, 0.0])
+@pytest.mark.parametrize("uniform", [True, False])
+def test_isotropic_energy_per_group_and_per_bond_sums(L, J2, uniform):
+    """Isotropic couplings: with each group's j the same on every sublattice
+    the per-cell energy sums bare S_i.S_j per group and applies j once per
+    cell; with one J1 pair's j changed (1.3 on pyrochlore sublattices 0-1) it
+    applies each bond's j. Both (and J2 = 0, whose group is skipped) against
+    the FP64 sum over the oracle's neighbour tables with the same matrices."""
+    c = dict(J1=1.0, J2=J2, J3=0.05, Delta=1.0, B=(0.1, 0.0, 0.3))
+    g, o = pair(L, c)
+    mats = [o.spec_matrix(k) for k in range(o.num_specs())]
+    if not uniform:
+        mats[0] = 1.3 * np.eye(3)
+        g.set_coupling_matrix(0, mats[0])
+    assert g.structured()
+    rng = np.random.default_rng(7 * L + (J2 != 0) + 2 * uniform)
+    for name, S in states(o, rng).items():
+        g.set_spins(S)
+        S32 = g.spins().astype(np.float64)
+        h = np.zeros_like(S32)
+        for k, M in enumerate(mats):
+            nb = o.neighbours(k)
+            for col in range(nb.shape[1]):
+                idx = nb[:, col]
+                ok = idx >= 0
+                h[ok] += S32[idx[ok]] @ M.T
+        e_ref = (0.5 * np.sum(S32 * h) - np.sum(S32 @ np.array(c["B"]))) / L**3
+        e, m = g.energy()
+        scale = 16 * (6 * 1.3 + 12 * abs(J2) + 12 * 0.05 + 1)
+        assert abs(e[0] - e_ref) <= REL * scale, (name, e[0], e_ref)
+        np.testing.assert_allclose(m[0], S32.sum(axis=0), atol=1e-6 * o.N)
+
+
 def test_ferromagnet_energy_known_answer():
     c = dict(J1=1.3, J2=-0.4, J3=0.25, Delta=1.0, B=(0.1, -0.2, 0.7))
     g = pc.pyrochlore_system(4, **c)
