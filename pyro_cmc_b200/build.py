@@ -11,7 +11,8 @@ LIB = os.path.join(HERE, "libpyrocmc.so")
 SOURCES = ["system.cu", "sweep.cu", "sweep_lifted.cu", "sweep_staged.cu", "sweep_cluster.cu", "grad.cu", "ssf.cu",
            "pt.cu", "pt_persistent.cu", "noalloc.cu", "lt.cu", "merge.cu", "energy_cell.cu",
            "hostio.cu"]
-HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh", "struct_field.cuh", "moves.cuh", "dft.cuh", "pt.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "pyro_struct.cuh", "struct_field.cuh", "moves.cuh", "dft.cuh", "pt.cuh",
+           "energy_cell.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -287,13 +287,13 @@ struct PersistArgs {
     int n_rounds, n_sweep;
     int exchange;       // 1: energy + exchange after each round's sweeps
     uint64_t* sweep;    // device sweep counter: read at entry, advanced by n_rounds * n_sweep at exit
-    // energy (one thread per site, bonds to higher sublattices, each bond once)
-    const Tile* e_tiles;
-    const int32_t* e_order;
-    int n_e_tiles;
-    double* partial;  // [n_e_tiles][4]
-    const int32_t* tile_begin;
-    const int32_t* tile_end;
+    // energy: one thread per cubic cell (cell_energy), tiles as EnergyCellArgs
+    const int4* c_tiles;
+    int n_c_tiles;
+    int uniform;      // as EnergyCellArgs::uniform
+    double* partial;  // [n_c_tiles][4]
+    const int32_t* c_begin;  // replica r's cell tiles: [c_begin[r], c_end[r])
+    const int32_t* c_end;
     double* e;    // per replica energy per cell
     double* mag;  // per replica sum of S
     int R;

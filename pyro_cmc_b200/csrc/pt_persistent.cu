@@ -13,11 +13,11 @@
 // with ordinary loads ordered by the barrier's fences (kVarCoherent), never
 // through the read-only path.
 //
-// The energy phase counts every bond once from its lower-sublattice end (one
-// thread per site, struct_field_upper) into per-tile FP64 partials, the next
-// phase sums each replica's partials in a fixed order (deterministic), and
-// block 0 runs the exchange round (pt_exchange_block, as the stand-alone
-// exchange kernel does).
+// The energy phase runs the per-cell energy of the stand-alone kernel
+// (cell_energy, energy_cell.cuh: one thread per cubic cell, every bond once)
+// with coherent loads into per-tile FP64 partials, the next phase sums each
+// replica's partials in a fixed order (deterministic), and block 0 runs the
+// exchange round (pt_exchange_block, as the stand-alone exchange kernel does).
 //
 // Every barrier wait is bounded (max_polls polls of ~64 ns): when one runs out
 // the block sets *err = kErrGridBarrier, every block leaves at its next
@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "energy_cell.cuh"
 #include "kernels.h"
 #include "moves.cuh"
 #include "pt.cuh"
@@ -137,27 +138,21 @@ __device__ __forceinline__ void persist_pass(const PersistArgs& p, int colour, u
     }
 }
 
-template <int ISO>
+// One thread per cubic cell (cell_energy with coherent loads) over the cell
+// tiles of the stand-alone energy kernel (kEnergyCellThreads cells each); a
+// block narrower than a tile takes its cells in turns.
+template <int ISO, bool UNI>
 __device__ __forceinline__ void persist_energy(const PersistArgs& p, double* red) {
-    const float* B = p.pass.B;
-    for (int u = blockIdx.x; u < p.n_e_tiles; u += gridDim.x) {
-        const int t = p.e_order[u];
-        const Tile tile = p.e_tiles[t];
-        const int r = tile.x, sl = tile.y & 0xff;
-        const ReplicaDev rep = p.pass.reps[r];
-        const float4* S = p.pass.spins + rep.off;
+    for (int t = blockIdx.x; t < p.n_c_tiles; t += gridDim.x) {
+        const int4 tile = p.c_tiles[t];  // (replica, first cell, cells, -)
+        const ReplicaDev rep = p.pass.reps[tile.x];
         double v[4] = {0.0, 0.0, 0.0, 0.0};
-        if (int(threadIdx.x) < tile.w) {
-            const int cell = tile.z + int(threadIdx.x);
-            const float4 s0 = __ldcg(S + size_t(sl) * rep.Nc + cell);
-            float3 h = make_float3(0.f, 0.f, 0.f);
-#define PC_CALL(K) h = struct_field_upper<K, ISO, false>(S, p.pass.mats, cell, rep.L, rep.Nc, rep.divL)
-            PC_SL_SWITCH(sl, PC_CALL)
-#undef PC_CALL
-            v[0] = double(s0.x * h.x + s0.y * h.y + s0.z * h.z) - double(s0.x * B[0] + s0.y * B[1] + s0.z * B[2]);
-            v[1] = s0.x;
-            v[2] = s0.y;
-            v[3] = s0.z;
+        for (int k = int(threadIdx.x); k < tile.z; k += int(blockDim.x)) {
+            double w[4] = {0.0, 0.0, 0.0, 0.0};
+            const Coords c = cell_coords(tile.y + k, rep.L, rep.divL);
+            cell_energy<ISO, UNI, false>(w, reinterpret_cast<const char*>(p.pass.spins + rep.off),
+                                         uint32_t(rep.Nc) << 4, c, p.pass.mats, p.pass.B);
+            for (int j = 0; j < 4; ++j) v[j] += w[j];
         }
         block_sum4(v, red);
         if (threadIdx.x == 0)
@@ -171,7 +166,7 @@ __device__ __forceinline__ void persist_finalize(const PersistArgs& p, double* r
     const double2* p2 = reinterpret_cast<const double2*>(p.partial);
     for (int r = blockIdx.x; r < p.R; r += gridDim.x) {
         double v[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int t = p.tile_begin[r] + int(threadIdx.x); t < p.tile_end[r]; t += blockDim.x) {
+        for (int t = p.c_begin[r] + int(threadIdx.x); t < p.c_end[r]; t += blockDim.x) {
             const double2 q0 = __ldcg(p2 + 2 * size_t(t)), q1 = __ldcg(p2 + 2 * size_t(t) + 1);
             v[0] += q0.x;
             v[1] += q0.y;
@@ -192,8 +187,16 @@ __host__ __device__ constexpr int persist_var() {
     return (ISO == 1 ? kVarIso : ISO == 2 ? kVarIsoNoJ2 : 0) | kVarCoherent;
 }
 
+// Registers per thread: what the colour passes alone compile to. The per-cell
+// energy phase would take up to 255 and with them fewer resident blocks for
+// every pass; capped, it spills to L1 instead (it runs once per round).
 template <int FUSED, int ISO>
-__global__ void __launch_bounds__(256) pt_persistent_kernel(const __grid_constant__ PersistArgs p) {
+__host__ __device__ constexpr int persist_max_regs() {
+    return FUSED ? (ISO == 2 ? 80 : ISO == 1 ? 64 : 56) : (ISO == 0 ? 64 : 80);
+}
+
+template <int FUSED, int ISO>
+__global__ void __maxnreg__((persist_max_regs<FUSED, ISO>())) pt_persistent_kernel(const __grid_constant__ PersistArgs p) {
     __shared__ unsigned int warp_acc[8];
     __shared__ double red[4 * 32];
     constexpr int VAR = persist_var<ISO>();
@@ -221,7 +224,14 @@ __global__ void __launch_bounds__(256) pt_persistent_kernel(const __grid_constan
             }
         }
         if (ok && p.exchange) {
-            persist_energy<ISO>(p, red);
+            if constexpr (ISO != 0) {
+                if (p.uniform)
+                    persist_energy<ISO, true>(p, red);
+                else
+                    persist_energy<ISO, false>(p, red);
+            } else {
+                persist_energy<0, false>(p, red);
+            }
             ok = grid_barrier(p);
             if (ok) {
                 persist_finalize(p, red);

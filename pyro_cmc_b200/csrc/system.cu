@@ -2016,12 +2016,12 @@ int launch_persistent(pc_system* s, int n_rounds, int n_sweep, int exchange) {
     p.n_sweep = n_sweep;
     p.exchange = exchange;
     p.sweep = s->d_sweep.p;
-    p.e_tiles = s->d_all_tiles.p;
-    p.e_order = s->d_all_order.p;
-    p.n_e_tiles = s->n_all_tiles;
-    p.partial = s->d_partial.p;
-    p.tile_begin = s->d_tile_begin.p;
-    p.tile_end = s->d_tile_end.p;
+    p.c_tiles = s->d_cell_tiles.p;
+    p.n_c_tiles = s->n_cell_tiles;
+    p.uniform = s->iso_uniform ? 1 : 0;
+    p.partial = s->d_cell_partial.p;
+    p.c_begin = s->d_cell_begin.p;
+    p.c_end = s->d_cell_end.p;
     p.e = s->d_e.p;
     p.mag = s->d_mag.p;
     p.R = s->R;

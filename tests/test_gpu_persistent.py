@@ -3,9 +3,9 @@ against the per-pass graph schedule of the same rounds: uneven-L ladders
 (src/temper.cpp:418-474 per ladder), both sweep schedules, the three coupling
 kinds the structured kernels distinguish (all isotropic; isotropic with J2 = 0;
 XXZ J1). The site updates and draws are the same, so the spins, the slot
-assignment and the exchange statistics are identical; the energy samples agree
-to the rounding of their FP32 bond sums (one thread per site here, one per
-cubic cell in the per-pass energy), 1e-5 relative. Then: S(q) samples taken
+assignment and the exchange statistics are identical; the energy samples
+(the same per-cell sums, the per-replica FP64 sums in another order) agree to
+1e-5 relative. Then: S(q) samples taken
 between the launches, the sweep and round counters carried on by the per-pass
 path, and the bounded grid-barrier wait running out (PC_ERR_TIMEOUT) with the
 system usable afterwards."""
