@@ -82,6 +82,11 @@ int pc_define_coupling(pc_system* sys, const char* name, const int64_t* rel_vecs
  * rebuilding the bond tables (and colour classes, which follow the nonzero
  * bonds). Used by the differentiable path to move J. */
 int pc_set_coupling_matrix(pc_system* sys, int spec, const double* J);
+/* The same for n couplings at once: specs[k] gets J[9k .. 9k + 8], and the
+ * tables are rebuilt once; nothing is rebuilt when every matrix already
+ * holds those values. PC_ERR_INVALID (nothing changed) for an index out of
+ * range. */
+int pc_set_coupling_matrices(pc_system* sys, int n, const int32_t* specs, const double* J);
 /* MC_runner::set_global_field / get_global_field (include/MC.hpp:126-127). */
 int pc_set_global_field(pc_system* sys, const double* B3);
 int pc_get_global_field(pc_system* sys, double* B3);

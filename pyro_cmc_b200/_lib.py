@@ -36,6 +36,7 @@ _SIGNATURES = {
     "pc_set_seed": (_I, [_P, _U64]),
     "pc_define_coupling": (_I, [_P, C.c_char_p, _I64P, _I32P, _DP]),
     "pc_set_coupling_matrix": (_I, [_P, _I, _DP]),
+    "pc_set_coupling_matrices": (_I, [_P, _I, _IP, _DP]),
     "pc_set_global_field": (_I, [_P, _DP]),
     "pc_get_global_field": (_I, [_P, _DP]),
     "pc_set_T_ref": (_I, [_P, _D]),

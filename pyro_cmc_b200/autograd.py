@@ -39,13 +39,21 @@ def spins_tensor(system: System) -> torch.Tensor:
     return torch.as_tensor(_DeviceArray(ptr, (system.N_total, 4), "<f4"), device="cuda")
 
 
+def _order(system: System):
+    """Orders the system's next calls after the work queued on the current
+    torch stream: nothing to do when the system runs on that stream
+    (System.set_stream), else the host waits for the stream."""
+    if getattr(system, "stream_ptr", None) != torch.cuda.current_stream().cuda_stream:
+        torch.cuda.current_stream().synchronize()
+
+
 def _load(system: System, spins: torch.Tensor):
     if spins.shape != (system.N_total, 4) or spins.dtype != torch.float32 or not spins.is_cuda:
         raise ValueError("spins must be a float32 CUDA tensor of shape [N_total, 4]")
     dst = spins_tensor(system)
     if spins.data_ptr() != dst.data_ptr():
         dst.copy_(spins.detach())
-        torch.cuda.current_stream().synchronize()
+        _order(system)
 
 
 def _apply_params(system: System, params: torch.Tensor):
@@ -56,17 +64,14 @@ def _apply_params(system: System, params: torch.Tensor):
     J1, J2, J3, bx, by, bz = [float(x) for x in params.detach().cpu().tolist()]
     if (J1, J2, J3) != (pp["J1"], pp["J2"], pp["J3"]):
         I3 = np.eye(3)
-        k = 0
+        mats = []
         if pp["split_J1"]:
             for mu, nu in PAIRS:
-                system.set_coupling_matrix(k, J1 * (I3 + (pp["Delta"] - 1.0) * np.outer(local_axis(mu), local_axis(nu))))
-                k += 1
+                mats.append(J1 * (I3 + (pp["Delta"] - 1.0) * np.outer(local_axis(mu), local_axis(nu))))
         else:
-            system.set_coupling_matrix(k, J1 * I3)
-            k += 1
-        for j in (J2, J3, J3):
-            system.set_coupling_matrix(k, j * I3)
-            k += 1
+            mats.append(J1 * I3)
+        mats += [J2 * I3, J3 * I3, J3 * I3]
+        system.set_coupling_matrices(range(len(mats)), mats)  # one rebuild of the tables
         pp.update(J1=J1, J2=J2, J3=J3)
     system.set_global_field([bx, by, bz])
 
@@ -126,7 +131,7 @@ class SSFFunction(torch.autograd.Function):
         _load(system, spins)
         nk = system.Nc(0)
         out = torch.empty((system.R, system.n_corr, nk, 2), dtype=torch.float64, device=spins.device)
-        torch.cuda.current_stream().synchronize()
+        _order(system)
         system.ssf_forward_device(out.data_ptr())
         ctx.system = system
         ctx.save_for_backward(spins)
@@ -139,7 +144,7 @@ class SSFFunction(torch.autograd.Function):
         _load(system, spins)
         go = grad_out.detach().to(torch.float64).contiguous()
         grad_spins = torch.empty_like(spins)
-        torch.cuda.current_stream().synchronize()
+        _order(system)
         system.ssf_backward_device(go.data_ptr(), grad_spins.data_ptr())
         return grad_spins, None
 
@@ -154,7 +159,7 @@ def _field_of(system: System, field: torch.Tensor, couplings: bool):
     spec's bonds of field_src field_tgt^T (pc_energy_grad_field with g = Nc)."""
     field = field.detach().contiguous()
     out = torch.empty_like(field)
-    torch.cuda.current_stream().synchronize()
+    _order(system)
     _, P, _ = system.energy_grad_field(field.data_ptr(), _nc_vector(system), out.data_ptr(), couplings=couplings)
     return out, P
 
@@ -248,7 +253,7 @@ def gradient_quench(system: System, steps: int = 500, lr: float = 0.05) -> np.nd
         new = spins[:, :3] - lr * t[:, :3]
         new = new / new.norm(dim=1, keepdim=True)
         spins[:, :3] = new
-        torch.cuda.current_stream().synchronize()
+        _order(system)
     e, _ = system.energy()
     hist.append(e)
     return np.array(hist)

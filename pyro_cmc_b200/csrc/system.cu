@@ -1070,13 +1070,27 @@ int pc_define_coupling(pc_system* sys, const char* name, const int64_t* rel_vecs
 }
 
 int pc_set_coupling_matrix(pc_system* sys, int spec, const double* J) {
+    return pc_set_coupling_matrices(sys, 1, &spec, J);
+}
+
+int pc_set_coupling_matrices(pc_system* sys, int n, const int32_t* specs, const double* J) {
     int rc = check_sys(sys);
     if (rc) return rc;
-    if (spec < 0 || spec >= int(sys->specs.size())) return fail(PC_ERR_INVALID, "spec index out of range");
-    Coupling& c = sys->specs[size_t(spec)];
-    for (int i = 0; i < 9; ++i) c.J[i] = J[i];
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) c.Jt[3 * a + b] = J[3 * b + a];
+    if (n < 0 || (n > 0 && (!specs || !J))) return fail(PC_ERR_INVALID, "null specs or matrices");
+    bool changed = false;
+    for (int k = 0; k < n; ++k) {
+        if (specs[k] < 0 || specs[k] >= int(sys->specs.size())) return fail(PC_ERR_INVALID, "spec index out of range");
+        for (int i = 0; i < 9; ++i) changed = changed || sys->specs[size_t(specs[k])].J[i] != J[9 * k + i];
+    }
+    // the tables, colour classes and structure follow the matrices alone
+    if (!changed) return PC_OK;
+    for (int k = 0; k < n; ++k) {
+        Coupling& c = sys->specs[size_t(specs[k])];
+        const double* Jk = J + 9 * k;
+        for (int i = 0; i < 9; ++i) c.J[i] = Jk[i];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) c.Jt[3 * a + b] = Jk[3 * b + a];
+    }
     rc = build_tables(sys, false, sys->tab_active);
     if (rc) return rc;
     rc = build_tables(sys, true, sys->tab_full);
@@ -1096,6 +1110,7 @@ int pc_set_coupling_matrix(pc_system* sys, int spec, const double* J) {
 int pc_set_global_field(pc_system* sys, const double* B3) {
     int rc = check_sys(sys, false);
     if (rc) return rc;
+    if (sys->B[0] == B3[0] && sys->B[1] == B3[1] && sys->B[2] == B3[2]) return PC_OK;
     for (int i = 0; i < 3; ++i) sys->B[i] = B3[i];
     sys->drop_graphs();
     return PC_OK;

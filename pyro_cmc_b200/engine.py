@@ -101,6 +101,7 @@ class System:
 
     def set_stream(self, stream_ptr: int):
         call("pc_set_stream", self._h, C.c_void_p(stream_ptr))
+        self.stream_ptr = int(stream_ptr)
 
     # ----------------------------------------------------------- couplings
     def define_coupling(self, name: str, rel_vecs: Sequence[Sequence[Sequence[int]]], J):
@@ -136,6 +137,13 @@ class System:
     def set_coupling_matrix(self, spec: int, J):
         Jm = _c(np.asarray(J, dtype=np.float64).reshape(9), np.float64)
         call("pc_set_coupling_matrix", self._h, int(spec), _dp(Jm))
+
+    def set_coupling_matrices(self, specs: Sequence[int], Js):
+        """Several coupling matrices at once (one rebuild of the tables; none
+        when every matrix already holds its value)."""
+        sp = _c(list(specs), np.int32)
+        Jm = _c(np.asarray(Js, dtype=np.float64).reshape(len(sp), 9), np.float64)
+        call("pc_set_coupling_matrices", self._h, len(sp), sp.ctypes.data_as(C.POINTER(C.c_int)), _dp(Jm))
 
     def set_global_field(self, B):
         Bv = _c(B, np.float64)

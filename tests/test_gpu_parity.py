@@ -431,6 +431,44 @@ def test_duplicate_coupling_name_raises():
         g.define_coupling("J2", [[], [], [], []], np.eye(3))
 
 
+def test_coupling_matrices_set_at_once_match_one_by_one():
+    """pc_set_coupling_matrices (one rebuild of the tables) gives the energy
+    and local fields of the same matrices set one at a time, against the FP64
+    sum over the oracle's neighbour tables; setting the values it already
+    holds changes nothing, and an index out of range changes nothing either."""
+    c = COUPLINGS[1]
+    a, o = pair(4, c)
+    b = pc.pyrochlore_system(4, **c)
+    specs = [0, 3, 6, 8]
+    mats = [1.3 * np.eye(3), 0.7 * np.eye(3), 0.2 * np.eye(3), -0.1 * np.eye(3)]
+    for k, M in zip(specs, mats):
+        a.set_coupling_matrix(k, M)
+    b.set_coupling_matrices(specs, mats)
+    b.set_coupling_matrices(specs, mats)
+    S = unit(np.random.default_rng(5), o.N)
+    for s in (a, b):
+        s.set_spins(S)
+    assert a.structured() and b.structured()
+    np.testing.assert_array_equal(a.energy()[0], b.energy()[0])
+    np.testing.assert_array_equal(a.local_field(), b.local_field())
+    full = [o.spec_matrix(k) for k in range(o.num_specs())]
+    for k, M in zip(specs, mats):
+        full[k] = M
+    S32 = b.spins().astype(np.float64)
+    h = np.zeros_like(S32)
+    for k, M in enumerate(full):
+        nb = o.neighbours(k)
+        for col in range(nb.shape[1]):
+            idx = nb[:, col]
+            ok = idx >= 0
+            h[ok] += S32[idx[ok]] @ M.T
+    e_ref = 0.5 * np.sum(S32 * h) / 4**3
+    assert abs(b.energy()[0][0] - e_ref) <= REL * 16 * (6 * 1.3 + 12 + 1)
+    with pytest.raises(pc.InvalidArgument):
+        b.set_coupling_matrices([0, 99], [np.eye(3), np.eye(3)])
+    np.testing.assert_array_equal(a.energy()[0], b.energy()[0])
+
+
 def test_nonstructural_coupling_uses_generic_path():
     # an asymmetric J2 gives the J2 group two different matrices (J on the
     # source side, J^T on the target side): the generic tables must take over
