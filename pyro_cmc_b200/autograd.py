@@ -36,7 +36,11 @@ def spins_tensor(system: System) -> torch.Tensor:
     """The system's own device spin buffer as a [N_total, 4] float32 tensor
     (a view, no copy)."""
     ptr = system.spins_device_ptr(0)
-    return torch.as_tensor(_DeviceArray(ptr, (system.N_total, 4), "<f4"), device="cuda")
+    view = getattr(system, "_spins_view", None)
+    if view is None or view[0] != ptr:
+        view = (ptr, torch.as_tensor(_DeviceArray(ptr, (system.N_total, 4), "<f4"), device="cuda"))
+        system._spins_view = view
+    return view[1].detach()  # a new tensor object on the same memory each call
 
 
 def _order(system: System):

@@ -64,6 +64,7 @@ class System:
             L = [int(L)] * (n_replicas or 1)
         self.L = [int(x) for x in L]
         self.R = len(self.L)
+        self._N_total = sum(16 * x ** 3 for x in self.L)
         Lv = _c(self.L, np.int32)
         h = C.c_void_p()
         call("pc_create", self.R, Lv.ctypes.data_as(_I32P), C.c_uint64(seed & 0xFFFFFFFFFFFFFFFF), C.byref(h))
@@ -97,7 +98,7 @@ class System:
 
     @property
     def N_total(self) -> int:
-        return sum(16 * L ** 3 for L in self.L)
+        return self._N_total
 
     def set_stream(self, stream_ptr: int):
         call("pc_set_stream", self._h, C.c_void_p(stream_ptr))
