@@ -299,6 +299,20 @@ int pc_pt_slots(pc_system* sys, int32_t* slot_of_replica);
  * all (the spin gradient alone costs about one energy evaluation). */
 int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* grad_S_dev, double* grad_J,
                    double* grad_B);
+/* Device-output forms for callers that keep the results on the GPU (the
+ * autograd path): the work is queued on the system's stream (pc_set_stream)
+ * and the calls return without waiting for it; a device error flag raised by
+ * these kernels is reported by the next call that waits.
+ * pc_energy_device: e_dev[r] = e_per_cell[r] (R doubles, device).
+ * pc_energy_grad_device: upstream g_dev[r] (R doubles, device; NULL: 1 for
+ * every replica); grad_S as pc_energy_grad (may be NULL); sums_dev (may be
+ * NULL) receives per replica a row of 4 + 9 * n_spec doubles: [sum over the
+ * cells of the owned bond energies - S.B (= e_per_cell * Nc), sum_i S_i (3),
+ * and with couplings != 0 the coupling products dE/dJ_spec (9 per spec, as
+ * pc_energy_grad's grad_J before the factor g/Nc)]; without couplings the
+ * products are not formed and those columns are left untouched. */
+int pc_energy_device(pc_system* sys, double* e_dev);
+int pc_energy_grad_device(pc_system* sys, const double* g_dev, void* grad_S_dev, double* sums_dev, int couplings);
 /* pc_energy_grad evaluated on an arbitrary field instead of the system's
  * spins: field_dev (device, float4[N_total], 16-byte aligned, any length per
  * site) stands for S in every formula above, with the system's couplings and
@@ -316,8 +330,19 @@ int pc_energy_grad_field(pc_system* sys, const void* field_dev, const double* g,
 int pc_ssf_forward(pc_system* sys, void* out_dev);
 /* Backward of pc_ssf_forward: given dLoss/dS (device, same layout as
  * out_dev: d/dRe, d/dIm), writes dLoss/dS_i into grad_S_dev (float4[N_total],
- * device). Recomputes the forward transform instead of storing it. */
+ * device). Recomputes the forward transform instead of storing it (see
+ * pc_ssf_backward_kept). */
 int pc_ssf_backward(pc_system* sys, const void* grad_out_dev, void* grad_S_dev);
+/* The same pair for callers that keep the results on the GPU (the autograd
+ * path): both are queued on the system's stream (pc_set_stream) and return
+ * without waiting. pc_ssf_forward_keep also keeps the forward amplitudes and
+ * hands out a token (nonzero) for them; pc_ssf_backward_kept with that token
+ * uses them instead of recomputing the forward transform, provided the
+ * system's spins are again those of that forward (the caller's contract, as
+ * with a tensor saved for backward) and no forward or backward ran in
+ * between (else the token is stale and the transform is recomputed). */
+int pc_ssf_forward_keep(pc_system* sys, void* out_dev, uint64_t* token);
+int pc_ssf_backward_kept(pc_system* sys, uint64_t token, const void* grad_out_dev, void* grad_S_dev);
 
 /* ------------------------------------------------------ allocation-free */
 

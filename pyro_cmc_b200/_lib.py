@@ -37,6 +37,8 @@ _SIGNATURES = {
     "pc_define_coupling": (_I, [_P, C.c_char_p, _I64P, _I32P, _DP]),
     "pc_set_coupling_matrix": (_I, [_P, _I, _DP]),
     "pc_set_coupling_matrices": (_I, [_P, _I, _IP, _DP]),
+    "pc_energy_device": (_I, [_P, _P]),
+    "pc_energy_grad_device": (_I, [_P, _P, _P, _P, _I]),
     "pc_set_global_field": (_I, [_P, _DP]),
     "pc_get_global_field": (_I, [_P, _DP]),
     "pc_set_T_ref": (_I, [_P, _D]),
@@ -86,6 +88,8 @@ _SIGNATURES = {
     "pc_spin_ft": (_I, [_P, _I, _DP]),
     "pc_ssf_forward": (_I, [_P, _P]),
     "pc_ssf_backward": (_I, [_P, _P, _P]),
+    "pc_ssf_forward_keep": (_I, [_P, _P, C.POINTER(C.c_uint64)]),
+    "pc_ssf_backward_kept": (_I, [_P, C.c_uint64, _P, _P]),
     "pc_energy_noalloc": (_I, [_P, _I, _DP, _P, _P]),
     "pc_autotune": (_I, [_P]),
     "pc_set_load_variant": (_I, [_P, _I]),

@@ -51,6 +51,13 @@ def _order(system: System):
         torch.cuda.current_stream().synchronize()
 
 
+def _join(system: System):
+    """Orders the current torch stream after the system's queued work (the
+    device-output calls return without waiting)."""
+    if getattr(system, "stream_ptr", None) != torch.cuda.current_stream().cuda_stream:
+        torch.cuda.synchronize()
+
+
 def _load(system: System, spins: torch.Tensor):
     if spins.shape != (system.N_total, 4) or spins.dtype != torch.float32 or not spins.is_cuda:
         raise ValueError("spins must be a float32 CUDA tensor of shape [N_total, 4]")
@@ -101,31 +108,69 @@ def _param_grads(system: System, gJ: np.ndarray, gB: np.ndarray) -> np.ndarray:
     return out
 
 
+def _param_grads_device(system: System, gJ: torch.Tensor, gB: torch.Tensor) -> torch.Tensor:
+    """_param_grads on device tensors: gJ [R, n_spec, 3, 3], gB [R, 3] -> [R, 6]."""
+    key = (gJ.device, gJ.shape[1])
+    cache = getattr(system, "_dparam_mats", None)
+    if cache is None or cache[0] != key:
+        # d(spec matrix)/dJ1, dJ2, dJ3 per spec
+        pp = system.pyro_params
+        D = np.zeros((3, gJ.shape[1], 3, 3))
+        k = 0
+        I3 = np.eye(3)
+        if pp["split_J1"]:
+            for mu, nu in PAIRS:
+                D[0, k] = I3 + (pp["Delta"] - 1.0) * np.outer(local_axis(mu), local_axis(nu))
+                k += 1
+        else:
+            D[0, k] = I3
+            k += 1
+        D[1, k] = I3
+        D[2, k + 1] = I3
+        D[2, k + 2] = I3
+        cache = (key, torch.as_tensor(D, dtype=torch.float64, device=gJ.device))
+        system._dparam_mats = cache
+    return torch.cat([torch.einsum("rsab,jsab->rj", gJ, cache[1]), gB], dim=1)
+
+
 class EnergyFunction(torch.autograd.Function):
+    """e_per_cell[r] of every replica (total_energy_per_unit_cell,
+    src/MC.cpp:305-312) with its gradients in the spins and, given params
+    [J1, J2, J3, Bx, By, Bz], in those; results stay on the device (the
+    device-output entry points, ordered by stream)."""
+
     @staticmethod
     def forward(ctx, spins, params, system):
         if params is not None:
             _apply_params(system, params)
         _load(system, spins)
-        e, _ = system.energy()
+        e = torch.empty(system.R, dtype=torch.float64, device=spins.device)
+        system.energy_device(e.data_ptr())
+        _join(system)
         ctx.system = system
         ctx.has_params = params is not None
         ctx.params_device = params.device if params is not None else None
         ctx.save_for_backward(spins)
-        return torch.as_tensor(e, dtype=torch.float64, device=spins.device)
+        return e
 
     @staticmethod
     def backward(ctx, grad_e):
         system = ctx.system
         (spins,) = ctx.saved_tensors
         _load(system, spins)
-        g = grad_e.detach().to("cpu", torch.float64).numpy()
+        g = grad_e.detach().to(device=spins.device, dtype=torch.float64).contiguous()
         grad_spins = torch.empty_like(spins)  # every site is written
-        _, gJ, gB = system.energy_grad(g, grad_spins.data_ptr(), couplings=ctx.has_params)
+        n_spec = len(system.spec_names)
+        sums = torch.zeros((system.R, 4 + 9 * n_spec), dtype=torch.float64, device=spins.device)
+        _order(system)
+        system.energy_grad_device(g.data_ptr(), grad_spins.data_ptr(), sums.data_ptr(), couplings=ctx.has_params)
+        _join(system)
         gp = None
         if ctx.has_params:
-            gp = torch.as_tensor(_param_grads(system, gJ.reshape(system.R, -1, 3, 3), gB).sum(axis=0),
-                                 dtype=torch.float64, device=ctx.params_device)
+            s = g / torch.as_tensor(_nc_vector(system), device=spins.device)
+            gJ = (s[:, None] * sums[:, 4:]).reshape(system.R, n_spec, 3, 3)
+            gB = -s[:, None] * sums[:, 1:4]
+            gp = _param_grads_device(system, gJ, gB).sum(dim=0).to(ctx.params_device)
         return grad_spins, gp, None
 
 
@@ -136,7 +181,8 @@ class SSFFunction(torch.autograd.Function):
         nk = system.Nc(0)
         out = torch.empty((system.R, system.n_corr, nk, 2), dtype=torch.float64, device=spins.device)
         _order(system)
-        system.ssf_forward_device(out.data_ptr())
+        ctx.token = system.ssf_forward_keep(out.data_ptr())  # the amplitudes stay for the backward
+        _join(system)
         ctx.system = system
         ctx.save_for_backward(spins)
         return out
@@ -149,7 +195,8 @@ class SSFFunction(torch.autograd.Function):
         go = grad_out.detach().to(torch.float64).contiguous()
         grad_spins = torch.empty_like(spins)
         _order(system)
-        system.ssf_backward_device(go.data_ptr(), grad_spins.data_ptr())
+        system.ssf_backward_kept(ctx.token, go.data_ptr(), grad_spins.data_ptr())
+        _join(system)
         return grad_spins, None
 
 

@@ -191,6 +191,7 @@ struct pc_system {
     DevBuf<double> d_theta;
     DevBuf<float4> d_field;
     DevBuf<double> d_grad_g, d_grad_out;  // energy-gradient upstream scalars and results
+    DevBuf<double> d_grad_ones;           // g = 1 per replica (pc_energy_grad_device without g)
     // structured energy gradient: specs per (sublattice, group, bond side) and
     // work items of up to kGradK tiles of one (replica, sublattice)
     bool grad_struct = false;
@@ -243,6 +244,8 @@ struct pc_system {
     DevBuf<uint64_t> d_round;
     std::map<std::pair<int, int>, std::pair<cudaGraphExec_t, int>> pt_graphs;  // (n_sweep, phase)
     uint64_t pt_sweeps_done = 0;
+    // amplitudes kept by pc_ssf_forward_keep: the token handed out with them (0: none)
+    uint64_t amp_token = 0, amp_serial = 0;
     // rounds in one persistent cooperative launch (pt_persistent.cu)
     bool pt_persistent = false;
     DevBuf<unsigned int> d_bar;                 // grid barrier state (pc::kBarrierWords)
@@ -307,6 +310,7 @@ struct pc_system {
         d_ssf_sum.release();
         d_ssf_sq.release();
         d_grad_g.release();
+        d_grad_ones.release();
         d_grad_out.release();
         d_grad_items.release();
         d_item_begin.release();
@@ -1756,14 +1760,14 @@ int pc_ssf_clear(pc_system* sys, int slot) {
     return PC_OK;
 }
 
-int pc_ssf_forward(pc_system* sys, void* out_dev) {
-    int rc = check_sys(sys);
-    if (rc) return rc;
+namespace {
+// S(q) of every replica into out_dev (see pc_ssf_forward), queued without
+// waiting; with keep_amp the amplitudes B^a(K) stay in the groups' d_amp.
+int ssf_forward_enqueue(pc_system* sys, void* out_dev, bool keep_amp) {
     if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
     if (sys->ssf_resolved) return fail(PC_ERR_UNSUPPORTED, "the differentiable S(q) is the contracted one");
     // out_dev is [R][n_corr][n_k][2] with replicas in index order; the kernel
     // indexes by position inside each size group, so offset per group.
-    size_t base = 0;
     for (auto& g : sys->groups) {
         const size_t nk = size_t(g.L) * g.L * g.L;
         // groups must be replica-contiguous for the packed layout
@@ -1773,14 +1777,64 @@ int pc_ssf_forward(pc_system* sys, void* out_dev) {
         size_t off = 0;
         for (int r = 0; r < g.reps[0]; ++r) off += size_t(sys->n_corr) * size_t(sys->Nc(r)) * 2;
         o.val = static_cast<double*>(out_dev) + off;
+        if (keep_amp) {
+            if (g.d_amp.n != g.reps.size() * 3 * nk) PC_CK(g.d_amp.alloc(g.reps.size() * 3 * nk));
+            o.amp = g.d_amp.p;
+        }
         pc::SsfGeom geom{g.L, g.P, g.Q, int(g.reps.size()), g.d_rep_index.p};
         pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, g.d_G.p, sys->stream);
         PC_LAUNCH_CK();
         pc::launch_ssf_z(geom, g.d_G.p, o, sys->stream);
         PC_LAUNCH_CK();
         sys->launches += 2;
-        base += g.reps.size() * nk;
     }
+    return PC_OK;
+}
+
+// dLoss/dS_i into grad_S_dev (see pc_ssf_backward), queued without waiting;
+// recompute: the forward amplitudes are formed again from the current spins
+// (else the groups' d_amp holds them).
+int ssf_backward_enqueue(pc_system* sys, const void* grad_out_dev, void* grad_S_dev, bool recompute) {
+    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
+    if (sys->ssf_resolved) return fail(PC_ERR_UNSUPPORTED, "the differentiable S(q) is the contracted one");
+    for (auto& g : sys->groups)
+        for (size_t i = 0; i < g.reps.size(); ++i)
+            if (g.reps[i] != g.reps[0] + int(i))
+                return fail(PC_ERR_UNSUPPORTED, "ssf backward needs size-sorted replicas");
+    PC_CK(cudaMemsetAsync(grad_S_dev, 0, sizeof(float4) * size_t(sys->N_tot), sys->stream));
+    for (auto& g : sys->groups) {
+        const size_t nk = size_t(g.L) * g.L * g.L;
+        if (g.d_amp.n != g.reps.size() * 3 * nk) {
+            PC_CK(g.d_amp.alloc(g.reps.size() * 3 * nk));
+            recompute = true;
+        }
+        pc::SsfGeom geom{g.L, g.P, g.Q, int(g.reps.size()), g.d_rep_index.p};
+        pc::SsfOut o = ssf_out_base(sys);
+        o.amp = g.d_amp.p;
+        if (recompute) {  // the forward amplitudes
+            pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, g.d_G.p, sys->stream);
+            PC_LAUNCH_CK();
+            pc::launch_ssf_z(geom, g.d_G.p, o, sys->stream);
+            PC_LAUNCH_CK();
+            sys->launches += 2;
+        }
+        size_t off = 0;
+        for (int r = 0; r < g.reps[0]; ++r) off += size_t(sys->n_corr) * size_t(sys->Nc(r)) * 2;
+        const double* dval = static_cast<const double*>(grad_out_dev) + off;
+        pc::launch_ssf_adjoint(geom, o, dval, g.d_amp.p, g.d_G.p, static_cast<float4*>(grad_S_dev), sys->d_reps.p,
+                               sys->stream);
+        PC_LAUNCH_CK();
+        sys->launches += 2;
+    }
+    return PC_OK;
+}
+}  // namespace
+
+int pc_ssf_forward(pc_system* sys, void* out_dev) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    rc = ssf_forward_enqueue(sys, out_dev, false);
+    if (rc) return rc;
     PC_CK(cudaStreamSynchronize(sys->stream));
     return PC_OK;
 }
@@ -1788,33 +1842,32 @@ int pc_ssf_forward(pc_system* sys, void* out_dev) {
 int pc_ssf_backward(pc_system* sys, const void* grad_out_dev, void* grad_S_dev) {
     int rc = check_sys(sys);
     if (rc) return rc;
-    if (!sys->ssf_ready) return fail(PC_ERR_STATE, "ssf not configured");
-    if (sys->ssf_resolved) return fail(PC_ERR_UNSUPPORTED, "the differentiable S(q) is the contracted one");
-    PC_CK(cudaMemsetAsync(grad_S_dev, 0, sizeof(float4) * size_t(sys->N_tot), sys->stream));
-    for (auto& g : sys->groups) {
-        for (size_t i = 0; i < g.reps.size(); ++i)
-            if (g.reps[i] != g.reps[0] + int(i))
-                return fail(PC_ERR_UNSUPPORTED, "ssf backward needs size-sorted replicas");
-        const size_t nk = size_t(g.L) * g.L * g.L;
-        if (g.d_amp.n != g.reps.size() * 3 * nk) PC_CK(g.d_amp.alloc(g.reps.size() * 3 * nk));
-        pc::SsfGeom geom{g.L, g.P, g.Q, int(g.reps.size()), g.d_rep_index.p};
-        pc::SsfOut o = ssf_out_base(sys);
-        o.amp = g.d_amp.p;
-        // recompute the forward amplitudes
-        pc::launch_ssf_xy(geom, sys->d_spins.p, sys->d_reps.p, g.d_G.p, sys->stream);
-        PC_LAUNCH_CK();
-        pc::launch_ssf_z(geom, g.d_G.p, o, sys->stream);
-        PC_LAUNCH_CK();
-        size_t off = 0;
-        for (int r = 0; r < g.reps[0]; ++r) off += size_t(sys->n_corr) * size_t(sys->Nc(r)) * 2;
-        const double* dval = static_cast<const double*>(grad_out_dev) + off;
-        pc::launch_ssf_adjoint(geom, o, dval, g.d_amp.p, g.d_G.p, static_cast<float4*>(grad_S_dev), sys->d_reps.p,
-                               sys->stream);
-        PC_LAUNCH_CK();
-        sys->launches += 4;
-    }
+    rc = ssf_backward_enqueue(sys, grad_out_dev, grad_S_dev, true);
+    sys->amp_token = 0;  // the kept amplitudes were overwritten
+    if (rc) return rc;
     PC_CK(cudaStreamSynchronize(sys->stream));
     return PC_OK;
+}
+
+int pc_ssf_forward_keep(pc_system* sys, void* out_dev, uint64_t* token) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!token) return fail(PC_ERR_INVALID, "pc_ssf_forward_keep: null token");
+    *token = 0;
+    sys->amp_token = 0;
+    rc = ssf_forward_enqueue(sys, out_dev, true);
+    if (rc) return rc;
+    sys->amp_token = ++sys->amp_serial;
+    *token = sys->amp_token;
+    return PC_OK;
+}
+
+int pc_ssf_backward_kept(pc_system* sys, uint64_t token, const void* grad_out_dev, void* grad_S_dev) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    const bool kept = token != 0 && token == sys->amp_token;
+    if (!kept) sys->amp_token = 0;
+    return ssf_backward_enqueue(sys, grad_out_dev, grad_S_dev, !kept);
 }
 
 int pc_ssf_current(pc_system* sys, int replica, double* out) {
@@ -2197,6 +2250,8 @@ int pc_pt_slots(pc_system* sys, int32_t* slot_of_replica) {
 namespace {
 int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double* e_per_cell, void* grad_S_dev,
                    double* grad_J, double* grad_B);
+int enqueue_energy_grad(pc_system* sys, const float4* spins, const double* g_dev, void* grad_S_dev, bool want_J,
+                        int* width_out);
 }
 
 int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* grad_S_dev, double* grad_J,
@@ -2204,6 +2259,45 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
     int rc = check_sys(sys);
     if (rc) return rc;
     return energy_grad_of(sys, sys->d_spins.p, g, e_per_cell, grad_S_dev, grad_J, grad_B);
+}
+
+int pc_energy_device(pc_system* sys, double* e_dev) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!e_dev || reinterpret_cast<uintptr_t>(e_dev) % 8 != 0)
+        return fail(PC_ERR_INVALID, "pc_energy_device: null or misaligned output");
+    rc = enqueue_energy(sys);
+    if (rc) return rc;
+    PC_CK(cudaMemcpyAsync(e_dev, sys->d_e.p, sizeof(double) * size_t(sys->R), cudaMemcpyDeviceToDevice, sys->stream));
+    return PC_OK;
+}
+
+int pc_energy_grad_device(pc_system* sys, const double* g_dev, void* grad_S_dev, double* sums_dev, int couplings) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if ((g_dev && reinterpret_cast<uintptr_t>(g_dev) % 8 != 0) ||
+        (grad_S_dev && reinterpret_cast<uintptr_t>(grad_S_dev) % 16 != 0) ||
+        (sums_dev && reinterpret_cast<uintptr_t>(sums_dev) % 8 != 0))
+        return fail(PC_ERR_INVALID, "pc_energy_grad_device: misaligned pointer");
+    const size_t R = size_t(sys->R);
+    if (!g_dev) {  // g = 1 for every replica
+        if (sys->d_grad_ones.n != R) {
+            PC_CK(sys->d_grad_ones.alloc(R));
+            const std::vector<double> ones(R, 1.0);
+            PC_CK(cudaMemcpy(sys->d_grad_ones.p, ones.data(), sizeof(double) * R, cudaMemcpyHostToDevice));
+        }
+        g_dev = sys->d_grad_ones.p;
+    }
+    int width = 0;
+    rc = enqueue_energy_grad(sys, sys->d_spins.p, g_dev, grad_S_dev, couplings != 0, &width);
+    if (rc) return rc;
+    if (sums_dev) {
+        const size_t row = size_t(4 + 9 * int(sys->specs.size()));
+        const size_t cols = couplings ? row : 4;
+        PC_CK(cudaMemcpy2DAsync(sums_dev, row * sizeof(double), sys->d_grad_out.p, size_t(width) * sizeof(double),
+                                cols * sizeof(double), R, cudaMemcpyDeviceToDevice, sys->stream));
+    }
+    return PC_OK;
 }
 
 int pc_energy_grad_field(pc_system* sys, const void* field_dev, const double* g, double* e_per_cell,
@@ -2220,23 +2314,19 @@ int pc_energy_grad_field(pc_system* sys, const void* field_dev, const double* g,
 }  // extern "C"
 
 namespace {
-int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double* e_per_cell, void* grad_S_dev,
-                   double* grad_J, double* grad_B) {
+// Queues the gradient kernels for the upstream g_dev (device, one double per
+// replica) on the system's stream; the per-replica sums land in d_grad_out,
+// *width doubles a replica: [sum of the owned bond energies - S.B, sum S (3),
+// the 9 * n_spec coupling products when formed].
+int enqueue_energy_grad(pc_system* sys, const float4* spins, const double* g_dev, void* grad_S_dev, bool want_J,
+                        int* width_out) {
     const int ns = int(sys->specs.size());
     // the structured kernel forms the coupling products only when they are asked for
     const bool structured = sys->grad_struct && sys->threads <= 256;
-    const int width = (structured && !grad_J) ? 4 : 4 + 9 * ns;
-    if (sys->d_grad_g.n != size_t(sys->R)) PC_CK(sys->d_grad_g.alloc(size_t(sys->R)));
+    const int width = (structured && !want_J) ? 4 : 4 + 9 * ns;
     if (sys->d_grad_out.n < size_t(sys->R) * size_t(4 + 9 * ns))  // the widest form, kept across calls
         PC_CK(sys->d_grad_out.alloc(size_t(sys->R) * size_t(4 + 9 * ns)));
-    DevBuf<double>& d_g = sys->d_grad_g;
     DevBuf<double>& d_out = sys->d_grad_out;
-    const size_t R = size_t(sys->R);
-    PC_CK(sys->stage(sizeof(double) * R * size_t(1 + width)));
-    double* st_g = static_cast<double*>(sys->h_stage);
-    double* st_out = st_g + R;
-    for (size_t r = 0; r < R; ++r) st_g[r] = g ? g[r] : 1.0;
-    PC_CK(cudaMemcpyAsync(d_g.p, st_g, sizeof(double) * R, cudaMemcpyHostToDevice, sys->stream));
     if (structured) {
         pc::GradStructArgs a;
         a.spins = spins;
@@ -2246,12 +2336,12 @@ int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double*
         a.n_items = sys->n_grad_items;
         a.width = width;
         for (int i = 0; i < 3; ++i) a.B[i] = float(sys->B[i]);
-        a.g = d_g.p;
+        a.g = g_dev;
         a.grad_S = static_cast<float4*>(grad_S_dev);
         a.partial = sys->d_grad_partial.p;
         a.mats = sys->mats;
         std::memcpy(a.spec_mask, sys->spec_mask, sizeof(a.spec_mask));
-        pc::launch_energy_grad_struct(a, grad_J != nullptr, sys->threads, sys->stream);
+        pc::launch_energy_grad_struct(a, want_J, sys->threads, sys->stream);
         PC_LAUNCH_CK();
         pc::launch_grad_finalize(sys->d_grad_partial.p, width, sys->d_item_begin.p, sys->d_item_end.p, sys->R,
                                  d_out.p, sys->stream);
@@ -2265,7 +2355,7 @@ int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double*
         a.n_tiles = sys->n_all_tiles;
         a.n_spec = ns;
         for (int i = 0; i < 3; ++i) a.B[i] = float(sys->B[i]);
-        a.g = d_g.p;
+        a.g = g_dev;
         a.grad_S = static_cast<float4*>(grad_S_dev);
         a.partial = sys->d_partial.p;
         pc::launch_energy_grad_partials(a, sys->threads, sys->stream);
@@ -2275,7 +2365,25 @@ int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double*
         PC_LAUNCH_CK();
     }
     sys->launches += 2;
-    PC_CK(cudaMemcpyAsync(st_out, d_out.p, sizeof(double) * R * size_t(width), cudaMemcpyDeviceToHost, sys->stream));
+    *width_out = width;
+    return PC_OK;
+}
+
+int energy_grad_of(pc_system* sys, const float4* spins, const double* g, double* e_per_cell, void* grad_S_dev,
+                   double* grad_J, double* grad_B) {
+    const int ns = int(sys->specs.size());
+    if (sys->d_grad_g.n != size_t(sys->R)) PC_CK(sys->d_grad_g.alloc(size_t(sys->R)));
+    const size_t R = size_t(sys->R);
+    PC_CK(sys->stage(sizeof(double) * R * size_t(1 + 4 + 9 * ns)));
+    double* st_g = static_cast<double*>(sys->h_stage);
+    double* st_out = st_g + R;
+    for (size_t r = 0; r < R; ++r) st_g[r] = g ? g[r] : 1.0;
+    PC_CK(cudaMemcpyAsync(sys->d_grad_g.p, st_g, sizeof(double) * R, cudaMemcpyHostToDevice, sys->stream));
+    int width = 0;
+    const int rc = enqueue_energy_grad(sys, spins, sys->d_grad_g.p, grad_S_dev, grad_J != nullptr, &width);
+    if (rc) return rc;
+    PC_CK(cudaMemcpyAsync(st_out, sys->d_grad_out.p, sizeof(double) * R * size_t(width), cudaMemcpyDeviceToHost,
+                          sys->stream));
     PC_CK(cudaStreamSynchronize(sys->stream));
     for (int r = 0; r < sys->R; ++r) {
         const double* o = st_out + size_t(r) * size_t(width);

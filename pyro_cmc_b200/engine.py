@@ -391,6 +391,17 @@ class System:
     def ssf_backward_device(self, grad_out_ptr: int, grad_spins_ptr: int):
         call("pc_ssf_backward", self._h, C.c_void_p(grad_out_ptr), C.c_void_p(grad_spins_ptr))
 
+    def ssf_forward_keep(self, out_ptr: int) -> int:
+        """pc_ssf_forward_keep: queued, keeps the amplitudes; returns their token."""
+        t = C.c_uint64()
+        call("pc_ssf_forward_keep", self._h, C.c_void_p(out_ptr), C.byref(t))
+        return int(t.value)
+
+    def ssf_backward_kept(self, token: int, grad_out_ptr: int, grad_spins_ptr: int):
+        """pc_ssf_backward_kept: queued; reuses the amplitudes of `token` when
+        still held."""
+        call("pc_ssf_backward_kept", self._h, C.c_uint64(token), C.c_void_p(grad_out_ptr), C.c_void_p(grad_spins_ptr))
+
     # ----------------------------------------------------------- tempering
     def pt_configure(self, T):
         Tv = _c(T, np.float64)
@@ -435,6 +446,20 @@ class System:
              None if grad_spins_ptr is None else C.c_void_p(grad_spins_ptr), None if gJ is None else _dp(gJ),
              _dp(gB))
         return e, None if gJ is None else gJ.reshape(self.R, n_spec, 3, 3), gB
+
+    def energy_device(self, e_ptr: int):
+        """Queues the energy per cell of every replica into the device array
+        at e_ptr (R doubles) on the system's stream, without waiting."""
+        call("pc_energy_device", self._h, C.c_void_p(e_ptr))
+
+    def energy_grad_device(self, g_ptr: int | None, grad_spins_ptr: int | None, sums_ptr: int | None,
+                           couplings: bool):
+        """Queues pc_energy_grad_device: upstream g (R device doubles, None:
+        1), dE/dS into grad_spins_ptr, per-replica sums (R x (4 + 9 n_spec)
+        device doubles) into sums_ptr; returns without waiting."""
+        call("pc_energy_grad_device", self._h, None if g_ptr is None else C.c_void_p(g_ptr),
+             None if grad_spins_ptr is None else C.c_void_p(grad_spins_ptr),
+             None if sums_ptr is None else C.c_void_p(sums_ptr), int(bool(couplings)))
 
     def energy_grad_field(self, field_ptr: int, g=None, grad_ptr: int | None = None, couplings: bool = True):
         """energy_grad evaluated on the device field at field_ptr (float4

@@ -166,3 +166,83 @@ def test_fit_recovers_couplings_from_quenched_ssf():
                                     steps=steps, lr=lr, iters=80, step_size=0.01)
     assert hist[-1] < 1e-2 * hist[0], hist[[0, -1]]
     assert abs(p[1] - 0.1) < 0.01 and abs(p[2] + 0.05) < 0.01, p
+
+
+def test_device_output_energy_and_gradient_match_the_host_calls():
+    """pc_energy_device and pc_energy_grad_device (results left on the device,
+    queued without waiting) give the host calls' energies, spin gradient and
+    per-replica sums bit for bit, with and without the coupling products, with
+    the upstream g on the device or 1 for every replica."""
+    import torch
+
+    s = pc.pyrochlore_system([4, 4, 4], J1=1.0, J2=0.1, J3=-0.05, B=(0.2, 0.0, 0.1), seed=2)
+    s.random_spins(9)
+    R, ns = s.R, len(s.spec_names)
+    nc = np.array([s.Nc(r) for r in range(R)], dtype=np.float64)
+    e_host, _ = s.energy()
+    e_dev = torch.empty(R, dtype=torch.float64, device="cuda")
+    s.energy_device(e_dev.data_ptr())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(e_dev.cpu().numpy(), e_host)
+    up = np.array([0.5, -1.0, 2.0])
+    for couplings in (True, False):
+        gs_host = torch.empty((s.N_total, 4), dtype=torch.float32, device="cuda")
+        e2, gJ, gB = s.energy_grad(up, gs_host.data_ptr(), couplings=couplings)
+        gs = torch.empty_like(gs_host)
+        sums = torch.zeros((R, 4 + 9 * ns), dtype=torch.float64, device="cuda")
+        gd = torch.as_tensor(up, device="cuda")
+        s.energy_grad_device(gd.data_ptr(), gs.data_ptr(), sums.data_ptr(), couplings)
+        torch.cuda.synchronize()
+        assert torch.equal(gs, gs_host)
+        v = sums.cpu().numpy()
+        np.testing.assert_array_equal(v[:, 0] / nc, e2)
+        np.testing.assert_array_equal(-up[:, None] * v[:, 1:4] / nc[:, None], gB)
+        if couplings:
+            np.testing.assert_array_equal(up[:, None] * v[:, 4:] / nc[:, None], gJ.reshape(R, -1))
+        else:
+            assert (v[:, 4:] == 0).all()
+    sums = torch.zeros((R, 4 + 9 * ns), dtype=torch.float64, device="cuda")
+    s.energy_grad_device(None, None, sums.data_ptr(), False)
+    torch.cuda.synchronize()
+    e3, _, gB3 = s.energy_grad(None, None, couplings=False)
+    v = sums.cpu().numpy()
+    np.testing.assert_array_equal(v[:, 0] / nc, e3)
+    np.testing.assert_array_equal(-v[:, 1:4] / nc[:, None], gB3)
+
+
+def test_kept_ssf_amplitudes_give_the_recomputed_backward():
+    """pc_ssf_forward_keep / pc_ssf_backward_kept: the forward values equal
+    pc_ssf_forward's, and the backward from the kept amplitudes equals
+    pc_ssf_backward's (which recomputes the transform) bit for bit; a token
+    made stale by a later forward on other spins falls back to recomputing."""
+    s = pc.pyrochlore_system([4, 4, 6], J1=1.0, J2=0.1, seed=3)
+    s.ssf_configure(["zz", "xy"], 0, [])
+    s.random_spins(4)
+    A = ag.spins_tensor(s).clone()
+    out = torch.empty((s.R, s.n_corr, s.Nc(0), 2), dtype=torch.float64, device="cuda")
+    n_val = sum(s.n_corr * s.Nc(r) * 2 for r in range(s.R))
+    out = torch.empty(n_val, dtype=torch.float64, device="cuda")
+    go = torch.randn(n_val, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    ref = torch.empty((s.N_total, 4), dtype=torch.float32, device="cuda")
+    s.ssf_backward_device(go.data_ptr(), ref.data_ptr())
+    ref_val = torch.empty_like(out)
+    s.ssf_forward_device(ref_val.data_ptr())
+    t1 = s.ssf_forward_keep(out.data_ptr())
+    torch.cuda.synchronize()
+    assert t1 != 0 and torch.equal(out, ref_val)
+    got = torch.empty_like(ref)
+    s.ssf_backward_kept(t1, go.data_ptr(), got.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref)
+    # stale: a forward on other spins in between, then the first spins again
+    t1 = s.ssf_forward_keep(out.data_ptr())
+    s.random_spins(5)
+    t2 = s.ssf_forward_keep(out.data_ptr())
+    torch.cuda.synchronize()
+    assert t2 != t1
+    ag.spins_tensor(s).copy_(A)
+    torch.cuda.synchronize()
+    got = torch.empty_like(ref)
+    s.ssf_backward_kept(t1, go.data_ptr(), got.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref)
