@@ -312,6 +312,13 @@ int pc_energy_grad(pc_system* sys, const double* g, double* e_per_cell, void* gr
  * pc_energy_grad's grad_J before the factor g/Nc)]; without couplings the
  * products are not formed and those columns are left untouched. */
 int pc_energy_device(pc_system* sys, double* e_dev);
+/* pc_energy_device plus, per replica, out_dev[r][9] = [the bare sums of
+ * S_i.S_j over the bonds of each of the six coupling groups (J1 towards
+ * pyrochlore sublattices in three groups, J2, J3a, J3b), sum_i S_i (3)] (device,
+ * queued without waiting): dE/dj of each group's isotropic coupling j I times
+ * Nc, from the energy pass itself. PC_ERR_UNSUPPORTED unless every group
+ * matrix is j I, j != 0, the same on all sublattices. */
+int pc_energy_groups_device(pc_system* sys, double* e_dev, double* out_dev);
 int pc_energy_grad_device(pc_system* sys, const double* g_dev, void* grad_S_dev, double* sums_dev, int couplings);
 /* pc_energy_grad evaluated on an arbitrary field instead of the system's
  * spins: field_dev (device, float4[N_total], 16-byte aligned, any length per

@@ -38,6 +38,7 @@ _SIGNATURES = {
     "pc_set_coupling_matrix": (_I, [_P, _I, _DP]),
     "pc_set_coupling_matrices": (_I, [_P, _I, _IP, _DP]),
     "pc_energy_device": (_I, [_P, _P]),
+    "pc_energy_groups_device": (_I, [_P, _P, _P]),
     "pc_energy_grad_device": (_I, [_P, _P, _P, _P, _I]),
     "pc_set_global_field": (_I, [_P, _DP]),
     "pc_get_global_field": (_I, [_P, _DP]),

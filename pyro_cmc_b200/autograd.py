@@ -21,6 +21,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from ._lib import ERR_UNSUPPORTED, PyroCMCError
 from .engine import PAIRS, System, local_axis
 
 
@@ -145,7 +146,19 @@ class EnergyFunction(torch.autograd.Function):
             _apply_params(system, params)
         _load(system, spins)
         e = torch.empty(system.R, dtype=torch.float64, device=spins.device)
-        system.energy_device(e.data_ptr())
+        ctx.groups = None
+        if params is not None and system.pyro_params["Delta"] == 1.0:
+            # isotropic J1, J2, J3: dE/dJ are the groups' bare bond sums, which
+            # the energy pass forms anyway (pc_energy_groups_device)
+            groups = torch.empty((system.R, 9), dtype=torch.float64, device=spins.device)
+            try:
+                system.energy_groups_device(e.data_ptr(), groups.data_ptr())
+                ctx.groups = groups
+            except PyroCMCError as err:
+                if err.code != ERR_UNSUPPORTED:
+                    raise
+        if ctx.groups is None:
+            system.energy_device(e.data_ptr())
         _join(system)
         ctx.system = system
         ctx.has_params = params is not None
@@ -163,10 +176,17 @@ class EnergyFunction(torch.autograd.Function):
         n_spec = len(system.spec_names)
         sums = torch.zeros((system.R, 4 + 9 * n_spec), dtype=torch.float64, device=spins.device)
         _order(system)
-        system.energy_grad_device(g.data_ptr(), grad_spins.data_ptr(), sums.data_ptr(), couplings=ctx.has_params)
+        fast = ctx.groups is not None
+        system.energy_grad_device(g.data_ptr(), grad_spins.data_ptr(), sums.data_ptr(),
+                                  couplings=ctx.has_params and not fast)
         _join(system)
         gp = None
-        if ctx.has_params:
+        if fast:
+            s = g / torch.as_tensor(_nc_vector(system), device=spins.device)
+            G = ctx.groups
+            dj = torch.stack([G[:, 0] + G[:, 1] + G[:, 2], G[:, 3], G[:, 4] + G[:, 5]], dim=1)
+            gp = torch.cat([s[:, None] * dj, -s[:, None] * G[:, 6:9]], dim=1).sum(dim=0).to(ctx.params_device)
+        elif ctx.has_params:
             s = g / torch.as_tensor(_nc_vector(system), device=spins.device)
             gJ = (s[:, None] * sums[:, 4:]).reshape(system.R, n_spec, 3, 3)
             gB = -s[:, None] * sums[:, 1:4]

@@ -216,12 +216,14 @@ __device__ __forceinline__ void load_own(float3 (&own)[16], const char* base, ui
 
 // The cubic cell at coordinates c of the lattice whose spins start at base
 // (sublattice stride sl_bytes): v[0] = its owned bond energies - S.B, v[1..3]
-// = its summed spin. NC: loads through the read-only path (the stand-alone
-// kernel); false: coherent weak loads (the persistent kernel, whose earlier
-// phases wrote the spins).
-template <int ISO, bool UNI, bool NC>
+// = its summed spin; GROUPS (with UNI): gs[G] = its bare sum of S_i.S_j over
+// the owned bonds of group G. NC: loads through the read-only path (the
+// stand-alone kernel); false: coherent weak loads (the persistent kernel,
+// whose earlier phases wrote the spins).
+template <int ISO, bool UNI, bool NC, bool GROUPS = false>
 __device__ __forceinline__ void cell_energy(double (&v)[4], const char* base, uint32_t sl_bytes, const Coords& c,
-                                            const PyroMats& mats, const float* B) {
+                                            const PyroMats& mats, const float* B, double* gs = nullptr) {
+    static_assert(!GROUPS || UNI, "group sums come from the per-group accumulators");
     float3 own[16];
     load_own<NC>(own, base, sl_bytes, c, std::make_integer_sequence<int, 16>{});
     float acc[kAcc];
@@ -231,6 +233,10 @@ __device__ __forceinline__ void cell_energy(double (&v)[4], const char* base, ui
     remote_bonds<0, ISO, UNI, NC>(acc, own, base, sl_bytes, c, mats);
 #pragma unroll
     for (int k = 0; k < (UNI ? kAcc : 4); ++k) v[0] += UNI ? double(mats.M[0][k][0]) * double(acc[k]) : double(acc[k]);
+    if constexpr (GROUPS) {
+#pragma unroll
+        for (int k = 0; k < kAcc; ++k) gs[k] = double(acc[k]);
+    }
     float3 m = own[0];
 #pragma unroll
     for (int sl = 1; sl < 16; ++sl) {

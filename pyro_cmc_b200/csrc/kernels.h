@@ -144,6 +144,7 @@ struct EnergyCellArgs {
     int iso;  // as EnergyArgs::iso
     int uniform;  // iso != 0 and every group's j the same on all 16 sublattices: per-group bond sums
     PyroMats mats;
+    double* group_partial;  // uniform only, or null: [n_tiles][kGroups] bare sums of S_i.S_j per group
 };
 void launch_energy_cells(const EnergyCellArgs& a, cudaStream_t st);
 

@@ -192,6 +192,7 @@ struct pc_system {
     DevBuf<float4> d_field;
     DevBuf<double> d_grad_g, d_grad_out;  // energy-gradient upstream scalars and results
     DevBuf<double> d_grad_ones;           // g = 1 per replica (pc_energy_grad_device without g)
+    DevBuf<double> d_group_partial, d_group_out;  // per-group bond sums (pc_energy_groups_device)
     // structured energy gradient: specs per (sublattice, group, bond side) and
     // work items of up to kGradK tiles of one (replica, sublattice)
     bool grad_struct = false;
@@ -311,6 +312,8 @@ struct pc_system {
         d_ssf_sq.release();
         d_grad_g.release();
         d_grad_ones.release();
+        d_group_partial.release();
+        d_group_out.release();
         d_grad_out.release();
         d_grad_items.release();
         d_item_begin.release();
@@ -871,7 +874,9 @@ int run_sweeps(pc_system* s, int n_sweeps, int n_or) {
     return PC_OK;
 }
 
-int enqueue_energy(pc_system* s) {
+// groups (iso_kind 1, iso_uniform): also the per-replica bare sums of S_i.S_j
+// per coupling group into d_group_out [R][kGroups]
+int enqueue_energy(pc_system* s, bool groups = false) {
     if (s->structured) {  // one thread per cubic cell, each bond once (energy_cell.cu)
         pc::EnergyCellArgs c;
         c.spins = s->d_spins.p;
@@ -883,12 +888,25 @@ int enqueue_energy(pc_system* s) {
         c.iso = s->iso_kind;
         c.uniform = s->iso_uniform ? 1 : 0;
         c.mats = s->mats;
+        c.group_partial = nullptr;
+        if (groups) {
+            if (s->d_group_partial.n != size_t(s->n_cell_tiles) * pc::kGroups)
+                PC_CK(s->d_group_partial.alloc(size_t(s->n_cell_tiles) * pc::kGroups));
+            if (s->d_group_out.n != size_t(s->R) * pc::kGroups) PC_CK(s->d_group_out.alloc(size_t(s->R) * pc::kGroups));
+            c.group_partial = s->d_group_partial.p;
+        }
         pc::launch_energy_cells(c, s->stream);
         PC_LAUNCH_CK();
         pc::launch_energy_finalize(s->d_cell_partial.p, s->d_cell_begin.p, s->d_cell_end.p, s->d_reps.p, s->R,
                                    s->d_e.p, s->d_mag.p, s->stream);
         PC_LAUNCH_CK();
         s->launches += 2;
+        if (groups) {
+            pc::launch_grad_finalize(s->d_group_partial.p, pc::kGroups, s->d_cell_begin.p, s->d_cell_end.p, s->R,
+                                     s->d_group_out.p, s->stream);
+            PC_LAUNCH_CK();
+            s->launches++;
+        }
         return PC_OK;
     }
     pc::EnergyArgs a;
@@ -2269,6 +2287,26 @@ int pc_energy_device(pc_system* sys, double* e_dev) {
     rc = enqueue_energy(sys);
     if (rc) return rc;
     PC_CK(cudaMemcpyAsync(e_dev, sys->d_e.p, sizeof(double) * size_t(sys->R), cudaMemcpyDeviceToDevice, sys->stream));
+    return PC_OK;
+}
+
+int pc_energy_groups_device(pc_system* sys, double* e_dev, double* out_dev) {
+    int rc = check_sys(sys);
+    if (rc) return rc;
+    if (!sys->structured || sys->iso_kind != 1 || !sys->iso_uniform)
+        return fail(PC_ERR_UNSUPPORTED, "pc_energy_groups_device needs isotropic couplings, every group nonzero and "
+                                        "the same on all sublattices");
+    if (!e_dev || !out_dev || reinterpret_cast<uintptr_t>(e_dev) % 8 != 0 ||
+        reinterpret_cast<uintptr_t>(out_dev) % 8 != 0)
+        return fail(PC_ERR_INVALID, "pc_energy_groups_device: null or misaligned output");
+    rc = enqueue_energy(sys, true);
+    if (rc) return rc;
+    const size_t R = size_t(sys->R), row = size_t(pc::kGroups + 3) * sizeof(double);
+    PC_CK(cudaMemcpyAsync(e_dev, sys->d_e.p, sizeof(double) * R, cudaMemcpyDeviceToDevice, sys->stream));
+    PC_CK(cudaMemcpy2DAsync(out_dev, row, sys->d_group_out.p, pc::kGroups * sizeof(double),
+                            pc::kGroups * sizeof(double), R, cudaMemcpyDeviceToDevice, sys->stream));
+    PC_CK(cudaMemcpy2DAsync(out_dev + pc::kGroups, row, sys->d_mag.p, 3 * sizeof(double), 3 * sizeof(double), R,
+                            cudaMemcpyDeviceToDevice, sys->stream));
     return PC_OK;
 }
 

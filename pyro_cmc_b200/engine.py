@@ -452,6 +452,13 @@ class System:
         at e_ptr (R doubles) on the system's stream, without waiting."""
         call("pc_energy_device", self._h, C.c_void_p(e_ptr))
 
+    def energy_groups_device(self, e_ptr: int, out_ptr: int):
+        """pc_energy_groups_device: energies (R device doubles) and per replica
+        [the six coupling groups' bare bond sums, sum S] (R x 9 device
+        doubles), queued; raises PyroCMCError code 4 (unsupported) unless the
+        couplings are isotropic, nonzero and uniform over the sublattices."""
+        call("pc_energy_groups_device", self._h, C.c_void_p(e_ptr), C.c_void_p(out_ptr))
+
     def energy_grad_device(self, g_ptr: int | None, grad_spins_ptr: int | None, sums_ptr: int | None,
                            couplings: bool):
         """Queues pc_energy_grad_device: upstream g (R device doubles, None:

@@ -246,3 +246,25 @@ def test_kept_ssf_amplitudes_give_the_recomputed_backward():
     s.ssf_backward_kept(t1, go.data_ptr(), got.data_ptr())
     torch.cuda.synchronize()
     assert torch.equal(got, ref)
+
+
+@pytest.mark.parametrize("J2", [0.1, 0.0])
+def test_isotropic_parameter_gradient_from_the_energy_pass(J2):
+    """With isotropic J1, J2, J3 (Delta = 1, every group nonzero) the gradient
+    in [J1, J2, J3, B] comes from the forward energy pass's per-group bond sums
+    (pc_energy_groups_device); it agrees with the general path's coupling
+    products (pc_energy_grad) to the rounding of the FP32 per-cell sums. With
+    J2 = 0 (its group skipped by the energy pass) the general path runs."""
+    s = pc.pyrochlore_system(6, n_replicas=4, J1=1.0, J2=J2, J3=-0.05, B=(0.2, 0.0, 0.1), seed=8)
+    s.random_spins(12)
+    spins = ag.spins_tensor(s).clone().requires_grad_(True)
+    params = torch.tensor([1.0, J2, -0.05, 0.2, 0.0, 0.1], dtype=torch.float64, requires_grad=True)
+    up = torch.tensor([0.3, -1.0, 2.0, 0.5], dtype=torch.float64, device="cuda")
+    e = ag.energy(s, spins, params)
+    (e * up).sum().backward()
+    gs_ref = torch.empty_like(spins)
+    e2, gJ, gB = s.energy_grad(up.cpu().numpy(), gs_ref.data_ptr(), couplings=True)
+    ref = ag._param_grads(s, gJ, gB).sum(axis=0)
+    np.testing.assert_allclose(params.grad.numpy(), ref, rtol=1e-5, atol=1e-7 * np.abs(ref).max())
+    np.testing.assert_allclose(e.detach().cpu().numpy(), e2, rtol=1e-5)
+    torch.testing.assert_close(spins.grad, gs_ref, rtol=1e-5, atol=1e-6)
