@@ -34,6 +34,9 @@ constexpr int kVarIso = 5, kVarIsoNoJ2 = 6;
 // for a kernel that writes them in an earlier phase of the same launch (the
 // persistent tempering kernel, whose grid barrier orders the phases).
 constexpr int kVarCoherent = 0x100;
+// Or'ed into kVarIso by the per-pass fused rotation kernel: neighbour
+// addresses from per-sublattice bases (load_nb's UB form).
+constexpr int kVarUniformBase = 0x200;
 // The per-replica constants of a Metropolis proposal at temperature T: the
 // kick width sqrt(T / T_ref) and 1 / T, rounded as the moves use them. Formed
 // once per replica whenever the temperatures change, not per site.

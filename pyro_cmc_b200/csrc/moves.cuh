@@ -334,8 +334,9 @@ __global__ void __launch_bounds__(512) colour_pass_kernel(const __grid_constant_
 template <int SL, int VAR_>
 __device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const PassArgs& a, const ReplicaDev& rep,
                                              const Coords& c, float4 (&v)[kStructNb], int phase) {
-    constexpr int VAR = VAR_ & ~kVarCoherent;
+    constexpr int VAR = VAR_ & ~(kVarCoherent | kVarUniformBase);
     constexpr bool NC = (VAR_ & kVarCoherent) == 0;
+    constexpr bool UB = (VAR_ & kVarUniformBase) != 0;
     static_assert(NC || VAR == 0 || VAR == kVarIso || VAR == kVarIsoNoJ2, "coherent loads: variants 0 and iso");
     constexpr int kJ3 = grp_begin(SL, 4);
     float3 h = make_float3(0.f, 0.f, 0.f);
@@ -350,12 +351,12 @@ __device__ __forceinline__ float3 site_field(const float4* __restrict__ S, const
         }
     } else if constexpr (VAR == kVarIso || VAR == kVarIsoNoJ2) {
         if (phase == 1) {
-            add_group_iso<SL, 0, NC>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 1, NC>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 2, NC>(h, S, rep.Nc, c, a.mats);
-            if constexpr (VAR == kVarIso) add_group_iso<SL, 3, NC>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 4, NC>(h, S, rep.Nc, c, a.mats);
-            add_group_iso<SL, 5, NC>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 0, NC, UB>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 1, NC, UB>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 2, NC, UB>(h, S, rep.Nc, c, a.mats);
+            if constexpr (VAR == kVarIso) add_group_iso<SL, 3, NC, UB>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 4, NC, UB>(h, S, rep.Nc, c, a.mats);
+            add_group_iso<SL, 5, NC, UB>(h, S, rep.Nc, c, a.mats);
         }
     } else if constexpr (VAR == 1) {
         if (phase == 0)
@@ -475,6 +476,11 @@ __device__ __forceinline__ bool struct_site(const PassArgs& a, float4* S, const 
 // coupling matrices per (sublattice, group) in the kernel parameters.
 template <int MODE, int VAR>
 __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant__ PassArgs a) {
+    // fused isotropic rotation passes with every group active: neighbour
+    // addresses from per-sublattice bases (measured faster there; other passes
+    // keep the full offset sums -- with J2 = 0 the faster tile moved, and the
+    // persistent kernel, which inherits the tile, lost more than the pass gained)
+    constexpr int VARX = (MODE == kFusedRotate && VAR == kVarIso) ? (VAR | kVarUniformBase) : VAR;
     __shared__ unsigned int warp_acc[8];
     pdl_wait();
     const uint64_t sweep = *a.sweep_base + a.sweep_offset;
@@ -492,7 +498,7 @@ __global__ void __launch_bounds__(256) struct_pass_kernel(const __grid_constant_
         if (int(threadIdx.x) < tile.w) {
             const int cell = tile.z + int(threadIdx.x);
             bool accepted = false;
-#define PC_CALL(K) accepted = struct_site<MODE, K, VAR>(a, S, rep, r, cell, sweep)
+#define PC_CALL(K) accepted = struct_site<MODE, K, VARX>(a, S, rep, r, cell, sweep)
             PC_SL_SWITCH(sl, PC_CALL)
 #undef PC_CALL
             mine += accepted ? 1u : 0u;
